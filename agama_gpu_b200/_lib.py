@@ -1,0 +1,110 @@
+"""ctypes binding of the in-tree CUDA library libagb.so (C ABI in include/agb.h).
+
+The library is required: there is no CPU path.  Importing this module on a
+machine without the built library raises ImportError; calling it without a
+CUDA device raises RuntimeError from the first evaluation.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libagb.so"
+
+AGB_OK = 0
+MODE_POT, MODE_GRAD, MODE_HESS, MODE_DENS = 0, 1, 2, 3
+PREC_FP64, PREC_MIXED = 0, 1
+OUT_NEGATE = 1
+
+KIND_MULTIPOLE = 1
+KIND_CYLSPLINE = 2
+KIND_NFW = 10
+KIND_PLUMMER = 11
+KIND_HERNQUIST = 12
+KIND_DEHNEN = 13
+KIND_ISOCHRONE = 14
+KIND_MIYAMOTONAGAI = 15
+KIND_LOGHALO = 16
+KIND_DISKANSATZ = 17
+KIND_UNIFORMACC = 18
+
+LAYOUT_HARMONIC_MAJOR = 0
+LAYOUT_INTERVAL_MAJOR = 1
+
+MAX_LEAVES = 32
+MAX_COMPONENTS = 24
+
+
+class AgbComponent(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("n_lm", ctypes.c_int32),
+        ("n_int", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("lmax", ctypes.c_int32),
+        ("log_scaling", ctypes.c_int32),
+        ("layout", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("table", ctypes.c_void_p),
+        ("table32", ctypes.c_void_p),
+        ("lm", ctypes.c_void_p),
+        ("grid_a", ctypes.c_void_p),
+        ("grid_b", ctypes.c_void_p),
+        ("extra", ctypes.c_void_p),
+        ("p", ctypes.c_double * 16),
+    ]
+
+
+class AgbLeaf(ctypes.Structure):
+    _fields_ = [
+        ("comp", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("sigma", ctypes.c_double),
+        ("gamma", ctypes.c_double * 3),
+        ("ampl", ctypes.c_double),
+    ]
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library with "
+            "`python -m agama_gpu_b200.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    lib.agb_last_error.restype = ctypes.c_char_p
+    lib.agb_version.restype = ctypes.c_char_p
+    lib.agb_launch_count.restype = ctypes.c_int64
+    lib.agb_eval.restype = ctypes.c_int
+    lib.agb_eval.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_int, ctypes.c_void_p]
+    return lib
+
+
+lib = _load()
+
+# symbols the header declares (checked by tests/test_capi.py)
+EXPORTED = [
+    "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
+    "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
+    "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
+]
+
+
+def last_error() -> str:
+    return lib.agb_last_error().decode()
+
+
+def check(rc: int, what: str) -> None:
+    if rc != AGB_OK:
+        raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
+
+
+def launch_count() -> int:
+    return int(lib.agb_launch_count())
+
+
+def launch_count_reset() -> None:
+    lib.agb_launch_count_reset()

@@ -1,0 +1,368 @@
+// eval.cu -- the fused per-point kernel and the C ABI (include/agb.h).
+//
+// One thread per point (grid-stride).  Each thread reads its position once,
+// walks the leaves (component + Shifted/Scaled/Evolving transform) in order,
+// evaluates each component in its own frame and accumulates
+//   Phi += A Phi_c,  grad += A sigma grad_c,  H/rho += A sigma^2 (H_c/rho_c)
+// in FP64, then writes the outputs once.  This replaces the reference's chain
+// of one launch per component plus CuPy elementwise passes for shifts, scales,
+// negation, lerps and sums (gpu_potential.py:1439-1918).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <stdarg.h>
+#include "agb_dev.cuh"
+#include "multipole.cuh"
+#include "cylspline.cuh"
+#include "analytic.cuh"
+
+// ---------------------------------------------------------------------------
+// errors and launch accounting
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+static thread_local long long g_launches = 0;
+
+static int set_err(int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+extern "C" const char* agb_last_error(void) { return g_err; }
+extern "C" const char* agb_version(void) { return "agama_gpu_b200 0.1 (sm_100a)"; }
+extern "C" int64_t agb_launch_count(void) { return g_launches; }
+extern "C" void agb_launch_count_reset(void) { g_launches = 0; }
+
+static int check_launch(const char* what)
+{
+    ++g_launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return set_err(AGB_ERR_DEVICE, "%s: launch failed: %s", what, cudaGetErrorString(e));
+    return AGB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the fused kernel
+// ---------------------------------------------------------------------------
+template <int MODE, typename R>
+__device__ __forceinline__ void eval_component(const DevComp& c, double x, double y, double z,
+                                               PointOut& o)
+{
+    switch (c.kind) {
+    case AGB_KIND_MULTIPOLE:     multipole_point<MODE, R>(c, x, y, z, o); break;
+    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE>(c, x, y, z, o); break;
+    case AGB_KIND_NFW:           nfw_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_PLUMMER:       plummer_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_HERNQUIST:     hernquist_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_DEHNEN:        dehnen_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_ISOCHRONE:     isochrone_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_MIYAMOTONAGAI: mn_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_LOGHALO:       loghalo_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_DISKANSATZ:    diskansatz_point<MODE>(c.p, x, y, z, o); break;
+    case AGB_KIND_UNIFORMACC:    uniform_point<MODE>(c.p, x, y, z, o); break;
+    default: break;
+    }
+}
+
+template <int MODE, typename R>
+__global__ void __launch_bounds__(256)
+agb_eval_kernel(const __grid_constant__ EvalArgs a)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        double x, y, z;
+        if (a.soa) {
+            x = a.x[i]; y = a.y[i]; z = a.z[i];
+        } else {
+            x = a.xyz[3 * i]; y = a.xyz[3 * i + 1]; z = a.xyz[3 * i + 2];
+        }
+        double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
+        double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int L = 0; L < a.n_leaves; ++L) {
+            const DevLeaf& lf = a.leaves[L];
+            const DevComp& c = a.comps[lf.comp];
+            const double lx = lf.sigma * x - lf.g0;
+            const double ly = lf.sigma * y - lf.g1;
+            const double lz = lf.sigma * z - lf.g2;
+            PointOut o;
+            o.phi = 0.0; o.rho = 0.0;
+            o.g[0] = o.g[1] = o.g[2] = 0.0;
+            #pragma unroll
+            for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
+            eval_component<MODE, R>(c, lx, ly, lz, o);
+            const double A = lf.ampl;
+            if (MODE == AGB_MODE_DENS) {
+                rho += (A * lf.sigma * lf.sigma) * o.rho;
+                continue;
+            }
+            phi += A * o.phi;
+            if (MODE != AGB_MODE_POT) {
+                const double As = A * lf.sigma;
+                g0 += As * o.g[0]; g1 += As * o.g[1]; g2 += As * o.g[2];
+                if (MODE == AGB_MODE_HESS) {
+                    const double As2 = As * lf.sigma;
+                    #pragma unroll
+                    for (int q = 0; q < 6; ++q) h[q] += As2 * o.h[q];
+                }
+            }
+        }
+        const double sg = (a.out_flags & AGB_OUT_NEGATE) ? -1.0 : 1.0;
+        if (MODE == AGB_MODE_DENS) {
+            a.rho[i] = rho;
+            continue;
+        }
+        if (a.phi) a.phi[i] = phi;
+        if (MODE != AGB_MODE_POT && a.grad) {
+            a.grad[3 * i] = sg * g0; a.grad[3 * i + 1] = sg * g1; a.grad[3 * i + 2] = sg * g2;
+        }
+        if (MODE == AGB_MODE_HESS) {
+            #pragma unroll
+            for (int q = 0; q < 6; ++q) a.hess[6 * i + q] = sg * h[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static int g_num_sms = 0;
+
+static int grid_for(long long n)
+{
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    const long long blocks = (n + 255) / 256;
+    const long long cap = (long long)g_num_sms * 64;
+    return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+
+template <int MODE, typename R>
+static void launch_eval(const EvalArgs& a, cudaStream_t st)
+{
+    agb_eval_kernel<MODE, R><<<grid_for(a.n), 256, 0, st>>>(a);
+}
+
+static int launch_mode(int mode, int precision, const EvalArgs& a, cudaStream_t st)
+{
+    const bool mixed = precision == AGB_PREC_MIXED;
+    switch (mode) {
+    case AGB_MODE_POT:  mixed ? launch_eval<AGB_MODE_POT, float>(a, st)  : launch_eval<AGB_MODE_POT, double>(a, st); break;
+    case AGB_MODE_GRAD: mixed ? launch_eval<AGB_MODE_GRAD, float>(a, st) : launch_eval<AGB_MODE_GRAD, double>(a, st); break;
+    case AGB_MODE_HESS: mixed ? launch_eval<AGB_MODE_HESS, float>(a, st) : launch_eval<AGB_MODE_HESS, double>(a, st); break;
+    case AGB_MODE_DENS: mixed ? launch_eval<AGB_MODE_DENS, float>(a, st) : launch_eval<AGB_MODE_DENS, double>(a, st); break;
+    default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
+    }
+    return check_launch("agb_eval_kernel");
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+static int comp_to_dev(const agb_component& s, DevComp& d, int precision)
+{
+    memset(&d, 0, sizeof(d));
+    d.kind = s.kind;
+    d.n_lm = s.n_lm; d.n_int = s.n_int; d.nz = s.nz; d.lmax = s.lmax;
+    d.log_scaling = s.log_scaling; d.layout = s.layout; d.lm_split = 0;
+    d.table = s.table; d.table32 = s.table32; d.lm = s.lm; d.lm_m = nullptr;
+    d.grid_a = s.grid_a; d.grid_b = s.grid_b; d.extra = s.extra;
+    memcpy(d.p, s.p, sizeof(d.p));
+    if (s.kind == AGB_KIND_MULTIPOLE) {
+        if (!s.table || !s.lm || s.n_lm < 1 || s.n_int < 1)
+            return set_err(AGB_ERR_ARG, "multipole component: missing table/lm or empty sizes");
+        if (s.lmax > AGB_MAX_LMAX)
+            return set_err(AGB_ERR_UNSUPPORTED, "multipole lmax=%d exceeds %d", s.lmax, AGB_MAX_LMAX);
+        if (!aligned16(s.table))
+            return set_err(AGB_ERR_ARG, "multipole table must be 16-byte aligned");
+        if (precision == AGB_PREC_MIXED) {
+            if (!s.table32 || !aligned16(s.table32))
+                return set_err(AGB_ERR_ARG, "mixed precision needs a 16-byte aligned FP32 table");
+        }
+    } else if (s.kind == AGB_KIND_CYLSPLINE) {
+        if (!s.table || !s.lm || !s.grid_a || !s.grid_b || !s.extra || s.n_int < 2 || s.nz < 2)
+            return set_err(AGB_ERR_ARG, "cylspline component: missing tables or grid < 2 nodes");
+        if (!aligned16(s.table))
+            return set_err(AGB_ERR_ARG, "cylspline table must be 16-byte aligned");
+        if (s.lmax > AGB_MAX_LMAX || (int)s.p[2] > s.lmax)
+            return set_err(AGB_ERR_ARG, "cylspline outer multipole orders out of range");
+    } else if (s.kind < AGB_KIND_NFW || s.kind > AGB_KIND_UNIFORMACC) {
+        return set_err(AGB_ERR_ARG, "unknown component kind %d", s.kind);
+    }
+    return AGB_OK;
+}
+
+extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                        int n_leaves, const double* xyz, int64_t n, int mode, int precision,
+                        double* phi, double* grad, double* hess, double* rho, int out_flags,
+                        void* stream)
+{
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_eval: negative point count");
+    if (n == 0) return AGB_OK;
+    if (!xyz) return set_err(AGB_ERR_ARG, "agb_eval: xyz is null");
+    if (!comps || n_comps < 1 || !leaves || n_leaves < 1)
+        return set_err(AGB_ERR_ARG, "agb_eval: empty component or leaf list");
+    if (n_leaves > AGB_MAX_LEAVES)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_eval: %d leaves exceed %d", n_leaves, AGB_MAX_LEAVES);
+    if (precision != AGB_PREC_FP64 && precision != AGB_PREC_MIXED)
+        return set_err(AGB_ERR_ARG, "agb_eval: unknown precision %d", precision);
+    switch (mode) {
+    case AGB_MODE_POT:  if (!phi) return set_err(AGB_ERR_ARG, "agb_eval: phi is null"); break;
+    case AGB_MODE_GRAD: if (!grad) return set_err(AGB_ERR_ARG, "agb_eval: grad is null"); break;
+    case AGB_MODE_HESS: if (!hess) return set_err(AGB_ERR_ARG, "agb_eval: hess is null"); break;
+    case AGB_MODE_DENS: if (!rho) return set_err(AGB_ERR_ARG, "agb_eval: rho is null"); break;
+    default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
+    }
+
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n; a.out_flags = out_flags; a.soa = 0; a.xyz = xyz;
+    a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    // pack only the components the leaves use
+    int remap[256];
+    for (int i = 0; i < 256; ++i) remap[i] = -1;
+    int nc = 0;
+    for (int L = 0; L < n_leaves; ++L) {
+        const int ci = leaves[L].comp;
+        if (ci < 0 || ci >= n_comps || ci >= 256)
+            return set_err(AGB_ERR_ARG, "agb_eval: leaf %d refers to component %d of %d", L, ci, n_comps);
+        if (remap[ci] < 0) {
+            if (nc >= AGB_MAX_COMPONENTS)
+                return set_err(AGB_ERR_UNSUPPORTED, "agb_eval: more than %d distinct components", AGB_MAX_COMPONENTS);
+            const int rc = comp_to_dev(comps[ci], a.comps[nc], precision);
+            if (rc) return rc;
+            remap[ci] = nc++;
+        }
+        DevLeaf& d = a.leaves[L];
+        d.comp = remap[ci];
+        d.sigma = leaves[L].sigma;
+        d.g0 = leaves[L].gamma[0]; d.g1 = leaves[L].gamma[1]; d.g2 = leaves[L].gamma[2];
+        d.ampl = leaves[L].ampl;
+    }
+    a.n_leaves = n_leaves;
+    return launch_mode(mode, precision, a, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// kernel-signature entries
+// ---------------------------------------------------------------------------
+static int mp_compat(int mode, const double* x, const double* y, const double* z,
+                     const double* poly, double logr_min, double dlogr, double inv_dlogr,
+                     int n_intervals, int n_lm, int lmax, const int* lm_l, const int* lm_m,
+                     int log_scaling, double invPhi0, double inner_s, double inner_U,
+                     double inner_W, double outer_s, double outer_U, double outer_W,
+                     double* phi, double* grad, double* hess, double* rho, int N, void* stream)
+{
+    if (N < 0) return set_err(AGB_ERR_ARG, "negative N");
+    if (N == 0) return AGB_OK;
+    if (!x || !y || !z || !poly || !lm_l || !lm_m)
+        return set_err(AGB_ERR_ARG, "multipole: null input pointer");
+    if (n_lm < 1 || n_intervals < 1) return set_err(AGB_ERR_ARG, "multipole: empty tables");
+    if (lmax > AGB_MAX_LMAX) return set_err(AGB_ERR_UNSUPPORTED, "lmax=%d exceeds %d", lmax, AGB_MAX_LMAX);
+    if (!aligned16(poly)) return set_err(AGB_ERR_ARG, "poly must be 16-byte aligned");
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = N; a.soa = 1; a.x = x; a.y = y; a.z = z;
+    a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    DevComp& c = a.comps[0];
+    c.kind = AGB_KIND_MULTIPOLE; c.n_lm = n_lm; c.n_int = n_intervals; c.lmax = lmax;
+    c.log_scaling = log_scaling; c.layout = AGB_LAYOUT_HARMONIC_MAJOR; c.lm_split = 1;
+    c.table = poly; c.lm = lm_l; c.lm_m = lm_m;
+    const double p[10] = {logr_min, dlogr, inv_dlogr, invPhi0, inner_s, inner_U, inner_W,
+                          outer_s, outer_U, outer_W};
+    memcpy(c.p, p, sizeof(p));
+    a.n_leaves = 1;
+    a.leaves[0].comp = 0; a.leaves[0].sigma = 1.0; a.leaves[0].ampl = 1.0;
+    return launch_mode(mode, AGB_PREC_FP64, a, (cudaStream_t)stream);
+}
+
+#define MP_SIG const double* x, const double* y, const double* z, const double* poly,       \
+    double logr_min, double dlogr, double inv_dlogr, int n_intervals, int n_lm, int lmax,   \
+    const int* lm_l, const int* lm_m, int log_scaling, double invPhi0, double inner_s,      \
+    double inner_U, double inner_W, double outer_s, double outer_U, double outer_W
+#define MP_FWD x, y, z, poly, logr_min, dlogr, inv_dlogr, n_intervals, n_lm, lmax, lm_l,    \
+    lm_m, log_scaling, invPhi0, inner_s, inner_U, inner_W, outer_s, outer_U, outer_W
+
+extern "C" int agb_multipole_potential(MP_SIG, double* phi_out, double* grad_out, int N, void* stream)
+{
+    (void)grad_out;
+    if (!phi_out) return set_err(AGB_ERR_ARG, "phi_out is null");
+    return mp_compat(AGB_MODE_POT, MP_FWD, phi_out, nullptr, nullptr, nullptr, N, stream);
+}
+extern "C" int agb_multipole_force(MP_SIG, double* phi_out, double* grad_out, int N, void* stream)
+{
+    if (!phi_out || !grad_out) return set_err(AGB_ERR_ARG, "phi_out/grad_out is null");
+    return mp_compat(AGB_MODE_GRAD, MP_FWD, phi_out, grad_out, nullptr, nullptr, N, stream);
+}
+extern "C" int agb_multipole_hess(MP_SIG, double* phi_out, double* grad_out, double* hess_out,
+                                  int N, void* stream)
+{
+    if (!phi_out || !grad_out || !hess_out) return set_err(AGB_ERR_ARG, "output pointer is null");
+    return mp_compat(AGB_MODE_HESS, MP_FWD, phi_out, grad_out, hess_out, nullptr, N, stream);
+}
+extern "C" int agb_multipole_density(MP_SIG, double inv_4piG, double* rho_out, int N, void* stream)
+{
+    if (!rho_out) return set_err(AGB_ERR_ARG, "rho_out is null");
+    if (inv_4piG != AGB_INV_4PIG && fabs(inv_4piG / AGB_INV_4PIG - 1.0) > 1e-12)
+        return set_err(AGB_ERR_UNSUPPORTED, "inv_4piG must be 1/(4 pi G) in Agama units");
+    return mp_compat(AGB_MODE_DENS, MP_FWD, nullptr, nullptr, nullptr, rho_out, N, stream);
+}
+
+static int cs_compat(int mode, const double* x, const double* y, const double* z, double Rscale,
+                     const double* lR_grid, int nR, const double* lz_grid, int nz,
+                     const double* node_arr, int n_harm, const int* m_arr, int mmax,
+                     int log_scaling, const double* W_outer, double r0_outer, int lmax_outer,
+                     int mmax_outer, double* phi, double* grad, double* hess, int N, void* stream)
+{
+    (void)mmax;
+    if (N < 0) return set_err(AGB_ERR_ARG, "negative N");
+    if (N == 0) return AGB_OK;
+    if (!x || !y || !z || !lR_grid || !lz_grid || !node_arr || !m_arr || !W_outer)
+        return set_err(AGB_ERR_ARG, "cylspline: null input pointer");
+    if (nR < 2 || nz < 2 || n_harm < 1) return set_err(AGB_ERR_ARG, "cylspline: grid too small");
+    if (lmax_outer > AGB_MAX_LMAX || mmax_outer > lmax_outer || mmax_outer < 0)
+        return set_err(AGB_ERR_ARG, "cylspline: outer orders out of range");
+    if (!aligned16(node_arr)) return set_err(AGB_ERR_ARG, "node_arr must be 16-byte aligned");
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = N; a.soa = 1; a.x = x; a.y = y; a.z = z;
+    a.phi = phi; a.grad = grad; a.hess = hess;
+    DevComp& c = a.comps[0];
+    c.kind = AGB_KIND_CYLSPLINE; c.n_lm = n_harm; c.n_int = nR; c.nz = nz; c.lmax = lmax_outer;
+    c.log_scaling = log_scaling; c.layout = 0; c.table = node_arr; c.lm = m_arr;
+    c.grid_a = lR_grid; c.grid_b = lz_grid; c.extra = W_outer;
+    c.p[0] = Rscale; c.p[1] = r0_outer; c.p[2] = (double)mmax_outer;
+    a.n_leaves = 1;
+    a.leaves[0].comp = 0; a.leaves[0].sigma = 1.0; a.leaves[0].ampl = 1.0;
+    return launch_mode(mode, AGB_PREC_FP64, a, (cudaStream_t)stream);
+}
+
+#define CS_SIG const double* x, const double* y, const double* z, double Rscale,              \
+    const double* lR_grid, int nR, const double* lz_grid, int nz, const double* node_arr,    \
+    int n_harm, const int* m_arr, int mmax, int log_scaling, const double* W_outer,          \
+    double r0_outer, int lmax_outer, int mmax_outer
+#define CS_FWD x, y, z, Rscale, lR_grid, nR, lz_grid, nz, node_arr, n_harm, m_arr, mmax,     \
+    log_scaling, W_outer, r0_outer, lmax_outer, mmax_outer
+
+extern "C" int agb_cylspl_potential(CS_SIG, double* phi_out, int N, void* stream)
+{
+    if (!phi_out) return set_err(AGB_ERR_ARG, "phi_out is null");
+    return cs_compat(AGB_MODE_POT, CS_FWD, phi_out, nullptr, nullptr, N, stream);
+}
+extern "C" int agb_cylspl_force(CS_SIG, double* phi_out, double* grad_out, int N, void* stream)
+{
+    if (!phi_out || !grad_out) return set_err(AGB_ERR_ARG, "output pointer is null");
+    return cs_compat(AGB_MODE_GRAD, CS_FWD, phi_out, grad_out, nullptr, N, stream);
+}
+extern "C" int agb_cylspl_hess(CS_SIG, double* phi_out, double* grad_out, double* hess_out, int N,
+                               void* stream)
+{
+    if (!phi_out || !grad_out || !hess_out) return set_err(AGB_ERR_ARG, "output pointer is null");
+    return cs_compat(AGB_MODE_HESS, CS_FWD, phi_out, grad_out, hess_out, N, stream);
+}

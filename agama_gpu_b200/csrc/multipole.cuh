@@ -1,0 +1,391 @@
+// multipole.cuh -- per-point evaluation of an Agama Multipole expansion.
+//
+// Follows the reference's kernels (_multipole_potential_kernel.cu):
+//   * log-r interval lookup, s clamp and the r < 1e-300 origin rule (:160-216);
+//   * inner power-law l=0 extrapolation U (r/r0)^s + W (:177-193, :492-520,
+//     :836-847) and outer W (r/rN)^-1 + U (r/rN)^s (:197-214, :522-549);
+//   * quintic Horner value/derivatives on s in [0,1] (:100-118);
+//   * Agama log-scaling: c=0 stores log(invPhi0 - 1/Phi0), c>0 store Phi_c/Phi0
+//     (:239-258, :566-585);
+//   * pole-safe gradient (:388-409), full Cartesian Hessian chain rule (:713-799),
+//     Laplacian density with zero density beyond the grid (:851, :915).
+// Differences in form, not in result:
+//   * Legendre functions come from the normalised recurrence with tabulated
+//     ALPHA/BETA (legendre_tables.cuh) instead of an un-normalised recurrence
+//     with a sqrt per step; cos/sin(m phi) from x/R, y/R and a rotation instead
+//     of atan2 + sincos;
+//   * the log-scaling chain rule is factored out of the harmonic loop: the loop
+//     accumulates sums of C_c Y T, dC_c Y T, ... and the monopole factor is
+//     applied once per point;
+//   * the loop is templated on the real type R: double (plain FP64) or float
+//     (mixed: FP32 recurrences and polynomials, per-|m| FP32 partial sums
+//     promoted to FP64, FP64 everywhere else).
+#pragma once
+#include "agb_dev.cuh"
+
+// Radial sums of one Multipole at one point (component frame).
+struct MPSums {
+    double A, B, D, L;              // sum C Y T, dC/ds Y T, d2C/ds2 Y T, l(l+1) C Y T
+    double Th, Pos;                 // C dY T, C (Y/sin) dT
+    double Thth, BTh, Ph, Phph, BPh, ThPh;
+};
+
+template <typename R> struct MPGroup {
+    R A, B, D, L, Th, Pos, Thth, BTh, Ph, Phph, BPh, ThPh;
+    __device__ __forceinline__ void zero() {
+        A = B = D = L = Th = Pos = Thth = BTh = Ph = Phph = BPh = ThPh = R(0);
+    }
+};
+
+template <int MODE, typename R>
+__device__ __forceinline__ void mp_flush(MPSums& t, MPGroup<R>& g)
+{
+    t.A += (double)g.A;
+    if (MODE != AGB_MODE_POT) t.B += (double)g.B;
+    if (MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS) t.D += (double)g.D;
+    if (MODE == AGB_MODE_DENS) t.L += (double)g.L;
+    if (MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS) {
+        t.Th += (double)g.Th;
+        t.Pos += (double)g.Pos;
+    }
+    if (MODE == AGB_MODE_HESS) {
+        t.Thth += (double)g.Thth; t.BTh += (double)g.BTh; t.Ph += (double)g.Ph;
+        t.Phph += (double)g.Phph; t.BPh += (double)g.BPh; t.ThPh += (double)g.ThPh;
+    }
+    g.zero();
+}
+
+template <typename R> struct MPConst;
+template <> struct MPConst<double> {
+    static __device__ __forceinline__ double alpha(int i) { return AGB_ALPHA[i]; }
+    static __device__ __forceinline__ double beta(int i) { return AGB_BETA[i]; }
+};
+template <> struct MPConst<float> {
+    static __device__ __forceinline__ float alpha(int i) { return AGB_ALPHA_F[i]; }
+    static __device__ __forceinline__ float beta(int i) { return AGB_BETA_F[i]; }
+};
+
+// Quintic coefficients of harmonic c in radial interval k.
+template <typename R> struct MPRec;
+template <> struct MPRec<double> {
+    static __device__ __forceinline__ void load(const DevComp& c, int ci, int k, double a[6])
+    {
+        const long long off = (c.layout == AGB_LAYOUT_INTERVAL_MAJOR)
+            ? ((long long)k * c.n_lm + ci) * 6
+            : ((long long)ci * c.n_int + k) * 6;
+        const double2* p = reinterpret_cast<const double2*>(c.table + off);
+        double2 v0 = __ldg(p), v1 = __ldg(p + 1), v2 = __ldg(p + 2);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y; a[4] = v2.x; a[5] = v2.y;
+    }
+};
+template <> struct MPRec<float> {
+    // FP32 table is interval-major with 8-float records (a0..a5, 0, 0).
+    static __device__ __forceinline__ void load(const DevComp& c, int ci, int k, float a[6])
+    {
+        const float4* p = reinterpret_cast<const float4*>(c.table32 + ((long long)k * c.n_lm + ci) * 8);
+        float4 v0 = __ldg(p), v1 = __ldg(p + 1);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v0.z; a[3] = v0.w; a[4] = v1.x; a[5] = v1.y;
+    }
+};
+
+__device__ __forceinline__ void mp_decode(const DevComp& c, int ci, int& l, int& m)
+{
+    if (c.lm_split) {
+        l = __ldg(c.lm + ci);
+        m = __ldg(c.lm_m + ci);
+    } else {
+        const int v = __ldg(c.lm + ci);
+        l = v >> 16;
+        m = (int)(short)(v & 0xffff);
+    }
+}
+
+// Harmonic sums over c = 1 .. n_lm-1 (c = 0 is the monopole, done in FP64).
+template <int MODE, typename R>
+__device__ __forceinline__ void mp_harmonics(const DevComp& c, int k, double s_d,
+                                             double cth_d, double sth_d,
+                                             double cph, double sph, MPSums& tot)
+{
+    constexpr bool NEED_B = MODE != AGB_MODE_POT;
+    constexpr bool NEED_D = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
+    constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
+    constexpr bool NEED_ANG2 = MODE == AGB_MODE_HESS;
+
+    const bool near_pole = sth_d < 1.0e-10;
+    const R s = (R)s_d;
+    const R cth = (R)cth_d;
+    const R sth = (R)sth_d;
+    const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
+    const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
+
+    double cm = 1.0, sm = 0.0;        // cos, sin of (cur * phi)
+    double sinpow = 1.0, sinpow_m1 = 0.0;
+    int cur = 0;
+    R Tc = R(1), Ts = R(0);
+    R Pp = R(0), Pc = (R)AGB_SEED[0], dPp = R(0), dPc = R(0);
+    int lc = 0;
+
+    MPGroup<R> g;
+    g.zero();
+
+    for (int ci = 1; ci < c.n_lm; ++ci) {
+        int l, m;
+        mp_decode(c, ci, l, m);
+        const int am = m < 0 ? -m : m;
+        // a harmonic outside 0 <= |m| <= l <= 32, or out of the sorted order,
+        // cannot be evaluated: skip it rather than index past the tables
+        if (l > AGB_MAX_LMAX || am > l || am < cur || (am == cur && l < lc)) continue;
+        if (am != cur) {
+            mp_flush<MODE, R>(tot, g);
+            for (int q = cur; q < am; ++q) {
+                const double t = cm * cph - sm * sph;
+                sm = sm * cph + cm * sph;
+                cm = t;
+                sinpow_m1 = sinpow;
+                sinpow *= sth_d;
+            }
+            cur = am;
+            Tc = (R)cm;
+            Ts = (R)sm;
+            Pc = (R)(AGB_SEED[am] * sinpow);
+            Pp = R(0);
+            dPp = R(0);
+            if (NEED_ANG) {
+                if (am == 1)
+                    dPc = (R)(AGB_SEED[1] * cth_d);
+                else
+                    dPc = near_pole ? R(0) : (R)((double)am * AGB_SEED[am] * sinpow_m1 * cth_d);
+            }
+            lc = am;
+        }
+        while (lc < l) {
+            ++lc;
+            const int ti = am * AGB_LEG_N + lc;
+            const R a = MPConst<R>::alpha(ti);
+            const R b = MPConst<R>::beta(ti);
+            const R Pn = a * (cth * Pc) - b * Pp;
+            if (NEED_ANG) {
+                const R dPn = a * (cth * dPc - sth * Pc) - b * dPp;
+                dPp = dPc;
+                dPc = dPn;
+            }
+            Pp = Pc;
+            Pc = Pn;
+        }
+
+        R q[6];
+        MPRec<R>::load(c, ci, k, q);
+        const R C = fma(s, fma(s, fma(s, fma(s, fma(s, q[5], q[4]), q[3]), q[2]), q[1]), q[0]);
+        R dC = R(0), d2C = R(0);
+        if (NEED_B)
+            dC = fma(s, fma(s, fma(s, fma(s, R(5) * q[5], R(4) * q[4]), R(3) * q[3]), R(2) * q[2]), q[1]);
+        if (NEED_D)
+            d2C = fma(s, fma(s, fma(s, R(20) * q[5], R(12) * q[4]), R(6) * q[3]), R(2) * q[2]);
+
+        const bool is_cos = m >= 0;
+        const R T = is_cos ? Tc : Ts;
+        const R YT = Pc * T;
+        g.A += C * YT;
+        if (NEED_B) g.B += dC * YT;
+        if (NEED_D) g.D += d2C * YT;
+        if (MODE == AGB_MODE_DENS) g.L += R(l * (l + 1)) * (C * YT);
+        if (NEED_ANG) {
+            const R dT = is_cos ? -R(am) * Ts : R(am) * Tc;
+            g.Th += C * (dPc * T);
+            R Pos = R(0);
+            if (am != 0) Pos = !near_pole ? Pc * inv_sth : (am == 1 ? dPc : R(0));
+            g.Pos += C * (Pos * dT);
+            if (NEED_ANG2) {
+                const R d2Y = near_pole ? R(0)
+                    : (-cot * dPc - (R(l * (l + 1)) - R(am * am) * inv_sth * inv_sth) * Pc);
+                g.Thth += C * (d2Y * T);
+                g.BTh  += dC * (dPc * T);
+                g.Ph   += C * (Pc * dT);
+                g.Phph += C * (Pc * (-R(am * am) * T));
+                g.BPh  += dC * (Pc * dT);
+                g.ThPh += C * (dPc * dT);
+            }
+        }
+    }
+    mp_flush<MODE, R>(tot, g);
+}
+
+__device__ __forceinline__ void mp_quintic0(const DevComp& c, int k, double s,
+                                            double& v, double& d1, double& d2)
+{
+    double q[6];
+    MPRec<double>::load(c, 0, k, q);
+    v = fma(s, fma(s, fma(s, fma(s, fma(s, q[5], q[4]), q[3]), q[2]), q[1]), q[0]);
+    d1 = fma(s, fma(s, fma(s, fma(s, 5.0 * q[5], 4.0 * q[4]), 3.0 * q[3]), 2.0 * q[2]), q[1]);
+    d2 = fma(s, fma(s, fma(s, 20.0 * q[5], 12.0 * q[4]), 6.0 * q[3]), 2.0 * q[2]);
+}
+
+// l=0 power-law extrapolation written as Phi(log r) with its two log-r derivatives.
+__device__ __forceinline__ void mp_extrap_out(int MODE_, double p0, double d1, double d2,
+                                              double px, double py, double pz, double r2,
+                                              PointOut& o)
+{
+    const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
+    const double inv_r2 = 1.0 / r2;
+    o.phi = MP0 * p0;
+    if (MODE_ == AGB_MODE_GRAD || MODE_ == AGB_MODE_HESS) {
+        const double gg = MP0 * d1;
+        o.g[0] = gg * (px * inv_r2);
+        o.g[1] = gg * (py * inv_r2);
+        o.g[2] = gg * (pz * inv_r2);
+    }
+    if (MODE_ == AGB_MODE_HESS) {
+        const double A = MP0 * (d2 - d1) * inv_r2 * inv_r2;
+        const double B = MP0 * d1 * inv_r2;
+        hess_radial(A, B, px, py, pz, o.h);
+    }
+}
+
+template <int MODE, typename R>
+__device__ __forceinline__ void multipole_point(const DevComp& c, double px, double py,
+                                                double pz, PointOut& o)
+{
+    const double logr_min = c.p[0], dlogr = c.p[1], inv_dlogr = c.p[2], invPhi0 = c.p[3];
+    const double in_s = c.p[4], in_U = c.p[5], in_W = c.p[6];
+    const double out_s = c.p[7], out_U = c.p[8], out_W = c.p[9];
+    const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
+
+    const double r2 = px * px + py * py + pz * pz;
+    const double r = sqrt(r2);
+    const double Rc = sqrt(px * px + py * py);
+
+    if (r < 1.0e-300) {                          // origin: Phi = W, zero derivatives
+        o.phi = (MODE == AGB_MODE_DENS) ? 0.0 : MP0 * in_W;
+        o.g[0] = o.g[1] = o.g[2] = 0.0;
+        for (int p = 0; p < 6; ++p) o.h[p] = 0.0;
+        o.rho = 0.0;
+        return;
+    }
+    const double logr = log(r);
+
+    if (logr < logr_min) {                       // inner l=0 power law
+        const double dlr = logr - logr_min;
+        const double rs = (in_s != 0.0) ? exp(in_s * dlr) : 1.0;
+        const double p0 = in_U * rs + in_W;
+        const double d1 = in_U * in_s * rs;
+        const double d2 = in_U * in_s * in_s * rs;
+        if (MODE == AGB_MODE_DENS) {
+            o.rho = MP0 * ((d2 + d1) / (r * r)) * AGB_INV_4PIG;
+            return;
+        }
+        mp_extrap_out(MODE, p0, d1, d2, px, py, pz, r2, o);
+        return;
+    }
+    int k = (int)((logr - logr_min) * inv_dlogr);
+    if (k < 0) k = 0;
+    if (k >= c.n_int) {                          // outer l=0 power law
+        if (MODE == AGB_MODE_DENS) { o.rho = 0.0; return; }
+        const double dlr = logr - (logr_min + c.n_int * dlogr);
+        const double en = exp(-dlr);
+        const double es = exp(out_s * dlr);
+        const double p0 = out_W * en + out_U * es;
+        const double d1 = -out_W * en + out_s * out_U * es;
+        const double d2 = out_W * en + out_s * out_s * out_U * es;
+        mp_extrap_out(MODE, p0, d1, d2, px, py, pz, r2, o);
+        return;
+    }
+    double s = (logr - (logr_min + k * dlogr)) * inv_dlogr;
+    s = fmin(fmax(s, 0.0), 1.0);
+
+    const double inv_r = 1.0 / r;
+    const double cth = pz * inv_r;
+    const double sth = Rc * inv_r;
+    const double cph = (Rc > 1.0e-300) ? px / Rc : 1.0;
+    const double sph = (Rc > 1.0e-300) ? py / Rc : 0.0;
+
+    // monopole (FP64) and the log-scaling factor F(log r) with derivatives
+    double c0, c0s, c0ss;
+    mp_quintic0(c, k, s, c0, c0s, c0ss);
+    const double dc0 = c0s * inv_dlogr;
+    const double d2c0 = c0ss * inv_dlogr * inv_dlogr;
+    double F = 1.0, dF = 0.0, d2F = 0.0, mono, dmono, d2mono;
+    if (c.log_scaling) {
+        const double ex = exp(c0);
+        const double P0 = 1.0 / (invPhi0 - ex);
+        const double dPdX = P0 * P0 * ex;
+        F = P0;
+        dF = dPdX * dc0;
+        d2F = dPdX * (d2c0 + dc0 * dc0 * P0 * (invPhi0 + ex));
+        mono = MP0 * F; dmono = MP0 * dF; d2mono = MP0 * d2F;
+    } else {
+        mono = MP0 * c0; dmono = MP0 * dc0; d2mono = MP0 * d2c0;
+    }
+
+    MPSums t = {};
+    mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
+
+    const double Bp = t.B * inv_dlogr;
+    const double Dp = t.D * inv_dlogr * inv_dlogr;
+    o.phi = mono + F * t.A;
+    if (MODE == AGB_MODE_POT) return;
+
+    const double Pr = dmono + F * Bp + dF * t.A;
+    if (MODE == AGB_MODE_DENS) {
+        const double inv_r2 = inv_r * inv_r;
+        const double lap = (d2mono + dmono) * inv_r2
+            + (F * (Dp + Bp - t.L) + dF * (2.0 * Bp + t.A) + d2F * t.A) * inv_r2;
+        o.rho = lap * AGB_INV_4PIG;
+        return;
+    }
+    const double Pth = F * t.Th;
+    const double Pos = F * t.Pos;
+    const double inv_r2 = inv_r * inv_r;
+    o.g[0] = Pr * (px * inv_r2) + Pth * (cth * cph * inv_r) + Pos * (-sph * inv_r);
+    o.g[1] = Pr * (py * inv_r2) + Pth * (cth * sph * inv_r) + Pos * (cph * inv_r);
+    o.g[2] = Pr * (pz * inv_r2) + Pth * (-sth * inv_r);
+    if (MODE != AGB_MODE_HESS) return;
+
+    // second derivatives in (log r, theta, phi)
+    const double Prr = d2mono + F * Dp + 2.0 * dF * Bp + d2F * t.A;
+    const double Pthth = F * t.Thth;
+    const double Prth = F * (t.BTh * inv_dlogr) + dF * t.Th;
+    const double Pph = F * t.Ph;
+    const double Pphph = F * t.Phph;
+    const double Prph = F * (t.BPh * inv_dlogr) + dF * t.Ph;
+    const double Pthph = F * t.ThPh;
+
+    // first and second derivatives of (log r, theta, phi) w.r.t. x, y, z
+    const double inv_R = (Rc > 1.0e-300) ? 1.0 / Rc : 0.0;
+    const double X[3] = {px, py, pz};
+    const double dlr[3] = {px * inv_r2, py * inv_r2, pz * inv_r2};
+    const double dth[3] = {cth * cph * inv_r, cth * sph * inv_r, -sth * inv_r};
+    const double dph[3] = {-sph * inv_R, cph * inv_R, 0.0};
+    const double inv_r3 = inv_r2 * inv_r, inv_r4 = inv_r2 * inv_r2, inv_r5 = inv_r4 * inv_r;
+    const double inv_s = (sth > 1.0e-14) ? 1.0 / sth : 0.0;
+    const double cos3 = cth * inv_s * inv_s * inv_s;
+    // f = cos(theta) = z / r
+    const double df[3] = {-pz * px * inv_r3, -pz * py * inv_r3, inv_r - pz * pz * inv_r3};
+    double d2ph_xx = 0.0, d2ph_xy = 0.0, d2ph_yy = 0.0;
+    if (Rc > 1.0e-14) {
+        const double iR4 = inv_R * inv_R * inv_R * inv_R;
+        d2ph_xx = 2.0 * px * py * iR4;
+        d2ph_xy = (py * py - px * px) * iR4;
+        d2ph_yy = -2.0 * px * py * iR4;
+    }
+    #pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        const int i = hess_i(p), j = hess_j(p);
+        const double dij = (i == j) ? 1.0 : 0.0;
+        const double d2lr = dij * inv_r2 - 2.0 * X[i] * X[j] * inv_r4;
+        // d2 f / dx_i dx_j = -(delta_ij z + delta_iz x_j + delta_jz x_i)/r^3 + 3 z x_i x_j / r^5
+        const double d2f = -(dij * pz + (i == 2 ? X[j] : 0.0) + (j == 2 ? X[i] : 0.0)) * inv_r3
+                         + 3.0 * pz * X[i] * X[j] * inv_r5;
+        const double d2th = -d2f * inv_s - df[i] * df[j] * cos3;
+        double d2ph = 0.0;
+        if (p == 0) d2ph = d2ph_xx;
+        else if (p == 1) d2ph = d2ph_yy;
+        else if (p == 3) d2ph = d2ph_xy;
+        o.h[p] = Prr * dlr[i] * dlr[j]
+               + Prth * (dlr[i] * dth[j] + dlr[j] * dth[i])
+               + Prph * (dlr[i] * dph[j] + dlr[j] * dph[i])
+               + Pthth * dth[i] * dth[j]
+               + Pthph * (dth[i] * dph[j] + dth[j] * dph[i])
+               + Pphph * dph[i] * dph[j]
+               + Pr * d2lr + Pth * d2th + Pph * d2ph;
+    }
+}

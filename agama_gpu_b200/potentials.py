@@ -1,0 +1,574 @@
+"""GPU potential classes with the reference's Python API (gpu_potential.py).
+
+Every class exposes potential / force / density / forceDeriv / evalDeriv /
+eval with (N,3) or (3,) inputs and Agama units, the same as the reference's
+classes (gpu_potential.py:633-935, 1260-1918; _analytic_potentials.py:77-1165).
+
+Evaluation model: a potential is a tree (Composite, Evolving, Shifted, Scaled
+over Multipole, CylSpline and analytic leaves).  At call time the tree is
+flattened into "leaves" -- (component, sigma, gamma, ampl) with
+Phi(x) = sum ampl * Phi_component(sigma * x - gamma) -- and the whole sum is
+evaluated by ONE fused CUDA kernel (libagb.so, agb_eval).  The reference
+instead launches one kernel per component and glues the results with CuPy
+elementwise passes (shift, scale, negate, lerp, add).
+
+Inputs may be torch tensors (CUDA or CPU), NumPy arrays or any DLPack /
+CUDA-array-interface object; host inputs are copied to the GPU first, as the
+reference's ``cp.asarray`` does.  Outputs are torch CUDA float64 tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import tempfile
+import uuid
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+import torch
+from scipy.interpolate import CubicHermiteSpline, CubicSpline
+
+from . import _lib
+from .coefs import read_coefs
+from .prep_cylspline import build_cylspline_tables
+from .prep_multipole import build_multipole_tables
+
+G_AGAMA = 4.30091727067736e-06                    # kpc (km/s)^2 / Msol
+INV_4PIG = 1.0 / (4.0 * math.pi * G_AGAMA)
+
+_PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_default_precision = os.environ.get("AGB_PRECISION", "fp64")
+
+
+def set_default_precision(precision: str) -> None:
+    """'fp64' (default) or 'mixed' for every potential without its own setting."""
+    global _default_precision
+    if precision not in _PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}, got {precision!r}")
+    _default_precision = precision
+
+
+# ---------------------------------------------------------------------------
+# inputs / outputs
+# ---------------------------------------------------------------------------
+
+def _cuda_device(dev: Optional[torch.device] = None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("agama_gpu_b200 needs a CUDA device (there is no CPU fallback)")
+    if dev is not None and dev.type == "cuda":
+        return dev
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _as_tensor(xyz) -> torch.Tensor:
+    if isinstance(xyz, torch.Tensor):
+        return xyz
+    if isinstance(xyz, np.ndarray):
+        return torch.from_numpy(np.ascontiguousarray(xyz, dtype=np.float64))
+    if hasattr(xyz, "__dlpack__"):
+        try:
+            return torch.from_dlpack(xyz)
+        except Exception:   # pragma: no cover - exotic producers
+            pass
+    if hasattr(xyz, "__cuda_array_interface__"):
+        return torch.as_tensor(xyz, device="cuda")
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(xyz, dtype=np.float64)))
+
+
+def prep_xyz(xyz) -> Tuple[torch.Tensor, bool]:
+    """(N,3) float64 contiguous CUDA tensor and whether the input was a single point.
+
+    Shape rules and messages follow gpu_potential.py:167-177.
+    """
+    t = _as_tensor(xyz)
+    dev = _cuda_device(t.device)
+    t = t.to(device=dev, dtype=torch.float64)
+    if t.dim() == 1:
+        if t.shape[0] != 3:
+            raise ValueError(f"Single-point xyz must have shape (3,), got {tuple(t.shape)}")
+        return t.reshape(1, 3).contiguous(), True
+    if t.dim() != 2 or t.shape[1] != 3:
+        raise ValueError(f"xyz must have shape (N,3), got {tuple(t.shape)}")
+    return t.contiguous(), False
+
+
+def _sq(a: torch.Tensor, single: bool):
+    return a[0] if single else a
+
+
+# ---------------------------------------------------------------------------
+# base class
+# ---------------------------------------------------------------------------
+
+Leaf = Tuple["_Component", float, np.ndarray, float]
+
+
+class _GPUPotBase:
+    """``+`` composition, the evaluation API and the flattening into leaves.
+
+    ``pot_a + pot_b`` -> CompositePotentialGPU (flattening nested composites),
+    ``sum([...])`` works through ``__radd__(0)`` (gpu_potential.py:85-101).
+    """
+
+    precision: Optional[str] = None
+
+    def __add__(self, other):
+        a = self._components if isinstance(self, CompositePotentialGPU) else [self]
+        b = other._components if isinstance(other, CompositePotentialGPU) else [other]
+        return CompositePotentialGPU(a + b)
+
+    def __radd__(self, other):
+        if other == 0:
+            return self
+        return NotImplemented
+
+    # subclasses implement: leaves at time t
+    def _leaves(self, t: float) -> List[Leaf]:
+        raise NotImplementedError
+
+    def set_precision(self, precision: Optional[str]):
+        """Per-object arithmetic of the Multipole sums: 'fp64', 'mixed' or None (default)."""
+        if precision is not None and precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        self.precision = precision
+        return self
+
+    # -- evaluation core ----------------------------------------------------
+    def _launch(self, arr: torch.Tensor, t: float, mode: int, want_phi: bool,
+                precision: Optional[str] = None, out=None):
+        n = arr.shape[0]
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        leaves = self._leaves(float(t))
+        if not leaves:
+            raise ValueError("potential has no components")
+        if len(leaves) > _lib.MAX_LEAVES:
+            raise ValueError(f"{len(leaves)} leaf components exceed the fused kernel's "
+                             f"limit of {_lib.MAX_LEAVES}")
+        comps: List[_lib.AgbComponent] = []
+        index = {}
+        leaf_arr = (_lib.AgbLeaf * len(leaves))()
+        for i, (c, sigma, gamma, ampl) in enumerate(leaves):
+            key = id(c)
+            if key not in index:
+                index[key] = len(comps)
+                comps.append(c._device_component(dev))
+            lf = leaf_arr[i]
+            lf.comp = index[key]
+            lf.sigma = sigma
+            lf.gamma[0], lf.gamma[1], lf.gamma[2] = float(gamma[0]), float(gamma[1]), float(gamma[2])
+            lf.ampl = ampl
+        comp_arr = (_lib.AgbComponent * len(comps))(*comps)
+        f64 = dict(dtype=torch.float64, device=dev)
+        phi = grad = hess = rho = None
+        if out is not None:
+            phi, grad, hess, rho = out
+        else:
+            if mode == _lib.MODE_DENS:
+                rho = torch.empty(n, **f64)
+            else:
+                if want_phi or mode == _lib.MODE_POT:
+                    phi = torch.empty(n, **f64)
+                if mode in (_lib.MODE_GRAD, _lib.MODE_HESS):
+                    grad = torch.empty((n, 3), **f64)
+                if mode == _lib.MODE_HESS:
+                    hess = torch.empty((n, 6), **f64)
+        if n == 0:
+            return phi, grad, hess, rho
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = _lib.lib.agb_eval(comp_arr, len(comps), leaf_arr, len(leaves), arr.data_ptr(), n,
+                               mode, prec, ptr(phi), ptr(grad), ptr(hess), ptr(rho),
+                               _lib.OUT_NEGATE, ctypes.c_void_p(stream))
+        _lib.check(rc, "agb_eval")
+        return phi, grad, hess, rho
+
+    # -- public API (gpu_potential.py:826-935) --------------------------------
+    def potential(self, xyz, t: float = 0.0):
+        """Phi in (km/s)^2: (N,) or a 0-d tensor for one point."""
+        arr, single = prep_xyz(xyz)
+        phi, _, _, _ = self._launch(arr, t, _lib.MODE_POT, True)
+        return _sq(phi, single)
+
+    def force(self, xyz, t: float = 0.0):
+        """F = -grad Phi in (km/s)^2/kpc: (N,3) or (3,)."""
+        arr, single = prep_xyz(xyz)
+        _, f, _, _ = self._launch(arr, t, _lib.MODE_GRAD, False)
+        return _sq(f, single)
+
+    def density(self, xyz, t: float = 0.0):
+        """rho = Laplacian(Phi)/(4 pi G) in Msol/kpc^3: (N,) or 0-d."""
+        arr, single = prep_xyz(xyz)
+        _, _, _, rho = self._launch(arr, t, _lib.MODE_DENS, False)
+        return _sq(rho, single)
+
+    def forceDeriv(self, xyz, t: float = 0.0):
+        """(force (N,3), deriv (N,6)); deriv = [dFx/dx, dFy/dy, dFz/dz, dFx/dy, dFy/dz, dFz/dx]."""
+        arr, single = prep_xyz(xyz)
+        _, f, d, _ = self._launch(arr, t, _lib.MODE_HESS, False)
+        return _sq(f, single), _sq(d, single)
+
+    def evalDeriv(self, xyz, t: float = 0.0):
+        """(Phi, force, deriv) from one kernel launch."""
+        arr, single = prep_xyz(xyz)
+        p, f, d, _ = self._launch(arr, t, _lib.MODE_HESS, True)
+        return _sq(p, single), _sq(f, single), _sq(d, single)
+
+    def eval(self, xyz, pot: bool = False, acc: bool = False, der: bool = False, t: float = 0.0):
+        """Any subset of (Phi, force, deriv) in that order; one array if one is asked for."""
+        if not (pot or acc or der):
+            raise ValueError("eval(): at least one of pot, acc, der must be True.")
+        arr, single = prep_xyz(xyz)
+        mode = _lib.MODE_HESS if der else (_lib.MODE_GRAD if acc else _lib.MODE_POT)
+        p, f, d, _ = self._launch(arr, t, mode, pot)
+        res = []
+        if pot:
+            res.append(_sq(p, single))
+        if acc:
+            res.append(_sq(f, single))
+        if der:
+            res.append(_sq(d, single))
+        return res[0] if len(res) == 1 else tuple(res)
+
+
+class _Component(_GPUPotBase):
+    """A leaf: one component with device tables."""
+
+    kind: int = 0
+
+    def _leaves(self, t: float) -> List[Leaf]:
+        return [(self, 1.0, np.zeros(3), 1.0)]
+
+    def _params(self) -> Sequence[float]:
+        return []
+
+    def _device_component(self, dev: torch.device) -> _lib.AgbComponent:
+        cache = self.__dict__.setdefault("_dev_cache", {})
+        hit = cache.get(dev)
+        if hit is None:
+            hit = self._upload(dev)
+            cache[dev] = hit
+        return hit[0]
+
+    def _upload(self, dev: torch.device):
+        c = _lib.AgbComponent()
+        c.kind = self.kind
+        for i, v in enumerate(self._params()):
+            c.p[i] = float(v)
+        return c, ()
+
+
+# ---------------------------------------------------------------------------
+# Multipole
+# ---------------------------------------------------------------------------
+
+class MultipolePotentialGPU(_Component):
+    """Agama Multipole BFE: quintic C2 splines in log r with log-scaling.
+
+    Same constructor as the reference (gpu_potential.py:654):
+    ``MultipolePotentialGPU(coefs, prune_threshold=1e-16)`` with a coefficient
+    object carrying R_grid, phi, dphi_dr, lm_labels (``read_coefs`` output).
+    """
+
+    kind = _lib.KIND_MULTIPOLE
+
+    def __init__(self, coefs, prune_threshold: float = 1e-16) -> None:
+        self.tables = build_multipole_tables(coefs, prune_threshold=prune_threshold)
+        t = self.tables
+        self._poly_im = t.interval_major()
+        self._poly32 = t.interval_major_f32()
+        self._lm = t.lm_packed()
+
+    @classmethod
+    def from_file(cls, path: Union[str, Path], **kw) -> "MultipolePotentialGPU":
+        """Load from an Agama .coef_mul_DR file (or the text of one section)."""
+        return cls(read_coefs(path if isinstance(path, Path) else str(path)), **kw)
+
+    @classmethod
+    def from_agama(cls, pot, **kw) -> "MultipolePotentialGPU":
+        """Build from an agama.Potential by exporting its coefficients (needs agama)."""
+        shm = "/dev/shm"
+        tmp_dir = shm if (os.path.isdir(shm) and os.access(shm, os.W_OK)) else tempfile.gettempdir()
+        tmp = os.path.join(tmp_dir, f"agama_gpu_{uuid.uuid4().hex}.coef")
+        try:
+            pot.export(tmp)
+            with open(tmp) as f:
+                head = f.read(512)
+            if "Coefficients" not in head:
+                raise ValueError(
+                    "from_agama(): the potential does not export expansion coefficients.\n"
+                    "Agama analytic types (NFW, Plummer, Dehnen, ...) do not store their\n"
+                    "parameters on export.  Construct the GPU class directly instead.")
+            return cls.from_file(tmp, **kw)
+        finally:
+            try:
+                os.unlink(tmp)
+            except FileNotFoundError:
+                pass
+
+    def _upload(self, dev):
+        t = self.tables
+        poly = torch.from_numpy(self._poly_im).to(dev)
+        poly32 = torch.from_numpy(self._poly32).to(dev)
+        lm = torch.from_numpy(self._lm).to(dev)
+        c = _lib.AgbComponent()
+        c.kind = self.kind
+        c.n_lm = t.n_lm
+        c.n_int = t.n_int
+        c.lmax = t.lmax
+        c.log_scaling = t.log_scaling
+        c.layout = _lib.LAYOUT_INTERVAL_MAJOR
+        c.table = poly.data_ptr()
+        c.table32 = poly32.data_ptr()
+        c.lm = lm.data_ptr()
+        for i, v in enumerate(t.scalars()):
+            c.p[i] = v
+        return c, (poly, poly32, lm)
+
+
+# ---------------------------------------------------------------------------
+# CylSpline
+# ---------------------------------------------------------------------------
+
+class CylSplinePotentialGPU(_Component):
+    """Agama CylSpline: per-harmonic bicubic Hermite splines in (asinh R, asinh z).
+
+    ``CylSplinePotentialGPU(coefs)`` as in gpu_potential.py:1281.  density()
+    returns -(Hxx+Hyy+Hzz)/(4 pi G) like the reference's wrapper
+    (gpu_potential.py:1389-1395), i.e. minus the Poisson density.
+    """
+
+    kind = _lib.KIND_CYLSPLINE
+
+    def __init__(self, coefs) -> None:
+        self.tables = build_cylspline_tables(coefs)
+        t = self.tables
+        self._cells = t.cell_major()
+        self._m = t.m_sorted()
+
+    @classmethod
+    def from_file(cls, path, **kw) -> "CylSplinePotentialGPU":
+        return cls(read_coefs(path if isinstance(path, Path) else str(path)), **kw)
+
+    def _upload(self, dev):
+        t = self.tables
+        cells = torch.from_numpy(self._cells).to(dev)
+        m = torch.from_numpy(self._m).to(dev)
+        lR = torch.from_numpy(np.ascontiguousarray(t.lR_grid)).to(dev)
+        lz = torch.from_numpy(np.ascontiguousarray(t.lz_grid)).to(dev)
+        W = torch.from_numpy(np.ascontiguousarray(t.W_outer)).to(dev)
+        c = _lib.AgbComponent()
+        c.kind = self.kind
+        c.n_lm = t.n_harm
+        c.n_int = len(t.lR_grid)
+        c.nz = len(t.lz_grid)
+        c.lmax = t.lmax_outer
+        c.log_scaling = t.log_scaling
+        c.layout = 1
+        c.table = cells.data_ptr()
+        c.lm = m.data_ptr()
+        c.grid_a = lR.data_ptr()
+        c.grid_b = lz.data_ptr()
+        c.extra = W.data_ptr()
+        c.p[0] = t.Rscale
+        c.p[1] = t.r0_outer
+        c.p[2] = float(t.mmax_outer)
+        return c, (cells, m, lR, lz, W)
+
+
+# ---------------------------------------------------------------------------
+# Composite / Evolving / Shifted / Scaled
+# ---------------------------------------------------------------------------
+
+class CompositePotentialGPU(_GPUPotBase):
+    """Sum of GPU potentials (gpu_potential.py:1439-1529), evaluated in one launch."""
+
+    def __init__(self, components: list) -> None:
+        if not components:
+            raise ValueError("CompositePotentialGPU requires at least one component.")
+        self._components = list(components)
+
+    def __repr__(self):
+        return f"CompositePotentialGPU({len(self._components)} components)"
+
+    @classmethod
+    def from_agama(cls, pot) -> "CompositePotentialGPU":
+        return cls([MultipolePotentialGPU.from_agama(pot)])
+
+    def _leaves(self, t: float) -> List[Leaf]:
+        out: List[Leaf] = []
+        for c in self._components:
+            out.extend(c._leaves(t))
+        return out
+
+
+class EvolvingPotentialGPU(_GPUPotBase):
+    """Snapshots at fixed times, linearly interpolated (or nearest) in time.
+
+    Semantics of gpu_potential.py:1536-1644: bracket [t_i, t_i+1] by binary
+    search, outputs = (1-alpha) * snapshot_i + alpha * snapshot_i+1; alpha 0/1
+    use one snapshot; ``interpolate=False`` or one snapshot -> nearest.
+    Both snapshots are summed inside the fused kernel.
+    """
+
+    def __init__(self, potentials: list, times, interpolate: bool = True) -> None:
+        if len(potentials) != len(times):
+            raise ValueError(f"len(potentials)={len(potentials)} != len(times)={len(times)}")
+        if len(potentials) < 1:
+            raise ValueError("Need at least one snapshot.")
+        self._pots = list(potentials)
+        self._times = np.asarray(times, dtype=np.float64)
+        self._interpolate = interpolate
+
+    def _bracket(self, t: float):
+        times = self._times
+        n = len(times)
+        if t <= times[0] or n == 1:
+            return 0, 0.0
+        if t >= times[-1]:
+            return n - 2, 1.0
+        lo, hi = 0, n - 2
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if times[mid + 1] <= t:
+                lo = mid + 1
+            else:
+                hi = mid
+        return lo, float((t - times[lo]) / (times[lo + 1] - times[lo]))
+
+    def _weights(self, t: float):
+        """[(snapshot index, weight)] used at time t."""
+        if len(self._pots) == 1 or not self._interpolate:
+            return [(int(np.argmin(np.abs(self._times - t))), 1.0)]
+        i, a = self._bracket(t)
+        if a == 0.0:
+            return [(i, 1.0)]
+        if a == 1.0:
+            return [(i + 1, 1.0)]
+        return [(i, 1.0 - a), (i + 1, a)]
+
+    def _leaves(self, t: float) -> List[Leaf]:
+        out: List[Leaf] = []
+        for i, w in self._weights(t):
+            for c, s, g, a in self._pots[i]._leaves(t):
+                out.append((c, s, g, a * w))
+        return out
+
+
+class ShiftedPotentialGPU(_GPUPotBase):
+    """``inner`` evaluated at x - center(t) (gpu_potential.py:1651-1764).
+
+    center: (3,) static; (T,4) rows [t, x, y, z] -> not-a-knot cubic spline;
+    (T,>=7) rows [t, x, y, z, vx, vy, vz] -> cubic Hermite.  Outside the time
+    range the centre is extrapolated linearly from the end value and slope.
+    """
+
+    def __init__(self, inner, center) -> None:
+        self._inner = inner
+        center = np.asarray(center, dtype=np.float64)
+        if center.ndim == 1 and center.shape == (3,):
+            self._is_static = True
+            self._center_static = center
+        elif center.ndim == 2 and center.shape[1] >= 4:
+            self._is_static = False
+            if not np.all(center[1:, 0] > center[:-1, 0]):
+                center = center[center[:, 0].argsort()]
+            self._times = center[:, 0]
+            pos = center[:, 1:4]
+            if center.shape[1] >= 7:
+                self._spline = CubicHermiteSpline(self._times, pos, center[:, 4:7])
+            else:
+                self._spline = CubicSpline(self._times, pos, bc_type="not-a-knot")
+            self._t0, self._tN = self._times[0], self._times[-1]
+            self._pos0, self._posN = self._spline(self._t0), self._spline(self._tN)
+            self._vel0, self._velN = self._spline(self._t0, 1), self._spline(self._tN, 1)
+        else:
+            raise ValueError("Center must be (3,) or (T, 4) or (T, 7).")
+
+    def _center_at(self, t: float) -> np.ndarray:
+        if self._is_static:
+            return self._center_static
+        if t < self._t0:
+            return self._pos0 + self._vel0 * (t - self._t0)
+        if t > self._tN:
+            return self._posN + self._velN * (t - self._tN)
+        return self._spline(t)
+
+    def _leaves(self, t: float) -> List[Leaf]:
+        c = np.asarray(self._center_at(t), dtype=np.float64)
+        return [(comp, s, g + s * c, a) for comp, s, g, a in self._inner._leaves(t)]
+
+
+class ScaledPotentialGPU(_GPUPotBase):
+    """Phi_s(x,t) = a(t) s(t) Phi(x s(t)), s = 1/scale(t) (gpu_potential.py:1767-1918).
+
+    scale: float; (T,2) rows [t, scale]; (T,3) rows [t, ampl, scale]; cubic
+    not-a-knot splines with linear extrapolation.  Force scales by a s^2,
+    Hessian and density by a s^3.
+    """
+
+    def __init__(self, inner, scale, ampl: float = 1.0) -> None:
+        self._inner = inner
+        if isinstance(scale, (int, float)):
+            arr = None
+        else:
+            arr = np.asarray(scale, dtype=np.float64)
+            if arr.ndim == 0:
+                arr = None
+        if arr is None:
+            self._is_static = True
+            self._scale_val = float(scale)
+            self._ampl_val = float(ampl)
+            return
+        if arr.ndim != 2 or arr.shape[1] not in (2, 3):
+            raise ValueError("scale must be a float, (T,2) array [t, scale(t)], "
+                             "or (T,3) array [t, ampl(t), scale(t)]. "
+                             f"Got shape {arr.shape}.")
+        times = arr[:, 0]
+        if not np.all(times[1:] > times[:-1]):
+            arr = arr[np.argsort(times)]
+            times = arr[:, 0]
+        self._is_static = False
+        self._times = times
+        self._t0, self._tN = float(times[0]), float(times[-1])
+        self._scale_spl = CubicSpline(times, arr[:, -1], bc_type="not-a-knot")
+        self._scale0 = float(self._scale_spl(self._t0))
+        self._scaleN = float(self._scale_spl(self._tN))
+        self._dscale0 = float(self._scale_spl(self._t0, 1))
+        self._dscaleN = float(self._scale_spl(self._tN, 1))
+        if arr.shape[1] == 3:
+            self._ampl_spl = CubicSpline(times, arr[:, 1], bc_type="not-a-knot")
+            self._ampl0 = float(self._ampl_spl(self._t0))
+            self._amplN = float(self._ampl_spl(self._tN))
+            self._dampl0 = float(self._ampl_spl(self._t0, 1))
+            self._damplN = float(self._ampl_spl(self._tN, 1))
+        else:
+            self._ampl_spl = None
+        self._ampl_val = float(ampl)
+
+    def _sa(self, t: float):
+        """(s, a) = (1/scale(t), ampl(t))."""
+        if self._is_static:
+            return 1.0 / self._scale_val, self._ampl_val
+        if t < self._t0:
+            sc = self._scale0 + self._dscale0 * (t - self._t0)
+        elif t > self._tN:
+            sc = self._scaleN + self._dscaleN * (t - self._tN)
+        else:
+            sc = float(self._scale_spl(t))
+        s = 1.0 / sc
+        if self._ampl_spl is None:
+            a = self._ampl_val
+        elif t < self._t0:
+            a = self._ampl0 + self._dampl0 * (t - self._t0)
+        elif t > self._tN:
+            a = self._amplN + self._damplN * (t - self._tN)
+        else:
+            a = float(self._ampl_spl(t))
+        return s, a
+
+    def _leaves(self, t: float) -> List[Leaf]:
+        s, a = self._sa(t)
+        return [(comp, sg * s, g, a * s * amp) for comp, sg, g, amp in self._inner._leaves(t)]

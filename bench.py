@@ -1,0 +1,343 @@
+"""Benchmark: force+Phi points/s of the fused evaluator on the time-dependent
+composite (Multipole lmax=32 x 100 nodes + MiyamotoNagai + DiskAnsatz + NFW
+Shifted on a (1000,4) track + Evolving over 16 lmax=16 snapshots) at N=4M
+isotropic Hernquist (a=10 kpc) points per GPU, mixed precision (headline) and
+plain FP64 side by side.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one potential+force evaluation of all N points at one time t (t
+varies per step inside the track and the snapshot range).  Inputs are
+resident in HBM for `value`; `e2e` goes through the public API from pinned
+host memory and reads the results back.  L2 is flushed (256 MiB write)
+between timed steps.  Under torchrun every rank evaluates its own N points
+(weak scaling, no data-path collective); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "force+Phi pts/s (mixed-precision fused kernel; FP64 kernel alongside)"
+WORKLOAD = ("time-dependent composite: Multipole lmax=32 x 100 nodes + MiyamotoNagai + "
+            "DiskAnsatz + Shifted NFW on (1000,4) track + Evolving 16 x lmax=16 snapshots; "
+            "isotropic Hernquist a=10 kpc points")
+G = 4.30091727067736e-06
+
+
+def step_times(k_total: int):
+    """Evaluation times inside the centre track (0..2) and the snapshots (0..1.5)."""
+    return [0.05 + 1.4 * ((0.6180339887 * (k + 1)) % 1.0) for k in range(k_total)]
+
+
+def flops_per_step(pot, xyz: np.ndarray, t: float) -> tuple:
+    """Algorithmic FLOPs of one Phi+F evaluation (convention of DESIGN.md):
+    Multipole 48*n_harm + 64 per point inside its grid (64 outside), analytic 30
+    per component.  Returns (fp32-eligible harmonic flops, fp64 flops)."""
+    from agama_gpu_b200 import _lib as L
+    f_harm = 0.0
+    f_point = 0.0
+    for comp, sigma, gamma, ampl in pot._leaves(t):
+        if comp.kind == L.KIND_MULTIPOLE:
+            tb = comp.tables
+            x = sigma * xyz - np.asarray(gamma)[None, :]
+            lr = np.log(np.maximum(np.linalg.norm(x, axis=1), 1e-300))
+            inside = np.count_nonzero((lr >= tb.logr_min) & (lr < tb.logr_min + tb.n_int * tb.dlogr))
+            f_harm += 48.0 * tb.n_lm * inside
+            f_point += 64.0 * len(xyz)
+        elif comp.kind == L.KIND_CYLSPLINE:
+            f_harm += 110.0 * comp.tables.n_harm * len(xyz)
+            f_point += 80.0 * len(xyz)
+        else:
+            f_point += 30.0 * len(xyz)
+    return f_harm, f_point
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+        return False
+
+    def summary(self):
+        if self.proc is None or not getattr(self, "out", ""):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the path, timed on the host cores."""
+    from agama_gpu_b200.synthetic import build_composite, composite_spec, hernquist_points
+    from oracle import cpu
+    spec = composite_spec()
+    pot = build_composite(spec)
+    n_sample = args.cpu_sample
+    xyz = hernquist_points(n_sample, 10.0, 12345)
+    threads = os.cpu_count() or 1
+    kind = "reference" if cpu.ref_available() else "port"
+    ts = step_times(args.warmup + args.steps)
+    for k in range(args.warmup):
+        cpu.eval_potential_reference(pot, 1, xyz, ts[k], threads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        cpu.eval_potential_reference(pot, 1, xyz, ts[args.warmup + k], threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = n_sample / dt
+    sample = (f"{n_sample} Hernquist points per step, Phi+F of the full composite; expansions "
+              f"by the reference's kernels compiled for the host (OpenMP), analytic terms restated")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pts/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "n_points": n_sample, "device": "host CPU"},
+            "cpu_baseline": {"value": value, "unit": "pts/s", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "pts/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def cpu_baseline_leg(pot, xyz: np.ndarray, t: float, n_sample: int):
+    from oracle import cpu
+    threads = os.cpu_count() or 1
+    sub = xyz[:n_sample]
+    cpu.eval_potential_reference(pot, 1, sub[:1000], t, threads)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cpu.eval_potential_reference(pot, 1, sub, t, threads)
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": n_sample / dt, "unit": "pts/s", "cores": threads,
+            "kind": "reference" if cpu.ref_available() else "port",
+            "sample": f"{n_sample} of the step's points, Phi+F, median of {reps} after a warm-up"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4_000_000, help="points per GPU")
+    ap.add_argument("--cpu-sample", type=int, default=100_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    from agama_gpu_b200.synthetic import build_composite, composite_spec, hernquist_points
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        tt = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    spec = composite_spec()
+    pot = build_composite(spec)
+    N = args.n
+    xyz_np = hernquist_points(N, 10.0, 1000 + rank)
+    xyz_host = torch.from_numpy(xyz_np).pin_memory()
+    xyz = xyz_host.to(dev)
+    phi = torch.empty(N, dtype=torch.float64, device=dev)
+    frc = torch.empty((N, 3), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ts = step_times(args.warmup + args.steps)
+    stream = torch.cuda.current_stream(dev)
+
+    def device_step(t, prec):
+        pot._launch(xyz, t, _lib.MODE_GRAD, True, precision=prec, out=(phi, frc, None, None))
+
+    def timed(prec):
+        for k in range(args.warmup):
+            device_step(ts[k], prec)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        _lib.launch_count_reset()
+        tot = 0.0
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            device_step(ts[args.warmup + k], prec)
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        launches = _lib.launch_count()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(tot / args.steps), launches
+
+    with ClockSampler(local) as clk:
+        ms64, l64 = timed("fp64")
+        ms32, l32 = timed("mixed")
+    clocks = clk.summary()
+
+    # accuracy of the mixed kernel against the FP64 kernel at one step's time
+    t_chk = ts[-1]
+    device_step(t_chk, "fp64")
+    f64 = frc.clone()
+    p64 = phi.clone()
+    device_step(t_chk, "mixed")
+    err_f = float((frc - f64).abs().max() / f64.abs().max())
+    err_p = float((phi - p64).abs().max() / p64.abs().max())
+
+    # end to end through the public API from pinned host memory
+    pot.set_precision("mixed")
+    phi_h = torch.empty(N, dtype=torch.float64).pin_memory()
+    frc_h = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+    for k in range(2):
+        pp, ff = pot.eval(xyz_host, pot=True, acc=True, t=ts[k])
+    torch.cuda.synchronize()
+    barrier()
+    e_tot = 0.0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pp, ff = pot.eval(xyz_host, pot=True, acc=True, t=ts[args.warmup + k])
+        phi_h.copy_(pp, non_blocking=True)
+        frc_h.copy_(ff, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e_tot += e0.elapsed_time(e1)
+    e2e_ms = max_over_ranks(e_tot / args.steps)
+    pot.set_precision(None)
+
+    # roofline of the dominant (only) kernel
+    pk64 = ctypes_peak(_lib, 0)
+    pk32 = ctypes_peak(_lib, 1)
+    fh, fp = flops_per_step(pot, xyz_np, t_chk)
+    t_roof_mixed = fh / (pk32 * 1e12) + fp / (pk64 * 1e12)
+    t_roof_fp64 = (fh + fp) / (pk64 * 1e12)
+    achieved32 = (fh + fp) / (ms32 * 1e-3) / 1e12
+    achieved64 = (fh + fp) / (ms64 * 1e-3) / 1e12
+    eff_peak32 = (fh + fp) / t_roof_mixed / 1e12
+
+    value = world * N / (ms32 * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "points_per_gpu": N, "precision": "mixed",
+                   "l2": "flushed (256 MiB write) between timed steps",
+                   "parallelism": f"points sharded, {world} rank(s), no data-path collective"},
+        "fp64": {"value": world * N / (ms64 * 1e-3), "unit": "pts/s", "ms_per_step": ms64},
+        "speedup_mixed_vs_fp64": ms64 / ms32,
+        "mixed_vs_fp64_error": {"force_max_rel": err_f, "phi_max_rel": err_p, "gate": 1e-6},
+        "adjoint_over_forward": None,
+        "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
+                "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": int(l32),
+        "roofline": {
+            "bound": "fp32+fp64 pipes (mixed); fp64 pipe (plain)", "unit": "TFLOP/s",
+            "achieved": achieved32, "peak": eff_peak32, "frac": achieved32 / eff_peak32,
+            "traffic": None,
+            "fp64_kernel": {"achieved": achieved64, "peak": pk64, "frac": achieved64 / pk64},
+            "flops_per_step": fh + fp, "fp32_eligible_flops": fh,
+            "peak_source": f"measured live: FMA-chain kernel, fp64 {pk64:.1f} / fp32 {pk32:.1f} TFLOP/s",
+            "hbm": {"bytes_per_step": N * (24 + 32), "achieved_gbs": N * 56 / (ms32 * 1e-3) / 1e9},
+        },
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_leg(pot, xyz_np, t_chk, args.cpu_sample)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def ctypes_peak(_lib, prec: int) -> float:
+    import ctypes
+    import torch
+    v = ctypes.c_double(0.0)
+    rc = _lib.lib.agb_measure_fma_peak(prec, ctypes.byref(v),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _lib.check(rc, "agb_measure_fma_peak")
+    return float(v.value)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,224 @@
+/*
+ * agb.h -- C ABI of the B200 evaluator for Agama-style galactic potentials.
+ *
+ * Plain C: device pointers, host pointers to small descriptor structs, sizes
+ * and a CUDA stream passed as void*.  No torch or CuPy types.  Every function
+ * returns 0 on success or a negative AGB_ERR_* code; agb_last_error() gives
+ * a thread-local message for the last failure on the calling thread.
+ *
+ * Two families of entry points:
+ *
+ *  1. Kernel-signature entries (agb_multipole_*, agb_cylspl_*): one per
+ *     reference kernel, same arguments in the same order and with the same
+ *     meaning, plus a trailing stream.  They replace the CuPy RawKernel
+ *     launches of the reference's wrapper one for one.  Outputs keep the
+ *     reference's convention (gradient and Hessian of Phi, not force).
+ *
+ *  2. The fused entry agb_eval(): any composite of Multipole, CylSpline and
+ *     analytic components, each seen through a Shifted/Scaled/Evolving
+ *     transform ("leaf"), summed per point in one kernel launch.  This is what
+ *     the Python PotentialGPU classes call.  It replaces the per-component
+ *     launches plus CuPy elementwise glue of CompositePotentialGPU
+ *     (gpu_potential.py:1439-1529), EvolvingPotentialGPU (:1536-1644),
+ *     ShiftedPotentialGPU (:1651-1764) and ScaledPotentialGPU (:1767-1918).
+ *
+ * All positions, tables and outputs are FP64 and live in device memory unless
+ * stated otherwise; the caller owns every buffer.
+ */
+#ifndef AGB_H
+#define AGB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AGB_OK               0
+#define AGB_ERR_ARG         -1   /* bad argument (null pointer, size, kind)  */
+#define AGB_ERR_DEVICE      -2   /* CUDA error reported by the runtime       */
+#define AGB_ERR_UNSUPPORTED -3   /* valid request this build cannot serve    */
+#define AGB_ERR_TIMEOUT     -4   /* a bounded device wait gave up            */
+
+/* evaluation modes */
+#define AGB_MODE_POT   0   /* Phi                                     */
+#define AGB_MODE_GRAD  1   /* Phi and grad Phi                        */
+#define AGB_MODE_HESS  2   /* Phi, grad Phi and the Hessian           */
+#define AGB_MODE_DENS  3   /* density = Laplacian(Phi) / (4 pi G)     */
+
+/* arithmetic of the Multipole harmonic sums */
+#define AGB_PREC_FP64  0   /* everything FP64                                      */
+#define AGB_PREC_MIXED 1   /* FP32 Legendre/m-phi recurrences and spline polynomials,
+                              FP64 for log r, interval index/offset, monopole,
+                              extrapolation, per-|m| partial sums and the
+                              composite sum                                       */
+
+/* output flags for agb_eval */
+#define AGB_OUT_NEGATE 1   /* write -grad (force) and -Hessian (forceDeriv layout) */
+
+/* component kinds */
+#define AGB_KIND_MULTIPOLE      1
+#define AGB_KIND_CYLSPLINE      2
+#define AGB_KIND_NFW           10
+#define AGB_KIND_PLUMMER       11
+#define AGB_KIND_HERNQUIST     12
+#define AGB_KIND_DEHNEN        13
+#define AGB_KIND_ISOCHRONE     14
+#define AGB_KIND_MIYAMOTONAGAI 15
+#define AGB_KIND_LOGHALO       16
+#define AGB_KIND_DISKANSATZ    17
+#define AGB_KIND_UNIFORMACC    18
+
+/* Multipole table layouts (agb_component.layout) */
+#define AGB_LAYOUT_HARMONIC_MAJOR 0  /* poly[(c*n_int + k)*6 + j]: the reference's layout */
+#define AGB_LAYOUT_INTERVAL_MAJOR 1  /* poly[(k*n_lm + c)*6 + j]: one contiguous slab per
+                                        radial interval                                  */
+
+#define AGB_MAX_LEAVES 32
+#define AGB_MAX_COMPONENTS 24
+#define AGB_MAX_LMAX 32
+
+/*
+ * One potential component.  Static for the life of its tables.
+ *
+ * MULTIPOLE  (tables from the quintic-spline builder, gpu_potential.py:408-631)
+ *   table      FP64 poly, layout per `layout`
+ *   table32    FP32 copy of the same polynomials (needed for AGB_PREC_MIXED)
+ *   lm         packed harmonic list, lm[c] = (l << 16) | (m & 0xffff), sorted by
+ *              (|m|, l, cos before sin), lm[0] = (0,0)
+ *   n_lm, n_int, lmax, log_scaling, layout
+ *   p[0..9]    logr_min, dlogr, inv_dlogr, invPhi0, inner_s, inner_U, inner_W,
+ *              outer_s, outer_U, outer_W
+ * CYLSPLINE  (tables from gpu_potential.py:1143-1253, relaid per cell)
+ *   table      cell-major nodes: ((iR*(nz-1) + iz)*n_lm + h)*16 doubles:
+ *              {fval, fx, fy, fxy} at the (lo,lo), (lo,hi), (hi,lo), (hi,hi) corners
+ *   lm         m of each harmonic h
+ *   grid_a     lR grid [n_int], grid_b lz grid [nz], extra W_outer [(8+1)^2]
+ *   n_lm = n_harm, n_int = nR, nz, log_scaling, lmax = lmax_outer
+ *   p[0] Rscale, p[1] r0_outer, p[2] mmax_outer
+ * Analytic kinds: p[] holds the profile parameters (see the Python layer).
+ */
+typedef struct agb_component {
+    int32_t kind;
+    int32_t n_lm;
+    int32_t n_int;
+    int32_t nz;
+    int32_t lmax;
+    int32_t log_scaling;
+    int32_t layout;
+    int32_t reserved;
+    const double*  table;
+    const float*   table32;
+    const int32_t* lm;
+    const double*  grid_a;
+    const double*  grid_b;
+    const double*  extra;
+    double p[16];
+} agb_component;
+
+/*
+ * A component seen through the modifier chain at the evaluation time:
+ *   Phi(x) += ampl * Phi_comp(sigma * x - gamma)
+ *   grad   += ampl * sigma   * grad_comp
+ *   Hessian/density += ampl * sigma^2 * (...)_comp
+ * Shifted(c): sigma 1, gamma c.  Scaled(s=1/scale, a): sigma s, ampl a*s.
+ * Evolving: the two bracketing snapshots with ampl (1-alpha) and alpha.
+ */
+typedef struct agb_leaf {
+    int32_t comp;       /* index into the component array */
+    int32_t reserved;
+    double  sigma;
+    double  gamma[3];
+    double  ampl;
+} agb_leaf;
+
+/* ---- library ---- */
+/* Live FMA throughput of the current GPU in TFLOP/s (precision AGB_PREC_FP64 ->
+   FP64, AGB_PREC_MIXED -> FP32).  A measurement utility for roofline reports;
+   no counterpart in the reference. */
+int agb_measure_fma_peak(int precision, double* tflops, void* stream);
+
+const char* agb_last_error(void);
+const char* agb_version(void);
+/* number of kernel launches issued by this library on the calling thread since
+   the last reset (for launch accounting in benchmarks) */
+int64_t agb_launch_count(void);
+void    agb_launch_count_reset(void);
+
+/*
+ * Fused evaluation of a composite at N points.
+ *   xyz   device, N x 3 row-major (x, y, z per point)
+ *   phi   device [N]     (may be NULL in GRAD/HESS modes)
+ *   grad  device [N*3]   (GRAD/HESS; may be NULL in HESS mode)
+ *   hess  device [N*6]   [Hxx, Hyy, Hzz, Hxy, Hyz, Hxz] (HESS)
+ *   rho   device [N]     (DENS)
+ *   out_flags AGB_OUT_NEGATE: grad -> force, hess -> forceDeriv
+ * Replaces the per-component launch chains listed in the file comment.
+ */
+int agb_eval(const agb_component* comps, int n_comps,
+             const agb_leaf* leaves, int n_leaves,
+             const double* xyz, int64_t n, int mode, int precision,
+             double* phi, double* grad, double* hess, double* rho,
+             int out_flags, void* stream);
+
+/*
+ * Kernel-signature entries.  Arguments are those of the reference kernels, in
+ * order, with SoA x, y, z device arrays, the reference's harmonic-major poly
+ * layout and lm_l/lm_m arrays sorted as gpu_potential.py:516 sorts them.
+ *   agb_multipole_potential  replaces multipole_potential_kernel
+ *                            (_multipole_potential_kernel.cu:415-434)
+ *   agb_multipole_force      replaces multipole_force_kernel (:436-455)
+ *   agb_multipole_hess       replaces multipole_hess_kernel (:466-800)
+ *   agb_multipole_density    replaces multipole_density_kernel (:809-958)
+ */
+int agb_multipole_potential(const double* x, const double* y, const double* z,
+        const double* poly, double logr_min, double dlogr, double inv_dlogr,
+        int n_intervals, int n_lm, int lmax, const int* lm_l, const int* lm_m,
+        int log_scaling, double invPhi0, double inner_s, double inner_U, double inner_W,
+        double outer_s, double outer_U, double outer_W,
+        double* phi_out, double* grad_out, int N, void* stream);
+int agb_multipole_force(const double* x, const double* y, const double* z,
+        const double* poly, double logr_min, double dlogr, double inv_dlogr,
+        int n_intervals, int n_lm, int lmax, const int* lm_l, const int* lm_m,
+        int log_scaling, double invPhi0, double inner_s, double inner_U, double inner_W,
+        double outer_s, double outer_U, double outer_W,
+        double* phi_out, double* grad_out, int N, void* stream);
+int agb_multipole_hess(const double* x, const double* y, const double* z,
+        const double* poly, double logr_min, double dlogr, double inv_dlogr,
+        int n_intervals, int n_lm, int lmax, const int* lm_l, const int* lm_m,
+        int log_scaling, double invPhi0, double inner_s, double inner_U, double inner_W,
+        double outer_s, double outer_U, double outer_W,
+        double* phi_out, double* grad_out, double* hess_out, int N, void* stream);
+int agb_multipole_density(const double* x, const double* y, const double* z,
+        const double* poly, double logr_min, double dlogr, double inv_dlogr,
+        int n_intervals, int n_lm, int lmax, const int* lm_l, const int* lm_m,
+        int log_scaling, double invPhi0, double inner_s, double inner_U, double inner_W,
+        double outer_s, double outer_U, double outer_W, double inv_4piG,
+        double* rho_out, int N, void* stream);
+
+/*
+ *   agb_cylspl_potential  replaces cylspl_potential_kernel (_cylspl_potential_kernel.cu:871-899)
+ *   agb_cylspl_force      replaces cylspl_force_kernel (:902-935)
+ *   agb_cylspl_hess       replaces cylspl_hess_kernel (:938-972)
+ * node_arr is the reference's layout [(mm*nR + iR)*nz + iz][4].
+ */
+int agb_cylspl_potential(const double* x, const double* y, const double* z,
+        double Rscale, const double* lR_grid, int nR, const double* lz_grid, int nz,
+        const double* node_arr, int n_harm, const int* m_arr, int mmax, int log_scaling,
+        const double* W_outer, double r0_outer, int lmax_outer, int mmax_outer,
+        double* phi_out, int N, void* stream);
+int agb_cylspl_force(const double* x, const double* y, const double* z,
+        double Rscale, const double* lR_grid, int nR, const double* lz_grid, int nz,
+        const double* node_arr, int n_harm, const int* m_arr, int mmax, int log_scaling,
+        const double* W_outer, double r0_outer, int lmax_outer, int mmax_outer,
+        double* phi_out, double* grad_out, int N, void* stream);
+int agb_cylspl_hess(const double* x, const double* y, const double* z,
+        double Rscale, const double* lR_grid, int nR, const double* lz_grid, int nz,
+        const double* node_arr, int n_harm, const int* m_arr, int mmax, int log_scaling,
+        const double* W_outer, double r0_outer, int lmax_outer, int mmax_outer,
+        double* phi_out, double* grad_out, double* hess_out, int N, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AGB_H */

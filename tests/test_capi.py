@@ -1,0 +1,80 @@
+"""The C ABI library loads, exports every declared symbol, and its descriptor
+structs have the same layout in C and in the ctypes binding (no GPU needed)."""
+import ctypes
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "agb.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(agb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from agama_gpu_b200 import _lib
+    names = declared_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(_lib.lib, n), f"libagb.so does not export {n}"
+    assert set(_lib.EXPORTED) <= set(names)
+
+
+def test_version_and_error_strings():
+    from agama_gpu_b200 import _lib
+    assert b"sm_100a" in _lib.lib.agb_version()
+    assert isinstance(_lib.last_error(), str)
+
+
+def test_argument_errors_need_no_gpu():
+    """Invalid calls are rejected on the host before any CUDA call."""
+    from agama_gpu_b200 import _lib
+    rc = _lib.lib.agb_eval(None, 0, None, 0, None, 10, 1, 0, None, None, None, None, 0, None)
+    assert rc == -1 and "null" in _lib.last_error()
+    comps = (_lib.AgbComponent * 1)()
+    comps[0].kind = 99
+    leaves = (_lib.AgbLeaf * 1)()
+    rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
+                           ctypes.c_void_p(16), None, None, 0, None)
+    assert rc == -1 and "unknown component kind" in _lib.last_error()
+    leaves[0].comp = 3
+    rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
+                           ctypes.c_void_p(16), None, None, 0, None)
+    assert rc == -1 and "refers to component" in _lib.last_error()
+    assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, None, None, None, 0, None) == 0
+    # lmax beyond the kernel's limit
+    comps[0].kind = _lib.KIND_MULTIPOLE
+    comps[0].lmax = 40
+    comps[0].n_lm = comps[0].n_int = 1
+    comps[0].table = comps[0].lm = 16
+    leaves[0].comp = 0
+    rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
+                           ctypes.c_void_p(16), None, None, 0, None)
+    assert rc == -3 and "lmax" in _lib.last_error()
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_struct_layout_matches_header(tmp_path):
+    from agama_gpu_b200 import _lib
+    src = tmp_path / "lay.c"
+    src.write_text(f'''#include <stdio.h>
+#include <stddef.h>
+#include "{HEADER}"
+int main(void) {{
+  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(agb_component), offsetof(agb_component, table),
+         offsetof(agb_component, p), sizeof(agb_leaf), offsetof(agb_leaf, sigma),
+         offsetof(agb_leaf, gamma), offsetof(agb_leaf, ampl));
+  return 0; }}''')
+    exe = tmp_path / "lay"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
+    C, L = _lib.AgbComponent, _lib.AgbLeaf
+    assert got == [ctypes.sizeof(C), C.table.offset, C.p.offset, ctypes.sizeof(L),
+                   L.sigma.offset, L.gamma.offset, L.ampl.offset]
