@@ -15,6 +15,7 @@ AGB_OK = 0
 MODE_POT, MODE_GRAD, MODE_HESS, MODE_DENS = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 OUT_NEGATE = 1
+OUT_NO_BINNING = 2
 
 KIND_MULTIPOLE = 1
 KIND_CYLSPLINE = 2
@@ -31,6 +32,10 @@ KIND_UNIFORMACC = 18
 LAYOUT_HARMONIC_MAJOR = 0
 LAYOUT_INTERVAL_MAJOR = 1
 
+STRUCT_LIST = 0
+STRUCT_ALL = 1
+STRUCT_EVEN = 2
+
 MAX_LEAVES = 32
 MAX_COMPONENTS = 24
 
@@ -44,7 +49,7 @@ class AgbComponent(ctypes.Structure):
         ("lmax", ctypes.c_int32),
         ("log_scaling", ctypes.c_int32),
         ("layout", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("structure", ctypes.c_int32),
         ("table", ctypes.c_void_p),
         ("table32", ctypes.c_void_p),
         ("lm", ctypes.c_void_p),
@@ -69,7 +74,7 @@ def _load():
     if not LIB_PATH.exists():
         raise ImportError(
             f"{LIB_PATH} is missing: build the CUDA library with "
-            "`python -m agama_gpu_b200.build` (there is no CPU fallback)")
+            "`python agama_gpu_b200/build.py` (there is no CPU fallback)")
     lib = ctypes.CDLL(str(LIB_PATH))
     lib.agb_last_error.restype = ctypes.c_char_p
     lib.agb_version.restype = ctypes.c_char_p
@@ -80,6 +85,16 @@ def _load():
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_int, ctypes.c_void_p]
+    lib.agb_eval_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_eval_workspace_bytes.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_int64, ctypes.c_int]
+    lib.agb_eval_ws.restype = ctypes.c_int
+    lib.agb_eval_ws.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     return lib
 
 
@@ -88,6 +103,7 @@ lib = _load()
 # symbols the header declares (checked by tests/test_capi.py)
 EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
+    "agb_eval_ws", "agb_eval_workspace_bytes",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
     "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
 ]

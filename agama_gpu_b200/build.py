@@ -1,7 +1,9 @@
 """Build the in-tree CUDA library agama_gpu_b200/libagb.so for sm_100a.
 
-    python -m agama_gpu_b200.build            # compile if sources changed
-    python -m agama_gpu_b200.build --force    # always recompile
+    python agama_gpu_b200/build.py            # compile if sources changed
+    python agama_gpu_b200/build.py --force    # always recompile
+
+(Run it as a script: importing the package needs the library it builds.)
 
 nvcc cross-compiles without a GPU; the .so stays in the source tree so it is
 the one Python loads (no JIT cache).

@@ -19,6 +19,8 @@ struct DevComp {
     int log_scaling;
     int layout;        // Multipole: AGB_LAYOUT_*; CylSpline: 0 reference, 1 cell-major
     int lm_split;      // 1: harmonic list given as separate l[] and m[] arrays
+    int structure;     // Multipole: AGB_STRUCT_* (column structure of the table)
+    int pad_;
     const double*  table;
     const float*   table32;
     const int32_t* lm;     // packed (l<<16 | m&0xffff), or l[] when lm_split
@@ -43,7 +45,8 @@ struct EvalArgs {
     int out_flags;
     int soa;                 // 1: x, y, z separate arrays (kernel-signature entries)
     int pad;
-    const double* xyz;       // AoS N x 3 when !soa
+    const double* xyz;       // AoS N x 3 when !soa (sorted copy when perm != null)
+    const int* perm;         // binned order: point pos is input point perm[pos]
     const double* x;
     const double* y;
     const double* z;

@@ -15,6 +15,7 @@
 #include "multipole.cuh"
 #include "cylspline.cuh"
 #include "analytic.cuh"
+#include "bin.cuh"
 
 // ---------------------------------------------------------------------------
 // errors and launch accounting
@@ -69,17 +70,18 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 }
 
 template <int MODE, typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < a.n; pos += stride) {
         double x, y, z;
         if (a.soa) {
-            x = a.x[i]; y = a.y[i]; z = a.z[i];
+            x = a.x[pos]; y = a.y[pos]; z = a.z[pos];
         } else {
-            x = a.xyz[3 * i]; y = a.xyz[3 * i + 1]; z = a.xyz[3 * i + 2];
+            x = a.xyz[3 * pos]; y = a.xyz[3 * pos + 1]; z = a.xyz[3 * pos + 2];
         }
+        const long long i = a.perm ? (long long)a.perm[pos] : pos;
         double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
         double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int L = 0; L < a.n_leaves; ++L) {
@@ -171,6 +173,7 @@ static int comp_to_dev(const agb_component& s, DevComp& d, int precision)
     d.kind = s.kind;
     d.n_lm = s.n_lm; d.n_int = s.n_int; d.nz = s.nz; d.lmax = s.lmax;
     d.log_scaling = s.log_scaling; d.layout = s.layout; d.lm_split = 0;
+    d.structure = s.structure;
     d.table = s.table; d.table32 = s.table32; d.lm = s.lm; d.lm_m = nullptr;
     d.grid_a = s.grid_a; d.grid_b = s.grid_b; d.extra = s.extra;
     memcpy(d.p, s.p, sizeof(d.p));
@@ -181,6 +184,19 @@ static int comp_to_dev(const agb_component& s, DevComp& d, int precision)
             return set_err(AGB_ERR_UNSUPPORTED, "multipole lmax=%d exceeds %d", s.lmax, AGB_MAX_LMAX);
         if (!aligned16(s.table))
             return set_err(AGB_ERR_ARG, "multipole table must be 16-byte aligned");
+        if (s.structure < AGB_STRUCT_LIST || s.structure > AGB_STRUCT_EVEN)
+            return set_err(AGB_ERR_ARG, "multipole structure %d unknown", s.structure);
+        if (s.structure != AGB_STRUCT_LIST) {
+            if (s.layout != AGB_LAYOUT_INTERVAL_MAJOR)
+                return set_err(AGB_ERR_ARG, "regular multipole tables must be interval-major");
+            int cols = 0;
+            for (int m = 0; m <= s.lmax; ++m)
+                for (int l = m; l <= s.lmax; ++l)
+                    if (s.structure == AGB_STRUCT_ALL || (l % 2) == 0) cols += (m == 0) ? 1 : 2;
+            if (cols != s.n_lm)
+                return set_err(AGB_ERR_ARG, "regular multipole table: n_lm=%d, structure needs %d columns",
+                               s.n_lm, cols);
+        }
         if (precision == AGB_PREC_MIXED) {
             if (!s.table32 || !aligned16(s.table32))
                 return set_err(AGB_ERR_ARG, "mixed precision needs a 16-byte aligned FP32 table");
@@ -198,18 +214,61 @@ static int comp_to_dev(const agb_component& s, DevComp& d, int precision)
     return AGB_OK;
 }
 
-extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf* leaves,
-                        int n_leaves, const double* xyz, int64_t n, int mode, int precision,
-                        double* phi, double* grad, double* hess, double* rho, int out_flags,
-                        void* stream)
+// Binning plan: the Multipole leaf with the most harmonics keys the sort.
+struct BinPlan {
+    bool on;
+    BinKey key;
+    int n_bins;
+};
+
+static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, int n_leaves,
+                            int64_t n, int out_flags)
+{
+    BinPlan b;
+    memset(&b, 0, sizeof(b));
+    if ((out_flags & AGB_OUT_NO_BINNING) || n < AGB_BIN_MIN_POINTS || n > 0x7fffffffLL) return b;
+    int best = -1, best_lm = 0;
+    for (int L = 0; L < n_leaves; ++L) {
+        const agb_component& c = comps[leaves[L].comp];
+        if (c.kind == AGB_KIND_MULTIPOLE && c.n_lm > best_lm && c.n_int + 2 <= AGB_MAX_BINS) {
+            best = L;
+            best_lm = c.n_lm;
+        }
+    }
+    if (best < 0 || best_lm < 2) return b;
+    const agb_component& c = comps[leaves[best].comp];
+    b.on = true;
+    b.key.sigma = leaves[best].sigma;
+    b.key.g0 = leaves[best].gamma[0]; b.key.g1 = leaves[best].gamma[1]; b.key.g2 = leaves[best].gamma[2];
+    b.key.logr_min = c.p[0];
+    b.key.inv_dlogr = c.p[2];
+    b.key.n_int = c.n_int;
+    b.n_bins = c.n_int + 2;
+    return b;
+}
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static size_t ws_bytes(const BinPlan& b, int64_t n)
+{
+    if (!b.on) return 0;
+    return al256(4 * (size_t)n) * 2 + al256(24 * (size_t)n) + al256(4 * (size_t)b.n_bins) * 2;
+}
+
+static int validate(const agb_component* comps, int n_comps, const agb_leaf* leaves, int n_leaves,
+                    const double* xyz, int64_t n, int mode, int precision, double* phi,
+                    double* grad, double* hess, double* rho)
 {
     if (n < 0) return set_err(AGB_ERR_ARG, "agb_eval: negative point count");
-    if (n == 0) return AGB_OK;
-    if (!xyz) return set_err(AGB_ERR_ARG, "agb_eval: xyz is null");
+    if (n > 0 && !xyz) return set_err(AGB_ERR_ARG, "agb_eval: xyz is null");
     if (!comps || n_comps < 1 || !leaves || n_leaves < 1)
         return set_err(AGB_ERR_ARG, "agb_eval: empty component or leaf list");
     if (n_leaves > AGB_MAX_LEAVES)
         return set_err(AGB_ERR_UNSUPPORTED, "agb_eval: %d leaves exceed %d", n_leaves, AGB_MAX_LEAVES);
+    for (int L = 0; L < n_leaves; ++L)
+        if (leaves[L].comp < 0 || leaves[L].comp >= n_comps || leaves[L].comp >= 256)
+            return set_err(AGB_ERR_ARG, "agb_eval: leaf %d refers to component %d of %d", L,
+                           leaves[L].comp, n_comps);
     if (precision != AGB_PREC_FP64 && precision != AGB_PREC_MIXED)
         return set_err(AGB_ERR_ARG, "agb_eval: unknown precision %d", precision);
     switch (mode) {
@@ -219,19 +278,17 @@ extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf*
     case AGB_MODE_DENS: if (!rho) return set_err(AGB_ERR_ARG, "agb_eval: rho is null"); break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
+    return AGB_OK;
+}
 
-    static thread_local EvalArgs a;
-    memset(&a, 0, sizeof(a));
-    a.n = n; a.out_flags = out_flags; a.soa = 0; a.xyz = xyz;
-    a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
-    // pack only the components the leaves use
+static int pack_args(EvalArgs& a, const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                     int n_leaves, int precision)
+{
     int remap[256];
     for (int i = 0; i < 256; ++i) remap[i] = -1;
     int nc = 0;
     for (int L = 0; L < n_leaves; ++L) {
         const int ci = leaves[L].comp;
-        if (ci < 0 || ci >= n_comps || ci >= 256)
-            return set_err(AGB_ERR_ARG, "agb_eval: leaf %d refers to component %d of %d", L, ci, n_comps);
         if (remap[ci] < 0) {
             if (nc >= AGB_MAX_COMPONENTS)
                 return set_err(AGB_ERR_UNSUPPORTED, "agb_eval: more than %d distinct components", AGB_MAX_COMPONENTS);
@@ -246,7 +303,108 @@ extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf*
         d.ampl = leaves[L].ampl;
     }
     a.n_leaves = n_leaves;
-    return launch_mode(mode, precision, a, (cudaStream_t)stream);
+    (void)n_comps;
+    return AGB_OK;
+}
+
+static unsigned long long g_bin_attr_set = 0;     // one bit per device
+
+// Sort the points by interval into the workspace; sets a.xyz / a.perm.
+static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t n, char* ws,
+                       cudaStream_t st)
+{
+    int* keys = (int*)ws;
+    int* perm = (int*)(ws + al256(4 * (size_t)n));
+    double* xs = (double*)(ws + 2 * al256(4 * (size_t)n));
+    int* counts = (int*)(ws + 2 * al256(4 * (size_t)n) + al256(24 * (size_t)n));
+    int* cursor = (int*)((char*)counts + al256(4 * (size_t)b.n_bins));
+    const size_t smem1 = 4 * (size_t)b.n_bins, smem3 = 8 * (size_t)b.n_bins;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(g_bin_attr_set & bit)) {
+        cudaFuncSetAttribute(bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * AGB_MAX_BINS);
+        cudaFuncSetAttribute(bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * AGB_MAX_BINS);
+        g_bin_attr_set |= bit;
+    }
+    if (cudaMemsetAsync(counts, 0, 4 * (size_t)b.n_bins, st) != cudaSuccess)
+        return set_err(AGB_ERR_DEVICE, "agb_eval: memset of bin counts failed");
+    const int tiles = (int)((n + AGB_BIN_TILE - 1) / AGB_BIN_TILE);
+    bin_count<<<tiles, 256, smem1, st>>>(xyz, n, b.key, b.n_bins, keys, counts);
+    int rc = check_launch("bin_count");
+    if (rc) return rc;
+    bin_scan<<<1, 1024, 0, st>>>(counts, cursor, b.n_bins);
+    if ((rc = check_launch("bin_scan"))) return rc;
+    bin_scatter<<<tiles, 256, smem3, st>>>(xyz, n, b.n_bins, keys, cursor, perm, xs);
+    if ((rc = check_launch("bin_scatter"))) return rc;
+    a.xyz = xs;
+    a.perm = perm;
+    return AGB_OK;
+}
+
+static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* leaves, int n_leaves,
+                     const double* xyz, int64_t n, int mode, int precision, double* phi,
+                     double* grad, double* hess, double* rho, int out_flags, void* workspace,
+                     size_t workspace_bytes, bool own_ws, void* stream)
+{
+    int rc = validate(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess, rho);
+    if (rc) return rc;
+    if (n == 0) return AGB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n; a.out_flags = out_flags; a.soa = 0; a.xyz = xyz; a.perm = nullptr;
+    a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    if ((rc = pack_args(a, comps, n_comps, leaves, n_leaves, precision))) return rc;
+
+    const BinPlan b = plan_binning(comps, leaves, n_leaves, n, out_flags);
+    const size_t need = ws_bytes(b, n);
+    void* ws = workspace;
+    if (need) {
+        if (own_ws) {
+            if (cudaMallocAsync(&ws, need, st) != cudaSuccess)
+                return set_err(AGB_ERR_DEVICE, "agb_eval: cannot allocate %zu bytes of scratch", need);
+        } else if (!ws || workspace_bytes < need) {
+            return set_err(AGB_ERR_ARG, "agb_eval_ws: workspace of %zu bytes is smaller than the "
+                           "%zu bytes agb_eval_workspace_bytes asks for", workspace_bytes, need);
+        }
+        if ((uintptr_t)ws & 255u) {
+            if (own_ws) cudaFreeAsync(ws, st);
+            return set_err(AGB_ERR_ARG, "agb_eval_ws: workspace must be 256-byte aligned");
+        }
+        rc = run_binning(a, b, xyz, n, (char*)ws, st);
+    }
+    if (!rc) rc = launch_mode(mode, precision, a, st);
+    if (need && own_ws) cudaFreeAsync(ws, st);
+    return rc;
+}
+
+extern "C" size_t agb_eval_workspace_bytes(const agb_component* comps, int n_comps,
+                                           const agb_leaf* leaves, int n_leaves, int64_t n,
+                                           int out_flags)
+{
+    if (!comps || !leaves || n_leaves < 1 || n_comps < 1) return 0;
+    for (int L = 0; L < n_leaves; ++L)
+        if (leaves[L].comp < 0 || leaves[L].comp >= n_comps) return 0;
+    return ws_bytes(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
+}
+
+extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                        int n_leaves, const double* xyz, int64_t n, int mode, int precision,
+                        double* phi, double* grad, double* hess, double* rho, int out_flags,
+                        void* stream)
+{
+    return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
+                     rho, out_flags, nullptr, 0, true, stream);
+}
+
+extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                           int n_leaves, const double* xyz, int64_t n, int mode, int precision,
+                           double* phi, double* grad, double* hess, double* rho, int out_flags,
+                           void* workspace, size_t workspace_bytes, void* stream)
+{
+    return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
+                     rho, out_flags, workspace, workspace_bytes, false, stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -210,6 +210,175 @@ __device__ __forceinline__ void mp_harmonics(const DevComp& c, int k, double s_d
     mp_flush<MODE, R>(tot, g);
 }
 
+// ---------------------------------------------------------------------------
+// Regular column structure (AGB_STRUCT_ALL / AGB_STRUCT_EVEN): every (l, m) up
+// to lmax (or every even l) has a column, in (|m|, l, cos, sin) order, so the
+// walk needs no harmonic list.  Per |m| group the sums over l are formed
+// without cos/sin(m phi): the group's cos-column and sin-column sums are
+// multiplied by cos(m phi), sin(m phi) (and their phi derivatives) once, in FP64.
+// The quintic is evaluated in the power basis with the powers of s (and the
+// derivative weights j s^(j-1), j (j-1) s^(j-2)) formed once per point.
+// ---------------------------------------------------------------------------
+template <typename R> struct MPPtr;
+template <> struct MPPtr<double> {
+    static constexpr int REC = 6;
+    static __device__ __forceinline__ const double* base(const DevComp& c, int k)
+    {
+        return c.table + (long long)k * c.n_lm * 6;
+    }
+    static __device__ __forceinline__ void load(const double* p, double a[6])
+    {
+        const double2* q = reinterpret_cast<const double2*>(p);
+        const double2 v0 = __ldg(q), v1 = __ldg(q + 1), v2 = __ldg(q + 2);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y; a[4] = v2.x; a[5] = v2.y;
+    }
+};
+template <> struct MPPtr<float> {
+    static constexpr int REC = 8;
+    static __device__ __forceinline__ const float* base(const DevComp& c, int k)
+    {
+        return c.table32 + (long long)k * c.n_lm * 8;
+    }
+    static __device__ __forceinline__ void load(const float* p, float a[6])
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        const float4 v0 = __ldg(q), v1 = __ldg(q + 1);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v0.z; a[3] = v0.w; a[4] = v1.x; a[5] = v1.y;
+    }
+};
+
+template <typename R> struct MPCol {         // per-group sums of one trig column (cos or sin)
+    R V, VR, VRR, VT, VTT, VRT, VP, L;
+    __device__ __forceinline__ void zero() { V = VR = VRR = VT = VTT = VRT = VP = L = R(0); }
+};
+
+template <int MODE, typename R>
+__device__ __forceinline__ void mp_col_acc(MPCol<R>& g, const R a[6], const R sp[6],
+                                           const R dw[6], const R ew[6], R Y, R dY, R d2Y,
+                                           R Pos, R ll1)
+{
+    constexpr bool NEED_B = MODE != AGB_MODE_POT;
+    constexpr bool NEED_D = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
+    constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
+    // C = sum a_j s^j as two short chains
+    const R C = fma(a[2], sp[2], fma(a[1], sp[1], a[0])) + fma(a[5], sp[5], fma(a[4], sp[4], a[3] * sp[3]));
+    g.V = fma(C, Y, g.V);
+    if (NEED_B) {
+        const R dC = fma(a[2], dw[2], a[1]) + fma(a[5], dw[5], fma(a[4], dw[4], a[3] * dw[3]));
+        g.VR = fma(dC, Y, g.VR);
+        if (MODE == AGB_MODE_HESS) g.VRT = fma(dC, dY, g.VRT);
+    }
+    if (NEED_D) {
+        const R d2C = fma(a[3], ew[3], R(2) * a[2]) + fma(a[5], ew[5], a[4] * ew[4]);
+        g.VRR = fma(d2C, Y, g.VRR);
+    }
+    if (MODE == AGB_MODE_DENS) g.L = fma(ll1 * C, Y, g.L);
+    if (NEED_ANG) {
+        g.VT = fma(C, dY, g.VT);
+        g.VP = fma(C, Pos, g.VP);
+        if (MODE == AGB_MODE_HESS) g.VTT = fma(C, d2Y, g.VTT);
+    }
+}
+
+template <int MODE, typename R, int PAR>
+__device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double s_d,
+                                                 double cth_d, double sth_d,
+                                                 double cph, double sph, MPSums& tot)
+{
+    constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
+    constexpr bool NEED_ANG2 = MODE == AGB_MODE_HESS;
+    const bool near_pole = sth_d < 1.0e-10;
+    const R s = (R)s_d;
+    R sp[6], dw[6], ew[6];
+    sp[0] = R(1); sp[1] = s; sp[2] = s * s; sp[3] = sp[2] * s; sp[4] = sp[2] * sp[2]; sp[5] = sp[4] * s;
+    dw[0] = R(0); dw[1] = R(1); dw[2] = R(2) * s; dw[3] = R(3) * sp[2]; dw[4] = R(4) * sp[3]; dw[5] = R(5) * sp[4];
+    ew[0] = R(0); ew[1] = R(0); ew[2] = R(2); ew[3] = R(6) * s; ew[4] = R(12) * sp[2]; ew[5] = R(20) * sp[3];
+    const R cth = (R)cth_d, sth = (R)sth_d;
+    const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
+    const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
+    const R np1 = near_pole ? R(0) : R(1);
+    const int lmax = c.lmax;
+    const R* rec = MPPtr<R>::base(c, k) + MPPtr<R>::REC;       // column 1 (column 0 = monopole)
+
+    double cm = 1.0, sm = 0.0, sinpow = 1.0, sinpow_m1 = 0.0;
+    for (int m = 0; m <= lmax; ++m) {
+        if (m > 0) {
+            const double t = cm * cph - sm * sph;
+            sm = sm * cph + cm * sph;
+            cm = t;
+            sinpow_m1 = sinpow;
+            sinpow *= sth_d;
+        }
+        int l0 = (PAR == 2) ? (m + (m & 1)) : m;
+        if (m == 0) l0 = PAR;                                   // column 0 is the monopole
+        if (l0 > lmax) continue;
+        const R q1 = (near_pole && m == 1) ? R(1) : R(0);       // pole rule for Y/sin(theta)
+        const R m2 = R(m * m) * inv_sth * inv_sth;
+        R Pc = (R)(AGB_SEED[m] * sinpow), Pp = R(0), dPc = R(0), dPp = R(0);
+        if (NEED_ANG && m > 0)
+            dPc = (m == 1) ? (R)(AGB_SEED[1] * cth_d)
+                           : (near_pole ? R(0) : (R)((double)m * AGB_SEED[m] * sinpow_m1 * cth_d));
+        MPCol<R> gc, gs;
+        gc.zero();
+        gs.zero();
+        const int tb = m * AGB_LEG_N;
+        auto step = [&](int L) {
+            const R a = MPConst<R>::alpha(tb + L), b = MPConst<R>::beta(tb + L);
+            const R Pn = fma(a * cth, Pc, -b * Pp);
+            if (NEED_ANG) {
+                const R dPn = fma(a, fma(cth, dPc, -sth * Pc), -b * dPp);
+                dPp = dPc;
+                dPc = dPn;
+            }
+            Pp = Pc;
+            Pc = Pn;
+        };
+        auto acc = [&](int L) {
+            const R ll1 = R(L * (L + 1));
+            R Pos = R(0), d2Y = R(0);
+            if (NEED_ANG) Pos = fma(Pc, inv_sth, q1 * dPc);
+            if (NEED_ANG2) d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
+            R a[6];
+            MPPtr<R>::load(rec, a);
+            rec += MPPtr<R>::REC;
+            mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            if (m > 0) {
+                MPPtr<R>::load(rec, a);
+                rec += MPPtr<R>::REC;
+                mp_col_acc<MODE, R>(gs, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            }
+        };
+        int l = m;
+        while (l < l0) step(++l);
+        acc(l);
+        for (l = l0 + PAR; l <= lmax; l += PAR) {
+            if (PAR == 2) step(l - 1);
+            step(l);
+            acc(l);
+        }
+        // combine the group's cos and sin sums with cos/sin(m phi) in FP64
+        const double md = (double)m;
+        const double dTc = -md * sm, dTs = md * cm;
+        tot.A += (double)gc.V * cm + (double)gs.V * sm;
+        if (MODE != AGB_MODE_POT) tot.B += (double)gc.VR * cm + (double)gs.VR * sm;
+        if (MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS)
+            tot.D += (double)gc.VRR * cm + (double)gs.VRR * sm;
+        if (MODE == AGB_MODE_DENS) tot.L += (double)gc.L * cm + (double)gs.L * sm;
+        if (NEED_ANG) {
+            tot.Th += (double)gc.VT * cm + (double)gs.VT * sm;
+            tot.Pos += (double)gc.VP * dTc + (double)gs.VP * dTs;
+        }
+        if (NEED_ANG2) {
+            tot.Thth += (double)gc.VTT * cm + (double)gs.VTT * sm;
+            tot.BTh += (double)gc.VRT * cm + (double)gs.VRT * sm;
+            tot.Ph += (double)gc.V * dTc + (double)gs.V * dTs;
+            tot.Phph += -md * md * ((double)gc.V * cm + (double)gs.V * sm);
+            tot.BPh += (double)gc.VR * dTc + (double)gs.VR * dTs;
+            tot.ThPh += (double)gc.VT * dTc + (double)gs.VT * dTs;
+        }
+    }
+}
+
 __device__ __forceinline__ void mp_quintic0(const DevComp& c, int k, double s,
                                             double& v, double& d1, double& d2)
 {
@@ -317,7 +486,12 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
     }
 
     MPSums t = {};
-    mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
+    if (c.structure == AGB_STRUCT_EVEN)
+        mp_harmonics_reg<MODE, R, 2>(c, k, s, cth, sth, cph, sph, t);
+    else if (c.structure == AGB_STRUCT_ALL)
+        mp_harmonics_reg<MODE, R, 1>(c, k, s, cth, sth, cph, sph, t);
+    else
+        mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
 
     const double Bp = t.B * inv_dlogr;
     const double Dp = t.D * inv_dlogr * inv_dlogr;

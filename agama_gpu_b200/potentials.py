@@ -113,6 +113,7 @@ class _GPUPotBase:
     """
 
     precision: Optional[str] = None
+    binning: bool = True          # sort points by radial interval before evaluating
 
     def __add__(self, other):
         a = self._components if isinstance(self, CompositePotentialGPU) else [self]
@@ -127,6 +128,11 @@ class _GPUPotBase:
     # subclasses implement: leaves at time t
     def _leaves(self, t: float) -> List[Leaf]:
         raise NotImplementedError
+
+    def set_binning(self, on: bool):
+        """Sort points by radial interval before evaluating (default) or keep input order."""
+        self.binning = bool(on)
+        return self
 
     def set_precision(self, precision: Optional[str]):
         """Per-object arithmetic of the Multipole sums: 'fp64', 'mixed' or None (default)."""
@@ -179,10 +185,13 @@ class _GPUPotBase:
             return phi, grad, hess, rho
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         stream = torch.cuda.current_stream(dev).cuda_stream
-        rc = _lib.lib.agb_eval(comp_arr, len(comps), leaf_arr, len(leaves), arr.data_ptr(), n,
-                               mode, prec, ptr(phi), ptr(grad), ptr(hess), ptr(rho),
-                               _lib.OUT_NEGATE, ctypes.c_void_p(stream))
-        _lib.check(rc, "agb_eval")
+        flags = _lib.OUT_NEGATE | (0 if self.binning else _lib.OUT_NO_BINNING)
+        nws = _lib.lib.agb_eval_workspace_bytes(comp_arr, len(comps), leaf_arr, len(leaves), n, flags)
+        ws = torch.empty(int(nws), dtype=torch.uint8, device=dev) if nws else None
+        rc = _lib.lib.agb_eval_ws(comp_arr, len(comps), leaf_arr, len(leaves), arr.data_ptr(), n,
+                                  mode, prec, ptr(phi), ptr(grad), ptr(hess), ptr(rho), flags,
+                                  ptr(ws), int(nws), ctypes.c_void_p(stream))
+        _lib.check(rc, "agb_eval_ws")
         return phi, grad, hess, rho
 
     # -- public API (gpu_potential.py:826-935) --------------------------------
@@ -277,8 +286,13 @@ class MultipolePotentialGPU(_Component):
     def __init__(self, coefs, prune_threshold: float = 1e-16) -> None:
         self.tables = build_multipole_tables(coefs, prune_threshold=prune_threshold)
         t = self.tables
-        self._poly_im = t.interval_major()
-        self._poly32 = t.interval_major_f32()
+        self._structure, reg = t.regular()
+        poly = t.poly if reg is None else reg
+        self._n_cols = poly.shape[0]
+        self._poly_im = np.ascontiguousarray(poly.transpose(1, 0, 2))
+        p32 = np.zeros((t.n_int, self._n_cols, 8), dtype=np.float32)
+        p32[:, :, :6] = self._poly_im.astype(np.float32)
+        self._poly32 = p32
         self._lm = t.lm_packed()
 
     @classmethod
@@ -315,11 +329,12 @@ class MultipolePotentialGPU(_Component):
         lm = torch.from_numpy(self._lm).to(dev)
         c = _lib.AgbComponent()
         c.kind = self.kind
-        c.n_lm = t.n_lm
+        c.n_lm = self._n_cols
         c.n_int = t.n_int
         c.lmax = t.lmax
         c.log_scaling = t.log_scaling
         c.layout = _lib.LAYOUT_INTERVAL_MAJOR
+        c.structure = self._structure
         c.table = poly.data_ptr()
         c.table32 = poly32.data_ptr()
         c.lm = lm.data_ptr()

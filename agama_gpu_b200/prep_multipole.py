@@ -71,6 +71,34 @@ class MultipoleTables:
     def lm_packed(self) -> np.ndarray:
         return ((self.lm_l.astype(np.int64) << 16) | (self.lm_m.astype(np.int64) & 0xFFFF)).astype(np.int32)
 
+    def regular(self, max_ratio: float = 1.5):
+        """Column structure for the kernels' regular walk.
+
+        Returns (structure, poly_reg) where structure is 1 (every l) or 2 (even l
+        only) and poly_reg (n_reg, n_int, 6) holds every (l, m) with l <= lmax of
+        that parity in (|m|, l, cos before sin) order -- the order the table
+        builder sorts by -- with zero columns for harmonics the builder pruned;
+        or (0, None) when the regular layout would exceed max_ratio times the
+        pruned column count.
+        """
+        L = self.lmax
+        even = bool(np.all(self.lm_l % 2 == 0))
+        order = []
+        for am in range(L + 1):
+            for l in range(am, L + 1):
+                if even and l % 2:
+                    continue
+                order.append((l, am))
+                if am > 0:
+                    order.append((l, -am))
+        if len(order) > max_ratio * self.n_lm:
+            return 0, None
+        pos = {lm: i for i, lm in enumerate(order)}
+        reg = np.zeros((len(order), self.n_int, 6))
+        for c, (l, m) in enumerate(zip(self.lm_l.tolist(), self.lm_m.tolist())):
+            reg[pos[(l, m)]] = self.poly[c]
+        return (2 if even else 1), reg
+
     def scalars(self) -> list:
         return [self.logr_min, self.dlogr, self.inv_dlogr, self.invPhi0, self.inner_s,
                 self.inner_U, self.inner_W, self.outer_s, self.outer_U, self.outer_W]

@@ -28,6 +28,7 @@
 #ifndef AGB_H
 #define AGB_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -54,7 +55,12 @@ extern "C" {
                               composite sum                                       */
 
 /* output flags for agb_eval */
-#define AGB_OUT_NEGATE 1   /* write -grad (force) and -Hessian (forceDeriv layout) */
+#define AGB_OUT_NEGATE     1   /* write -grad (force) and -Hessian (forceDeriv layout) */
+#define AGB_OUT_NO_BINNING 2   /* evaluate the points in input order (no scratch memory) */
+
+/* agb_eval sorts the points by the radial interval of its heaviest Multipole
+   leaf (a counting sort in device scratch) when there are at least this many */
+#define AGB_BIN_MIN_POINTS 16384
 
 /* component kinds */
 #define AGB_KIND_MULTIPOLE      1
@@ -74,6 +80,11 @@ extern "C" {
 #define AGB_LAYOUT_INTERVAL_MAJOR 1  /* poly[(k*n_lm + c)*6 + j]: one contiguous slab per
                                         radial interval                                  */
 
+/* Multipole column structure (agb_component.structure) */
+#define AGB_STRUCT_LIST 0
+#define AGB_STRUCT_ALL  1
+#define AGB_STRUCT_EVEN 2
+
 #define AGB_MAX_LEAVES 32
 #define AGB_MAX_COMPONENTS 24
 #define AGB_MAX_LMAX 32
@@ -87,6 +98,11 @@ extern "C" {
  *   lm         packed harmonic list, lm[c] = (l << 16) | (m & 0xffff), sorted by
  *              (|m|, l, cos before sin), lm[0] = (0,0)
  *   n_lm, n_int, lmax, log_scaling, layout
+ *   structure  AGB_STRUCT_LIST: the columns are exactly the harmonics in lm;
+ *              AGB_STRUCT_ALL / AGB_STRUCT_EVEN: the columns are every (l, m)
+ *              with l <= lmax (every l, or even l only), ordered by (|m|, l,
+ *              cos before sin), pruned harmonics present as zero columns; the
+ *              kernel then walks the harmonics without reading lm
  *   p[0..9]    logr_min, dlogr, inv_dlogr, invPhi0, inner_s, inner_U, inner_W,
  *              outer_s, outer_U, outer_W
  * CYLSPLINE  (tables from gpu_potential.py:1143-1253, relaid per cell)
@@ -106,7 +122,7 @@ typedef struct agb_component {
     int32_t lmax;
     int32_t log_scaling;
     int32_t layout;
-    int32_t reserved;
+    int32_t structure;
     const double*  table;
     const float*   table32;
     const int32_t* lm;
@@ -160,6 +176,21 @@ int agb_eval(const agb_component* comps, int n_comps,
              const double* xyz, int64_t n, int mode, int precision,
              double* phi, double* grad, double* hess, double* rho,
              int out_flags, void* stream);
+
+/*
+ * agb_eval with caller-provided device scratch for the interval sort (no
+ * allocation inside).  workspace: 256-byte aligned, at least
+ * agb_eval_workspace_bytes(...) bytes (0 when the call does not sort; then
+ * workspace may be NULL).  The scratch is about 32 bytes per point.
+ */
+size_t agb_eval_workspace_bytes(const agb_component* comps, int n_comps,
+                                const agb_leaf* leaves, int n_leaves, int64_t n,
+                                int out_flags);
+int agb_eval_ws(const agb_component* comps, int n_comps,
+                const agb_leaf* leaves, int n_leaves,
+                const double* xyz, int64_t n, int mode, int precision,
+                double* phi, double* grad, double* hess, double* rho,
+                int out_flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Kernel-signature entries.  Arguments are those of the reference kernels, in

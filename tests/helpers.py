@@ -113,8 +113,8 @@ def tree_allowance(pot, xyz, t: float = 0.0):
         if m.any():
             c[m] = outer_condition(comp.tables, x[m])
         a_phi += abs(ampl) * c
-        a_g += abs(ampl * sigma) * c / r
-        a_h += abs(ampl * sigma * sigma) * c / (r * r)
+        a_g += abs(ampl * sigma) * np.divide(c, r, out=np.zeros_like(c), where=c > 0)
+        a_h += abs(ampl * sigma * sigma) * np.divide(c, r * r, out=np.zeros_like(c), where=c > 0)
     return a_phi, a_g, a_h
 
 
@@ -125,7 +125,7 @@ def close_pointwise(a, b, tol, allow=None) -> bool:
     if _finite_pair(a, b) is None:
         return False
     f = np.isfinite(b)
-    d = np.where(f, np.abs(a - b), 0.0).max(axis=1)
+    d = np.abs(np.where(f, a, 0.0) - np.where(f, b, 0.0)).max(axis=1)
     lim = tol * np.where(f, np.abs(b), 0.0).max(axis=1)
     if allow is not None:
         lim = lim + 64 * EPS * np.asarray(allow)
@@ -139,7 +139,7 @@ def close_global(a, b, tol, allow=None) -> bool:
     if _finite_pair(a, b) is None:
         return False
     f = np.isfinite(b)
-    d = np.where(f, np.abs(a - b), 0.0).max(axis=1)
+    d = np.abs(np.where(f, a, 0.0) - np.where(f, b, 0.0)).max(axis=1)
     lim = tol * (np.abs(b[f]).max() if f.any() else 0.0)
     if allow is not None:
         lim = lim + 64 * EPS * np.asarray(allow)

@@ -48,7 +48,12 @@ def test_argument_errors_need_no_gpu():
     rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
                            ctypes.c_void_p(16), None, None, 0, None)
     assert rc == -1 and "refers to component" in _lib.last_error()
-    assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, None, None, None, 0, None) == 0
+    comps[0].kind = _lib.KIND_NFW
+    leaves[0].comp = 0
+    # zero points: nothing to do, no device touched
+    assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, ctypes.c_void_p(16),
+                             None, None, 0, None) == 0
+    assert _lib.lib.agb_eval_workspace_bytes(comps, 1, leaves, 1, 10**6, 0) == 0   # no Multipole
     # lmax beyond the kernel's limit
     comps[0].kind = _lib.KIND_MULTIPOLE
     comps[0].lmax = 40
