@@ -408,6 +408,58 @@ extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_le
 }
 
 // ---------------------------------------------------------------------------
+// agb_eval_static: the fused evaluation with its sorting scratch in a fixed
+// device array of this library, for callers that must not allocate.
+//
+// Some host programs cannot let a library allocate device memory and cannot
+// hand it scratch either: an N-body or orbit code that reserves the whole GPU
+// for its own particle pool, a latency-critical loop that must never pay the
+// device-wide synchronisation of cudaMalloc/cudaFree, or a plain C/Fortran
+// caller whose interface only passes the arrays it already owns.  This entry
+// point serves them.  The scratch lives in g_static_scratch below
+// (AGB_STATIC_SCRATCH_BYTES = 32 MiB), which every GPU that loads this library
+// holds until the process exits; it limits one call to AGB_STATIC_MAX_POINTS
+// points.  Host code cannot use the array's name as a device address: the
+// address is fetched with cudaGetSymbolAddress once per device, on the first
+// call made with that device current, and that first call should be made
+// before any stream capture begins.  All calls share the one array and it
+// keeps whatever the last call left there (the bin counts that must start at
+// zero are cleared by every call), so calls whose work overlaps on the GPU
+// (other streams, other host threads) race on it: serialise them.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_static_scratch[AGB_STATIC_SCRATCH_BYTES];
+static void* g_static_scratch_addr[64] = {nullptr};
+
+extern "C" int agb_eval_static(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                               int n_leaves, const double* xyz, int64_t n, int mode,
+                               int precision, double* phi, double* grad, double* hess,
+                               double* rho, int out_flags, void* stream)
+{
+    if (n > AGB_STATIC_MAX_POINTS)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_static: %lld points exceed its fixed scratch "
+                       "limit of %d points (use agb_eval or agb_eval_ws)", (long long)n,
+                       AGB_STATIC_MAX_POINTS);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return set_err(AGB_ERR_DEVICE, "agb_eval_static: no usable current CUDA device");
+    if (!g_static_scratch_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_err(AGB_ERR_DEVICE, "agb_eval_static: cudaGetSymbolAddress failed: %s",
+                           cudaGetErrorString(e));
+        g_static_scratch_addr[dev] = p;
+    }
+    const size_t need = agb_eval_workspace_bytes(comps, n_comps, leaves, n_leaves, n, out_flags);
+    if (need > (size_t)AGB_STATIC_SCRATCH_BYTES)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_static: needs %zu bytes of scratch, more "
+                       "than its fixed %d", need, AGB_STATIC_SCRATCH_BYTES);
+    return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
+                     rho, out_flags, g_static_scratch_addr[dev], (size_t)AGB_STATIC_SCRATCH_BYTES,
+                     false, stream);
+}
+
+// ---------------------------------------------------------------------------
 // kernel-signature entries
 // ---------------------------------------------------------------------------
 static int mp_compat(int mode, const double* x, const double* y, const double* z,

@@ -193,6 +193,26 @@ int agb_eval_ws(const agb_component* comps, int n_comps,
                 int out_flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * agb_eval_static -- agb_eval that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that may not allocate device memory (a
+ * code that reserved the GPU for its own pools, a loop that must not pay
+ * cudaMalloc's device synchronisation, a C/Fortran caller that only passes
+ * arrays it owns).  The point-sorting scratch is a fixed 32 MiB device array
+ * inside this library (held on every GPU that loads it), so one call takes at
+ * most AGB_STATIC_MAX_POINTS points; larger calls fail with
+ * AGB_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ */
+#define AGB_STATIC_SCRATCH_BYTES (32 * 1024 * 1024)
+#define AGB_STATIC_MAX_POINTS 1000000
+int agb_eval_static(const agb_component* comps, int n_comps,
+                    const agb_leaf* leaves, int n_leaves,
+                    const double* xyz, int64_t n, int mode, int precision,
+                    double* phi, double* grad, double* hess, double* rho,
+                    int out_flags, void* stream);
+
+/*
  * Kernel-signature entries.  Arguments are those of the reference kernels, in
  * order, with SoA x, y, z device arrays, the reference's harmonic-major poly
  * layout and lm_l/lm_m arrays sorted as gpu_potential.py:516 sorts them.
