@@ -21,6 +21,7 @@
 //     (mixed: FP32 recurrences and polynomials, per-|m| FP32 partial sums
 //     promoted to FP64, FP64 everywhere else).
 #pragma once
+#include <type_traits>
 #include "agb_dev.cuh"
 
 // Radial sums of one Multipole at one point (component frame).
@@ -333,29 +334,33 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
             Pp = Pc;
             Pc = Pn;
         };
-        auto acc = [&](int L) {
+        // one l: both trig columns' records are loaded before any arithmetic so
+        // the loads of a loop body issue together (no branch inside the body)
+        auto acc = [&](int L, auto has_sin) {
+            R ac[6], as[6];
+            MPPtr<R>::load(rec, ac);
+            if (has_sin) MPPtr<R>::load(rec + MPPtr<R>::REC, as);
+            rec += has_sin ? 2 * MPPtr<R>::REC : MPPtr<R>::REC;
             const R ll1 = R(L * (L + 1));
             R Pos = R(0), d2Y = R(0);
             if (NEED_ANG) Pos = fma(Pc, inv_sth, q1 * dPc);
             if (NEED_ANG2) d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
-            R a[6];
-            MPPtr<R>::load(rec, a);
-            rec += MPPtr<R>::REC;
-            mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
-            if (m > 0) {
-                MPPtr<R>::load(rec, a);
-                rec += MPPtr<R>::REC;
-                mp_col_acc<MODE, R>(gs, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            mp_col_acc<MODE, R>(gc, ac, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            if (has_sin) mp_col_acc<MODE, R>(gs, as, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+        };
+        auto walk = [&](auto has_sin) {
+            int l = m;
+            while (l < l0) step(++l);
+            acc(l, has_sin);
+            #pragma unroll 2
+            for (l = l0 + PAR; l <= lmax; l += PAR) {
+                if (PAR == 2) step(l - 1);
+                step(l);
+                acc(l, has_sin);
             }
         };
-        int l = m;
-        while (l < l0) step(++l);
-        acc(l);
-        for (l = l0 + PAR; l <= lmax; l += PAR) {
-            if (PAR == 2) step(l - 1);
-            step(l);
-            acc(l);
-        }
+        if (m == 0) walk(std::false_type());
+        else walk(std::true_type());
         // combine the group's cos and sin sums with cos/sin(m phi) in FP64
         const double md = (double)m;
         const double dTc = -md * sm, dTs = md * cm;
