@@ -12,7 +12,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libagb.so"
 
 AGB_OK = 0
-MODE_POT, MODE_GRAD, MODE_HESS, MODE_DENS = 0, 1, 2, 3
+MODE_POT, MODE_GRAD, MODE_HESS, MODE_DENS, MODE_VJP = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 OUT_NEGATE = 1
 OUT_NO_BINNING = 2
@@ -85,6 +85,11 @@ def _load():
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_int, ctypes.c_void_p]
+    lib.agb_eval_vjp.restype = ctypes.c_int
+    lib.agb_eval_vjp.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_eval_static.restype = ctypes.c_int
     lib.agb_eval_static.argtypes = lib.agb_eval.argtypes
     lib.agb_eval_workspace_bytes.restype = ctypes.c_size_t
@@ -105,7 +110,7 @@ lib = _load()
 # symbols the header declares (checked by tests/test_capi.py)
 EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
-    "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static",
+    "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
     "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
 ]

@@ -54,6 +54,8 @@ struct EvalArgs {
     double* grad;
     double* hess;
     double* rho;
+    const double* gphi;      // VJP mode: dL/dPhi [N] (may be null)
+    const double* gforce;    // VJP mode: dL/dF [N,3] (may be null)
     DevComp comps[AGB_MAX_COMPONENTS];
     DevLeaf leaves[AGB_MAX_LEAVES];
 };

@@ -149,7 +149,11 @@ __device__ __forceinline__ void cs_load(const DevComp& c, int h, int iR, int iz,
     }
 }
 
-template <int MODE>
+// EXACT: add the dPhi/dphi * d2(phi)/dx_i dx_j terms of the Cartesian Hessian,
+// which the reference's conversion omits (_cylspl_potential_kernel.cu:836-852);
+// used for derivatives (the VJP), not for forceDeriv, which keeps the
+// reference's values.
+template <int MODE, bool EXACT = false>
 __device__ __forceinline__ void cylspline_point(const DevComp& c, double px, double py,
                                                 double pz, PointOut& o)
 {
@@ -294,6 +298,12 @@ __device__ __forceinline__ void cylspline_point(const DevComp& c, double px, dou
         o.h[3] = H_RR * xy * R2i + H_Rp * (x2 - y2) * R3i - H_pp * xy * R2i * R2i - dPdR * xy * R3i;
         o.h[4] = H_Rz * (y * Ri) + H_zp * (x * R2i);
         o.h[5] = H_Rz * (x * Ri) - H_zp * (y * R2i);
+        if (EXACT) {
+            const double R4i = R2i * R2i;
+            o.h[0] += 2.0 * Pp * xy * R4i;
+            o.h[1] -= 2.0 * Pp * xy * R4i;
+            o.h[3] += Pp * (y2 - x2) * R4i;
+        }
     } else {
         o.h[0] = H_RR; o.h[1] = H_RR; o.h[2] = H_zz;
         o.h[3] = 0.0; o.h[4] = 0.0; o.h[5] = 0.0;

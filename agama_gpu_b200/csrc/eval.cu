@@ -49,13 +49,13 @@ static int check_launch(const char* what)
 // ---------------------------------------------------------------------------
 // the fused kernel
 // ---------------------------------------------------------------------------
-template <int MODE, typename R>
+template <int MODE, typename R, bool EXACT>
 __device__ __forceinline__ void eval_component(const DevComp& c, double x, double y, double z,
                                                PointOut& o)
 {
     switch (c.kind) {
     case AGB_KIND_MULTIPOLE:     multipole_point<MODE, R>(c, x, y, z, o); break;
-    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE>(c, x, y, z, o); break;
+    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE, EXACT>(c, x, y, z, o); break;
     case AGB_KIND_NFW:           nfw_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_PLUMMER:       plummer_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_HERNQUIST:     hernquist_point<MODE>(c.p, x, y, z, o); break;
@@ -69,10 +69,14 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
     }
 }
 
+// Hessian-carrying modes hold about twice the live state: one block per SM
+// with up to 255 registers beats two blocks with heavy spilling.
 template <int MODE, typename R>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP) ? 1 : 2)
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
+    // the VJP mode evaluates every component with its Hessian and contracts at the end
+    constexpr int CM = (MODE == AGB_MODE_VJP) ? AGB_MODE_HESS : MODE;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < a.n; pos += stride) {
         double x, y, z;
@@ -95,22 +99,32 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             o.g[0] = o.g[1] = o.g[2] = 0.0;
             #pragma unroll
             for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
-            eval_component<MODE, R>(c, lx, ly, lz, o);
+            eval_component<CM, R, MODE == AGB_MODE_VJP>(c, lx, ly, lz, o);
             const double A = lf.ampl;
-            if (MODE == AGB_MODE_DENS) {
+            if (CM == AGB_MODE_DENS) {
                 rho += (A * lf.sigma * lf.sigma) * o.rho;
                 continue;
             }
             phi += A * o.phi;
-            if (MODE != AGB_MODE_POT) {
+            if (CM != AGB_MODE_POT) {
                 const double As = A * lf.sigma;
                 g0 += As * o.g[0]; g1 += As * o.g[1]; g2 += As * o.g[2];
-                if (MODE == AGB_MODE_HESS) {
+                if (CM == AGB_MODE_HESS) {
                     const double As2 = As * lf.sigma;
                     #pragma unroll
                     for (int q = 0; q < 6; ++q) h[q] += As2 * o.h[q];
                 }
             }
+        }
+        if (MODE == AGB_MODE_VJP) {
+            // L(Phi, F): dL/dx = gPhi grad(Phi) + (dF/dx)^T gF = gPhi grad(Phi) - H gF
+            const double gp = a.gphi ? a.gphi[i] : 0.0;
+            double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+            if (a.gforce) { f0 = a.gforce[3 * i]; f1 = a.gforce[3 * i + 1]; f2 = a.gforce[3 * i + 2]; }
+            a.grad[3 * i]     = gp * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
+            a.grad[3 * i + 1] = gp * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
+            a.grad[3 * i + 2] = gp * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
+            continue;
         }
         const double sg = (a.out_flags & AGB_OUT_NEGATE) ? -1.0 : 1.0;
         if (MODE == AGB_MODE_DENS) {
@@ -160,6 +174,7 @@ static int launch_mode(int mode, int precision, const EvalArgs& a, cudaStream_t 
     case AGB_MODE_GRAD: mixed ? launch_eval<AGB_MODE_GRAD, float>(a, st) : launch_eval<AGB_MODE_GRAD, double>(a, st); break;
     case AGB_MODE_HESS: mixed ? launch_eval<AGB_MODE_HESS, float>(a, st) : launch_eval<AGB_MODE_HESS, double>(a, st); break;
     case AGB_MODE_DENS: mixed ? launch_eval<AGB_MODE_DENS, float>(a, st) : launch_eval<AGB_MODE_DENS, double>(a, st); break;
+    case AGB_MODE_VJP:  mixed ? launch_eval<AGB_MODE_VJP, float>(a, st)  : launch_eval<AGB_MODE_VJP, double>(a, st); break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
     return check_launch("agb_eval_kernel");
@@ -276,6 +291,7 @@ static int validate(const agb_component* comps, int n_comps, const agb_leaf* lea
     case AGB_MODE_GRAD: if (!grad) return set_err(AGB_ERR_ARG, "agb_eval: grad is null"); break;
     case AGB_MODE_HESS: if (!hess) return set_err(AGB_ERR_ARG, "agb_eval: hess is null"); break;
     case AGB_MODE_DENS: if (!rho) return set_err(AGB_ERR_ARG, "agb_eval: rho is null"); break;
+    case AGB_MODE_VJP:  if (!grad) return set_err(AGB_ERR_ARG, "agb_eval_vjp: g_xyz is null"); break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
     return AGB_OK;
@@ -342,6 +358,9 @@ static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t
     return AGB_OK;
 }
 
+static thread_local const double* g_vjp_phi = nullptr;    // set by agb_eval_vjp for one call
+static thread_local const double* g_vjp_force = nullptr;
+
 static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* leaves, int n_leaves,
                      const double* xyz, int64_t n, int mode, int precision, double* phi,
                      double* grad, double* hess, double* rho, int out_flags, void* workspace,
@@ -355,6 +374,7 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
     memset(&a, 0, sizeof(a));
     a.n = n; a.out_flags = out_flags; a.soa = 0; a.xyz = xyz; a.perm = nullptr;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    a.gphi = g_vjp_phi; a.gforce = g_vjp_force;
     if ((rc = pack_args(a, comps, n_comps, leaves, n_leaves, precision))) return rc;
 
     const BinPlan b = plan_binning(comps, leaves, n_leaves, n, out_flags);
@@ -396,6 +416,21 @@ extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf*
 {
     return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
                      rho, out_flags, nullptr, 0, true, stream);
+}
+
+extern "C" int agb_eval_vjp(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                            int n_leaves, const double* xyz, int64_t n, int precision,
+                            const double* g_phi, const double* g_force, double* g_xyz,
+                            void* workspace, size_t workspace_bytes, void* stream)
+{
+    g_vjp_phi = g_phi;
+    g_vjp_force = g_force;
+    const int rc = eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, AGB_MODE_VJP, precision,
+                             nullptr, g_xyz, nullptr, nullptr, 0, workspace, workspace_bytes,
+                             workspace == nullptr, stream);
+    g_vjp_phi = nullptr;
+    g_vjp_force = nullptr;
+    return rc;
 }
 
 extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_leaf* leaves,

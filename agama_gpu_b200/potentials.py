@@ -142,11 +142,8 @@ class _GPUPotBase:
         return self
 
     # -- evaluation core ----------------------------------------------------
-    def _launch(self, arr: torch.Tensor, t: float, mode: int, want_phi: bool,
-                precision: Optional[str] = None, out=None):
-        n = arr.shape[0]
-        dev = arr.device
-        prec = _PRECISIONS[precision or self.precision or _default_precision]
+    def _c_args(self, t: float, dev: torch.device):
+        """(component array, n_comps, leaf array, n_leaves) of the tree at time t."""
         leaves = self._leaves(float(t))
         if not leaves:
             raise ValueError("potential has no components")
@@ -166,7 +163,22 @@ class _GPUPotBase:
             lf.sigma = sigma
             lf.gamma[0], lf.gamma[1], lf.gamma[2] = float(gamma[0]), float(gamma[1]), float(gamma[2])
             lf.ampl = ampl
-        comp_arr = (_lib.AgbComponent * len(comps))(*comps)
+        return (_lib.AgbComponent * len(comps))(*comps), len(comps), leaf_arr, len(leaves)
+
+    def _flags(self) -> int:
+        return _lib.OUT_NEGATE | (0 if self.binning else _lib.OUT_NO_BINNING)
+
+    def _workspace(self, cargs, n: int, dev: torch.device):
+        nws = int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3], n,
+                                                    self._flags()))
+        return (torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None), nws
+
+    def _launch(self, arr: torch.Tensor, t: float, mode: int, want_phi: bool,
+                precision: Optional[str] = None, out=None):
+        n = arr.shape[0]
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        cargs = self._c_args(t, dev)
         f64 = dict(dtype=torch.float64, device=dev)
         phi = grad = hess = rho = None
         if out is not None:
@@ -185,14 +197,33 @@ class _GPUPotBase:
             return phi, grad, hess, rho
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         stream = torch.cuda.current_stream(dev).cuda_stream
-        flags = _lib.OUT_NEGATE | (0 if self.binning else _lib.OUT_NO_BINNING)
-        nws = _lib.lib.agb_eval_workspace_bytes(comp_arr, len(comps), leaf_arr, len(leaves), n, flags)
-        ws = torch.empty(int(nws), dtype=torch.uint8, device=dev) if nws else None
-        rc = _lib.lib.agb_eval_ws(comp_arr, len(comps), leaf_arr, len(leaves), arr.data_ptr(), n,
-                                  mode, prec, ptr(phi), ptr(grad), ptr(hess), ptr(rho), flags,
-                                  ptr(ws), int(nws), ctypes.c_void_p(stream))
+        ws, nws = self._workspace(cargs, n, dev)
+        rc = _lib.lib.agb_eval_ws(*cargs, arr.data_ptr(), n, mode, prec, ptr(phi), ptr(grad),
+                                  ptr(hess), ptr(rho), self._flags(), ptr(ws), nws,
+                                  ctypes.c_void_p(stream))
         _lib.check(rc, "agb_eval_ws")
         return phi, grad, hess, rho
+
+    def _vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
+             g_force: Optional[torch.Tensor], precision: Optional[str] = None,
+             out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """dL/dx = g_phi * grad(Phi) - H g_force for cotangents of (Phi, force)."""
+        n = arr.shape[0]
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        gx = out if out is not None else torch.empty((n, 3), dtype=torch.float64, device=dev)
+        if n == 0:
+            return gx
+        cargs = self._c_args(t, dev)
+        gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
+        gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+        ws, nws = self._workspace(cargs, n, dev)
+        rc = _lib.lib.agb_eval_vjp(*cargs, arr.data_ptr(), n, prec, ptr(gp), ptr(gf), gx.data_ptr(),
+                                   ptr(ws), nws,
+                                   ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        _lib.check(rc, "agb_eval_vjp")
+        return gx
 
     # -- public API (gpu_potential.py:826-935) --------------------------------
     def potential(self, xyz, t: float = 0.0):

@@ -46,6 +46,7 @@ extern "C" {
 #define AGB_MODE_GRAD  1   /* Phi and grad Phi                        */
 #define AGB_MODE_HESS  2   /* Phi, grad Phi and the Hessian           */
 #define AGB_MODE_DENS  3   /* density = Laplacian(Phi) / (4 pi G)     */
+#define AGB_MODE_VJP   4   /* dL/dx from dL/dPhi and dL/dF (agb_eval_vjp) */
 
 /* arithmetic of the Multipole harmonic sums */
 #define AGB_PREC_FP64  0   /* everything FP64                                      */
@@ -191,6 +192,21 @@ int agb_eval_ws(const agb_component* comps, int n_comps,
                 const double* xyz, int64_t n, int mode, int precision,
                 double* phi, double* grad, double* hess, double* rho,
                 int out_flags, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Vector-Jacobian product of the composite w.r.t. positions (the backward of
+ * a potential/force evaluation):  g_xyz = g_phi * grad(Phi) - H g_force,
+ * H the Hessian of Phi (F = -grad Phi, dF/dx = -H).  One fused launch: every
+ * component is evaluated with its Hessian and the contraction happens per
+ * point, H is never written.  g_phi [N] and g_force [N,3] may be NULL (zero).
+ * workspace as for agb_eval_ws (NULL: allocated stream-ordered inside).
+ * No counterpart in the reference (it has no derivatives w.r.t. inputs).
+ */
+int agb_eval_vjp(const agb_component* comps, int n_comps,
+                 const agb_leaf* leaves, int n_leaves,
+                 const double* xyz, int64_t n, int precision,
+                 const double* g_phi, const double* g_force, double* g_xyz,
+                 void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * agb_eval_static -- agb_eval that allocates nothing.  No counterpart in the

@@ -1,0 +1,190 @@
+"""Derivatives: position VJP (fused Hessian contraction), autograd Function,
+leapfrog forward (eager and CUDA-graph) and its checkpointed adjoint, checked
+against central finite differences and the oracle."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from helpers import cs_coefs
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _composite(static=True):
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import circular_track, nfw_multipole
+    parts = [agb.MultipolePotentialGPU(nfw_multipole(lmax=6, n_nodes=40, seed=2)),
+             agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3),
+             agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))]
+    if not static:
+        parts.append(agb.ShiftedPotentialGPU(agb.NFWPotentialGPU(mass=2e11, scaleRadius=8.0),
+                                             circular_track(T=100, radius=40.0)))
+    return agb.CompositePotentialGPU(parts)
+
+
+def _pts(n, seed, lo=0.3, hi=60.0):
+    rng = np.random.default_rng(seed)
+    r = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+    u = rng.normal(size=(n, 3))
+    return u / np.linalg.norm(u, axis=1)[:, None] * r[:, None]
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-6), ("mixed", 5e-5)])
+def test_vjp_matches_finite_differences(prec, tol):
+    import torch
+    pot = _composite(static=False)
+    xyz = _pts(400, 1)
+    # the CylSpline grid starts at R = 0.1: inside that the reference's outer
+    # asymptote (gradient without its theta term) is not the derivative of its Phi
+    xyz = xyz[np.hypot(xyz[:, 0], xyz[:, 1]) > 0.2][:300]
+    rng = np.random.default_rng(2)
+    gphi = rng.normal(size=300)
+    gf = rng.normal(size=(300, 3))
+    x = torch.from_numpy(xyz).cuda()
+    gx = pot._vjp(x, 0.4, torch.from_numpy(gphi).cuda(), torch.from_numpy(gf).cuda(),
+                  precision=prec).cpu().numpy()
+
+    def L(xx):
+        p, f, _, _ = pot._launch(torch.from_numpy(xx).cuda(), 0.4, 1, True, precision="fp64")
+        return (p.cpu().numpy() * gphi) + np.sum(f.cpu().numpy() * gf, axis=1)
+
+    fd = np.zeros_like(xyz)
+    for d in range(3):
+        h = 1e-5 * np.maximum(np.linalg.norm(xyz, axis=1), 1.0)
+        e = np.zeros_like(xyz)
+        e[:, d] = h
+        fd[:, d] = (L(xyz + e) - L(xyz - e)) / (2 * h)
+    err = np.abs(gx - fd).max() / np.abs(fd).max()
+    assert err < tol, err
+
+
+def _exact_cyl_correction(pot, xyz, t):
+    """The terms dPhi/dphi d2(phi)/dx_i dx_j that the reference's CylSpline Hessian
+    omits, from the oracle's Phi by central differences in phi (for the check)."""
+    from agama_gpu_b200 import _lib
+    corr = np.zeros((len(xyz), 6))
+    for comp, sigma, gamma, ampl in pot._leaves(t):
+        if comp.kind != _lib.KIND_CYLSPLINE:
+            continue
+        x = sigma * xyz - np.asarray(gamma)[None, :]
+        R2 = x[:, 0] ** 2 + x[:, 1] ** 2
+        ph = np.arctan2(x[:, 1], x[:, 0])
+        R = np.sqrt(R2)
+        dph = 1e-5
+        def rot(a):
+            return np.stack([R * np.cos(ph + a), R * np.sin(ph + a), x[:, 2]], 1)
+        Pp = (cpu.eval_component(comp, 0, rot(dph))[0] - cpu.eval_component(comp, 0, rot(-dph))[0]) / (2 * dph)
+        xy, d = x[:, 0] * x[:, 1], R2 * R2
+        f = ampl * sigma * sigma
+        corr[:, 0] += f * 2 * Pp * xy / d
+        corr[:, 1] -= f * 2 * Pp * xy / d
+        corr[:, 3] += f * Pp * (x[:, 1] ** 2 - x[:, 0] ** 2) / d
+    return corr
+
+
+def test_vjp_matches_oracle_hessian():
+    import torch
+    pot = _composite(static=False)
+    xyz = _pts(30_000, 3, 0.3, 120.0)
+    xyz = xyz[np.hypot(xyz[:, 0], xyz[:, 1]) > 0.2][:20_000]     # inside the CylSpline grid
+    rng = np.random.default_rng(4)
+    gphi, gf = rng.normal(size=20_000), rng.normal(size=(20_000, 3))
+    gx = pot._vjp(torch.from_numpy(xyz).cuda(), 0.7, torch.from_numpy(gphi).cuda(),
+                  torch.from_numpy(gf).cuda(), precision="fp64").cpu().numpy()
+    _, g, h, _ = cpu.eval_potential(pot, 2, xyz, 0.7)
+    h = h + _exact_cyl_correction(pot, xyz, 0.7)
+    H = np.zeros((len(xyz), 3, 3))
+    for q, (i, j) in enumerate([(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)]):
+        H[:, i, j] = H[:, j, i] = h[:, q]
+    ref = gphi[:, None] * g - np.einsum("nij,nj->ni", H, gf)
+    assert np.abs(gx - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+def test_autograd_function():
+    import torch
+    from agama_gpu_b200.autograd import potential_and_force
+    pot = _composite()
+    x = torch.from_numpy(_pts(500, 5)).cuda().requires_grad_(True)
+    w = torch.randn(500, dtype=torch.float64, device="cuda")
+    u = torch.randn(500, 3, dtype=torch.float64, device="cuda")
+    phi, F = potential_and_force(pot, x)
+    (gx,) = torch.autograd.grad((w * phi).sum() + (u * F).sum(), x)
+    ref = pot._vjp(x.detach(), 0.0, w, u)
+    assert torch.allclose(gx, ref, rtol=0, atol=0)
+    p2, f2 = pot.eval(x.detach(), pot=True, acc=True)
+    assert torch.equal(phi.detach(), p2) and torch.equal(F.detach(), f2)
+
+
+def _disk_ics(n, seed):
+    import torch
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(4, 20, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    x = np.stack([R * np.cos(ph), R * np.sin(ph), rng.normal(0, 0.5, n)], 1)
+    vc = 200.0
+    v = np.stack([-vc * np.sin(ph), vc * np.cos(ph), rng.normal(0, 10, n)], 1)
+    return torch.from_numpy(x).cuda(), torch.from_numpy(v).cuda()
+
+
+@pytest.mark.parametrize("static", [True, False])
+def test_leapfrog_adjoint_matches_finite_differences(static):
+    import torch
+    from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
+    pot = _composite(static=static)
+    x0, v0 = _disk_ics(16, 7)
+    target = x0 + 1.0
+    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64")
+    n_steps = 90
+
+    def loss(xx, vv):
+        xT, vT, _ = integ.run(xx, vv, n_steps, checkpoint_every=16)
+        return float(((xT - target) ** 2).sum())
+
+    xT, vT, ck = integ.run(x0, v0, n_steps, checkpoint_every=16)
+    lx, lv = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT))
+    rng = np.random.default_rng(0)
+    for (p, d) in [(int(rng.integers(16)), int(rng.integers(3))) for _ in range(6)]:
+        for which, lam, h in (("x", lx, 1e-4), ("v", lv, 1e-3)):
+            xp, vp = x0.clone(), v0.clone()
+            xm, vm = x0.clone(), v0.clone()
+            if which == "x":
+                xp[p, d] += h; xm[p, d] -= h
+            else:
+                vp[p, d] += h; vm[p, d] -= h
+            fd = (loss(xp, vp) - loss(xm, vm)) / (2 * h)
+            an = float(lam[p, d])
+            assert abs(an - fd) <= 1e-5 * max(abs(fd), 1e-3 * float(lam.abs().max())), (which, an, fd)
+
+
+def test_leapfrog_graph_replay_equals_eager():
+    import torch
+    from agama_gpu_b200.integrate import Leapfrog
+    pot = _composite(static=True)
+    x0, v0 = _disk_ics(5000, 9)
+    a = Leapfrog(pot, 0.001, use_graph=True, graph_steps=8)
+    b = Leapfrog(pot, 0.001, use_graph=False)
+    assert a.use_graph and not b.use_graph
+    xa, va, _ = a.run(x0, v0, 40, checkpoint_every=64)
+    xb, vb, _ = b.run(x0, v0, 40, checkpoint_every=64)
+    assert torch.equal(xa, xb) and torch.equal(va, vb)
+    xa2, _, _ = a.run(x0, v0, 40, checkpoint_every=64)     # graph reused on a second run
+    assert torch.equal(xa2, xa)
+
+
+def test_leapfrog_autograd_wrapper():
+    import torch
+    from agama_gpu_b200.integrate import leapfrog
+    pot = _composite(static=True)
+    x0, v0 = _disk_ics(64, 11)
+    x0.requires_grad_(True)
+    v0.requires_grad_(True)
+    xT, vT = leapfrog(pot, x0, v0, 0.002, 50, checkpoint_every=8)
+    loss = (xT ** 2).sum() + 0.1 * (vT ** 2).sum()
+    gx, gv = torch.autograd.grad(loss, (x0, v0))
+    assert torch.isfinite(gx).all() and torch.isfinite(gv).all()
+    from agama_gpu_b200.integrate import Leapfrog
+    integ = Leapfrog(pot, 0.002)
+    xT2, vT2, ck = integ.run(x0.detach(), v0.detach(), 50, checkpoint_every=8)
+    lx, lv = integ.adjoint(ck, 50, 2 * xT2, 0.2 * vT2)
+    assert torch.allclose(gx, lx, rtol=1e-12, atol=0) and torch.allclose(gv, lv, rtol=1e-12, atol=0)
