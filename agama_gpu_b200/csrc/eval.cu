@@ -16,6 +16,7 @@
 #include "cylspline.cuh"
 #include "analytic.cuh"
 #include "bin.cuh"
+#include "mp_grad.cuh"
 
 // ---------------------------------------------------------------------------
 // errors and launch accounting
@@ -440,6 +441,66 @@ extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_le
 {
     return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
                      rho, out_flags, workspace, workspace_bytes, false, stream);
+}
+
+// ---------------------------------------------------------------------------
+// gradient w.r.t. one Multipole leaf's quintic coefficients
+// ---------------------------------------------------------------------------
+extern "C" size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* comp,
+                                                          const agb_leaf* leaf, int64_t n)
+{
+    if (!comp || !leaf) return 0;
+    agb_leaf l = *leaf;
+    l.comp = 0;
+    return ws_bytes(plan_binning(comp, &l, 1, n, 0), n);
+}
+
+extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
+                                       const double* xyz, int64_t n, const double* g_phi,
+                                       const double* g_force, double* g_table, void* workspace,
+                                       size_t workspace_bytes, void* stream)
+{
+    if (!comp || !leaf || !g_table) return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: null argument");
+    if (comp->kind != AGB_KIND_MULTIPOLE)
+        return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: component is not a Multipole");
+    if (comp->layout != AGB_LAYOUT_INTERVAL_MAJOR)
+        return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: the table must be interval-major");
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: negative point count");
+    if (n == 0) return AGB_OK;
+    if (!xyz) return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: xyz is null");
+    static thread_local MPGradArgs g;
+    memset(&g, 0, sizeof(g));
+    int rc = comp_to_dev(*comp, g.c, AGB_PREC_FP64);
+    if (rc) return rc;
+    g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
+    g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
+    g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force; g.grad = g_table;
+    cudaStream_t st = (cudaStream_t)stream;
+    agb_leaf l = *leaf;
+    l.comp = 0;
+    const BinPlan b = plan_binning(comp, &l, 1, n, 0);
+    const size_t need = ws_bytes(b, n);
+    void* ws = workspace;
+    const bool own = (workspace == nullptr);
+    if (need) {
+        if (own) {
+            if (cudaMallocAsync(&ws, need, st) != cudaSuccess)
+                return set_err(AGB_ERR_DEVICE, "agb_multipole_table_vjp: cannot allocate scratch");
+        } else if (workspace_bytes < need || ((uintptr_t)ws & 255u)) {
+            return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: workspace too small or misaligned");
+        }
+        static thread_local EvalArgs tmp;
+        memset(&tmp, 0, sizeof(tmp));
+        rc = run_binning(tmp, b, xyz, n, (char*)ws, st);
+        g.xyz = tmp.xyz;
+        g.perm = tmp.perm;
+    }
+    if (!rc) {
+        mp_grad_kernel<<<grid_for(n), 256, 0, st>>>(g);
+        rc = check_launch("mp_grad_kernel");
+    }
+    if (need && own) cudaFreeAsync(ws, st);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

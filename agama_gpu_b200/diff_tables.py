@@ -1,0 +1,97 @@
+"""Differentiable construction of the Multipole quintic tables (torch, FP64).
+
+The same steps as prep_multipole.build_multipole_tables -- log-scaling of the
+node values, the tridiagonal system for the quintic's second derivatives,
+the six Horner coefficients per interval -- written with torch operations so
+that a gradient with respect to the coefficients (from the table-VJP kernel)
+can be carried back to the node tables Phi_lm(r_i) and dPhi_lm/dr(r_i).
+
+Held fixed (treated as constants of the tables): the radial grid, invPhi0,
+the inner/outer extrapolation constants, the harmonic set after pruning.
+A grid that had to be resampled to log-uniform is not supported here.
+"""
+from __future__ import annotations
+
+from typing import Tuple
+
+import numpy as np
+import torch
+
+
+def quintic_poly_torch(logr: torch.Tensor, f: torch.Tensor, df: torch.Tensor, h: float) -> torch.Tensor:
+    """(n_cols, n-1, 6) quintic coefficients from values f and log-r slopes df (n, n_cols)."""
+    n = logr.shape[0]
+    ih = 1.0 / (logr[1:] - logr[:-1])                         # (n-1,)
+    A = torch.zeros((n, n), dtype=f.dtype, device=f.device)
+    rhs = torch.zeros_like(f)
+    idx = torch.arange(n, device=f.device)
+    diag = torch.zeros(n, dtype=f.dtype, device=f.device)
+    diag[1:] += 3.0 * ih
+    diag[:-1] += 3.0 * ih
+    A[idx, idx] = diag
+    A[idx[:-1], idx[1:]] = -ih
+    A[idx[1:], idx[:-1]] = -ih
+    w = ih[:, None]
+    left = (20.0 * (f[1:] - f[:-1]) * w - 12.0 * df[1:] - 8.0 * df[:-1]) * w * w   # row i > 0
+    right = (20.0 * (f[1:] - f[:-1]) * w - 12.0 * df[:-1] - 8.0 * df[1:]) * w * w  # row i < n-1
+    rhs = rhs.index_add(0, idx[1:], -left)
+    rhs = rhs.index_add(0, idx[:-1], right)
+    h0, hn = ih[0], ih[-1]
+    A[0, 1] = -2.0 * h0
+    A[n - 1, n - 2] = -2.0 * hn
+    rhs = rhs.clone()
+    rhs[0] = (30.0 * (f[1] - f[0]) * h0 - 14.0 * df[1] - 16.0 * df[0]) * h0 * h0
+    rhs[n - 1] = (-30.0 * (f[n - 1] - f[n - 2]) * hn + 14.0 * df[n - 2] + 16.0 * df[n - 1]) * hn * hn
+    d2f = torch.linalg.solve(A, rhs)
+    f0, f1 = f[:-1], f[1:]
+    m0, m1 = df[:-1] * h, df[1:] * h
+    q0, q1 = d2f[:-1] * (h * h), d2f[1:] * (h * h)
+    dd = f1 - f0
+    a = torch.stack([f0, m0, 0.5 * q0,
+                     10.0 * dd - 6.0 * m0 - 4.0 * m1 - 1.5 * q0 + 0.5 * q1,
+                     -15.0 * dd + 8.0 * m0 + 7.0 * m1 + 1.5 * q0 - q1,
+                     6.0 * dd - 3.0 * m0 - 3.0 * m1 + 0.5 * (q1 - q0)], dim=-1)
+    return a.permute(1, 0, 2)
+
+
+def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) -> torch.Tensor:
+    """Quintic coefficients (n_lm, n_int, 6) from node tables (nR, n_lm) in the
+    builder's harmonic order (``tables.node_phi`` layout); differentiable."""
+    if tables.resampled:
+        raise ValueError("node gradients need a log-uniform input grid (this one was resampled)")
+    dev = phi.device
+    r = torch.as_tensor(tables.r_grid, dtype=torch.float64, device=dev)
+    logr = torch.log(r)
+    dphi_dlogr = dphi_dr * r[:, None]
+    if tables.log_scaling:
+        p0 = phi[:, 0]
+        inv = float(tables.invPhi0)
+        f0 = torch.log(inv - 1.0 / p0)
+        df0 = dphi_dlogr[:, 0] / (p0 * (inv * p0 - 1.0))
+        ratio = phi[:, 1:] / p0[:, None]
+        dfc = (dphi_dlogr[:, 1:] - ratio * dphi_dlogr[:, 0:1]) / p0[:, None]
+        f = torch.cat([f0[:, None], ratio], dim=1)
+        df = torch.cat([df0[:, None], dfc], dim=1)
+    else:
+        f, df = phi, dphi_dlogr
+    return quintic_poly_torch(logr, f, df, float(tables.dlogr))
+
+
+def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Carry dL/dpoly back to the node tables in the coefficient file's column order.
+
+    Returns (dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_cols); columns
+    the table builder pruned (all-zero) get zero (build with prune_threshold=0
+    to differentiate every harmonic).
+    """
+    dev = grad_poly.device
+    phi = torch.tensor(tables.node_phi, dtype=torch.float64, device=dev, requires_grad=True)
+    dphi = torch.tensor(tables.node_dphi_dr, dtype=torch.float64, device=dev, requires_grad=True)
+    poly = multipole_poly_from_nodes(tables, phi, dphi)
+    gphi, gdphi = torch.autograd.grad(poly, (phi, dphi), grad_outputs=grad_poly.to(torch.float64))
+    cols = torch.as_tensor(np.asarray(tables.node_cols), dtype=torch.long, device=dev)
+    out_p = torch.zeros((phi.shape[0], n_file_cols), dtype=torch.float64, device=dev)
+    out_d = torch.zeros_like(out_p)
+    out_p[:, cols] = gphi
+    out_d[:, cols] = gdphi
+    return out_p, out_d

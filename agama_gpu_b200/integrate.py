@@ -143,8 +143,14 @@ class Leapfrog:
 
     # -- adjoint -----------------------------------------------------------------------
     def adjoint(self, ckpts: List, n_steps: int, lam_x: torch.Tensor,
-                lam_v: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
-        """(dL/dx0, dL/dv0) from (dL/dx_T, dL/dv_T) and the forward's checkpoints."""
+                lam_v: torch.Tensor, table_grads: bool = False):
+        """(dL/dx0, dL/dv0) from (dL/dx_T, dL/dv_T) and the forward's checkpoints.
+
+        With table_grads=True also returns {Multipole component: dL/dpoly}, the
+        gradient with respect to each Multipole's quintic coefficients summed over
+        all force evaluations (component.node_gradients() carries it to the nodes).
+        """
+        tg = {} if table_grads else None
         lx = lam_x.detach().to(torch.float64).contiguous().clone()
         lv = lam_v.detach().to(torch.float64).contiguous().clone()
         pending = None                      # cotangent on F(x_n) from the later half-kick
@@ -168,13 +174,19 @@ class Leapfrog:
                     gF.add_(pending)
                 self.pot._vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
                               precision=self.precision, out=gx)
+                if tg is not None:
+                    self.pot._table_vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF, tg)
                 lx.add_(gx)
                 lv.add_(lx, alpha=self.dt)
                 pending = lv * self.h
         if pending is not None:
             _, x0, _ = ckpts[0]
             self.pot._vjp(x0, self.t0, None, pending, precision=self.precision, out=gx)
+            if tg is not None:
+                self.pot._table_vjp(x0, self.t0, None, pending, tg)
             lx.add_(gx)
+        if tg is not None:
+            return lx, lv, tg
         return lx, lv
 
 

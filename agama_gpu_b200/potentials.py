@@ -225,6 +225,21 @@ class _GPUPotBase:
         _lib.check(rc, "agb_eval_vjp")
         return gx
 
+    def _table_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
+                   g_force: Optional[torch.Tensor], acc: Optional[dict] = None) -> dict:
+        """dL/dpoly of every Multipole in the tree: {component: (n_lm, n_int, 6)}, summed
+        over the leaves that use it and added into ``acc`` when given."""
+        acc = {} if acc is None else acc
+        for comp, sigma, gamma, ampl in self._leaves(float(t)):
+            if comp.kind != _lib.KIND_MULTIPOLE:
+                continue
+            g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
+            if comp in acc:
+                acc[comp].add_(g)
+            else:
+                acc[comp] = g
+        return acc
+
     # -- public API (gpu_potential.py:826-935) --------------------------------
     def potential(self, xyz, t: float = 0.0):
         """Phi in (km/s)^2: (N,) or a 0-d tensor for one point."""
@@ -316,10 +331,25 @@ class MultipolePotentialGPU(_Component):
 
     def __init__(self, coefs, prune_threshold: float = 1e-16) -> None:
         self.tables = build_multipole_tables(coefs, prune_threshold=prune_threshold)
+        self._n_file_cols = len(coefs.lm_labels)
         t = self.tables
         self._structure, reg = t.regular()
         poly = t.poly if reg is None else reg
         self._n_cols = poly.shape[0]
+        # device column of each of the builder's harmonics (identity for the list layout)
+        if reg is None:
+            self._col_of = np.arange(t.n_lm)
+        else:
+            cols = {}
+            even = self._structure == _lib.STRUCT_EVEN
+            for am in range(t.lmax + 1):
+                for l in range(am, t.lmax + 1):
+                    if even and l % 2:
+                        continue
+                    cols[(l, am)] = len(cols)
+                    if am > 0:
+                        cols[(l, -am)] = len(cols)
+            self._col_of = np.array([cols[(int(l), int(m))] for l, m in zip(t.lm_l, t.lm_m)])
         self._poly_im = np.ascontiguousarray(poly.transpose(1, 0, 2))
         p32 = np.zeros((t.n_int, self._n_cols, 8), dtype=np.float32)
         p32[:, :, :6] = self._poly_im.astype(np.float32)
@@ -352,6 +382,54 @@ class MultipolePotentialGPU(_Component):
                 os.unlink(tmp)
             except FileNotFoundError:
                 pass
+
+    def table_vjp(self, xyz: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
+                  g_force: Optional[torch.Tensor], leaf=None) -> torch.Tensor:
+        """dL/dpoly (n_lm, n_int, 6) of this Multipole, in the layout of ``tables.poly``.
+
+        g_phi (N,) and g_force (N,3) are cotangents of the potential and force of
+        the tree this component belongs to; ``leaf`` = (sigma, gamma, ampl) of the
+        component in that tree (default: the component on its own).  FP64.
+        Points outside the radial grid contribute nothing: the extrapolation
+        constants (and invPhi0) are held fixed.
+        """
+        dev = xyz.device
+        comp = self._device_component(dev)
+        lf = _lib.AgbLeaf()
+        sigma, gamma, ampl = leaf if leaf is not None else (1.0, np.zeros(3), 1.0)
+        lf.comp = 0
+        lf.sigma = float(sigma)
+        lf.gamma[0], lf.gamma[1], lf.gamma[2] = (float(g) for g in gamma)
+        lf.ampl = float(ampl)
+        n = xyz.shape[0]
+        g = torch.zeros((self.tables.n_int, self._n_cols, 6), dtype=torch.float64, device=dev)
+        if n:
+            arr = xyz.to(dtype=torch.float64).contiguous()
+            gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
+            gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
+            nws = int(_lib.lib.agb_multipole_table_vjp_workspace_bytes(ctypes.byref(comp),
+                                                                       ctypes.byref(lf), n))
+            ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
+            ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+            rc = _lib.lib.agb_multipole_table_vjp(
+                ctypes.byref(comp), ctypes.byref(lf), arr.data_ptr(), n, ptr(gp), ptr(gf),
+                g.data_ptr(), ptr(ws), nws,
+                ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+            _lib.check(rc, "agb_multipole_table_vjp")
+        cols = torch.from_numpy(self._col_of).to(dev)
+        return g.index_select(1, cols).permute(1, 0, 2).contiguous()
+
+    def node_gradients(self, grad_poly: torch.Tensor):
+        """(dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_columns), from dL/dpoly.
+
+        Chains through a differentiable restatement of the table construction
+        (diff_tables); invPhi0 and the extrapolation constants are held fixed.
+        """
+        from .diff_tables import node_vjp
+        n_file = int(max(self.tables.node_cols)) + 1 if self._n_file_cols is None else self._n_file_cols
+        return node_vjp(self.tables, grad_poly, n_file)
+
+    _n_file_cols = None
 
     def _upload(self, dev):
         t = self.tables

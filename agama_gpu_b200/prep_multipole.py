@@ -53,6 +53,10 @@ class MultipoleTables:
     outer_U: float
     outer_W: float
     r_grid: np.ndarray
+    node_phi: np.ndarray = None      # (nR, n_lm) Phi at the nodes, builder's harmonic order
+    node_dphi_dr: np.ndarray = None  # (nR, n_lm) dPhi/dr at the nodes
+    node_cols: np.ndarray = None     # (n_lm,) column of each harmonic in the coefficient file
+    resampled: bool = False          # the input grid was not log-uniform and was resampled
 
     @property
     def n_lm(self) -> int:
@@ -264,7 +268,8 @@ def build_multipole_tables(coefs, prune_threshold: float = 1e-16) -> MultipoleTa
     dphi_dlogr = dphi_dr * r[:, None]
     d0_dr = dphi_dr[:, 0]
 
-    if spread > 1e-3:
+    resampled = spread > 1e-3
+    if resampled:
         n_new = max(nR, 1000)
         logr_new = np.linspace(logr[0], logr[-1], n_new)
         r_new = np.exp(logr_new)
@@ -292,6 +297,7 @@ def build_multipole_tables(coefs, prune_threshold: float = 1e-16) -> MultipoleTa
     order = np.lexsort((lm_m < 0, lm_l, np.abs(lm_m)))
     lm_l, lm_m = lm_l[order], lm_m[order]
     phi, dphi_dlogr = phi[:, order], dphi_dlogr[:, order]
+    cols = order.copy()
 
     keep = np.ones(n_lm, dtype=bool)
     if prune_threshold > 0:
@@ -299,6 +305,7 @@ def build_multipole_tables(coefs, prune_threshold: float = 1e-16) -> MultipoleTa
     if not keep.all():
         phi, dphi_dlogr = phi[:, keep], dphi_dlogr[:, keep]
         lm_l, lm_m = lm_l[keep], lm_m[keep]
+        cols = cols[keep]
         lmax = int(lm_l.max())
 
     p0 = phi[:, 0]
@@ -323,4 +330,6 @@ def build_multipole_tables(coefs, prune_threshold: float = 1e-16) -> MultipoleTa
                            log_scaling=int(log_scaling), invPhi0=float(invPhi0),
                            inner_s=float(in_s), inner_U=float(in_U), inner_W=float(in_W),
                            outer_s=float(out_s), outer_U=float(out_U), outer_W=float(out_W),
-                           r_grid=r)
+                           r_grid=r, node_phi=np.ascontiguousarray(phi),
+                           node_dphi_dr=np.ascontiguousarray(dphi_dlogr / r[:, None]),
+                           node_cols=cols, resampled=bool(resampled))

@@ -209,6 +209,25 @@ int agb_eval_vjp(const agb_component* comps, int n_comps,
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Gradient of a loss with respect to one Multipole leaf's quintic coefficients
+ * (the table half of the backward): accumulates into g_table, laid out like the
+ * component's interval-major FP64 table [n_int][n_lm][6], the sum over points
+ * of dL/da_{c,k,j} for cotangents g_phi [N] (dL/dPhi) and g_force [N,3]
+ * (dL/dF) of the composite's outputs; leaf gives the component's transform.
+ * Points outside the radial grid contribute nothing (the extrapolation
+ * constants are held fixed).  FP64; points are sorted by interval in scratch
+ * (workspace as for agb_eval_ws, NULL: allocated stream-ordered inside) and
+ * each warp reduces its lanes before one atomic add per coefficient.
+ * No counterpart in the reference.
+ */
+size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* comp,
+                                               const agb_leaf* leaf, int64_t n);
+int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
+                            const double* xyz, int64_t n, const double* g_phi,
+                            const double* g_force, double* g_table,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * agb_eval_static -- agb_eval that allocates nothing.  No counterpart in the
  * reference: it exists for callers that may not allocate device memory (a
  * code that reserved the GPU for its own pools, a loop that must not pay

@@ -188,3 +188,114 @@ def test_leapfrog_autograd_wrapper():
     xT2, vT2, ck = integ.run(x0.detach(), v0.detach(), 50, checkpoint_every=8)
     lx, lv = integ.adjoint(ck, 50, 2 * xT2, 0.2 * vT2)
     assert torch.allclose(gx, lx, rtol=1e-12, atol=0) and torch.allclose(gv, lv, rtol=1e-12, atol=0)
+
+
+def _mp_variants():
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    reg = agb.MultipolePotentialGPU(nfw_multipole(lmax=6, n_nodes=30, seed=3, amp=0.3))
+    c = nfw_multipole(lmax=5, n_nodes=30, seed=4, amp=0.3)
+    c.phi[:, 3] = c.phi[:, 7] * 0.5 + 1.0      # odd l present: every-l structure
+    c.dphi_dr[:, 3] = c.dphi_dr[:, 7] * 0.5
+    lst = agb.MultipolePotentialGPU(c)
+    t = lst.tables
+    lst._structure, lst._n_cols = 0, t.n_lm
+    lst._poly_im, lst._poly32 = t.interval_major(), t.interval_major_f32()
+    lst._col_of = np.arange(t.n_lm)
+    return [reg, lst]
+
+
+@pytest.mark.parametrize("which", [0, 1])
+def test_table_vjp_matches_torch_autograd(which):
+    import torch
+    from oracle import torch_mp
+    mp = _mp_variants()[which]
+    tb = mp.tables
+    xyz = _pts(3000, 21, 0.05, 900.0)
+    xyz = xyz[np.hypot(xyz[:, 0], xyz[:, 1]) > 1e-3 * np.linalg.norm(xyz, axis=1)][:2000]
+    sigma, gamma, ampl = 0.8, np.array([0.3, -0.2, 0.1]), 1.7
+    xl = sigma * xyz - gamma
+    r = np.linalg.norm(xl, axis=1)
+    inside = (np.log(r) >= tb.logr_min) & (np.log(r) < tb.logr_min + tb.n_int * tb.dlogr)
+    rng = np.random.default_rng(22)
+    gphi, gf = rng.normal(size=len(xyz)), rng.normal(size=(len(xyz), 3))
+    g = mp.table_vjp(torch.from_numpy(xyz).cuda(), 0.0, torch.from_numpy(gphi).cuda(),
+                     torch.from_numpy(gf).cuda(), leaf=(sigma, gamma, ampl)).cpu().numpy()
+    # the same loss through torch autograd: Phi = A phi(x'), F = -dPhi/dx
+    poly = torch.tensor(tb.poly, dtype=torch.float64, requires_grad=True)
+    x = torch.tensor(xyz[inside], dtype=torch.float64, requires_grad=True)
+    xl_t = sigma * x - torch.as_tensor(gamma)
+    phi = ampl * torch_mp.multipole_phi(poly, tb.lm_l, tb.lm_m, tb.scalars(), tb.log_scaling, xl_t)
+    (dphi,) = torch.autograd.grad(phi.sum(), x, create_graph=True)
+    L = (torch.as_tensor(gphi[inside]) * phi).sum() - (torch.as_tensor(gf[inside]) * dphi).sum()
+    (ref,) = torch.autograd.grad(L, poly)
+    ref = ref.numpy()
+    assert np.abs(g - ref).max() <= 1e-10 * np.abs(ref).max(), np.abs(g - ref).max() / np.abs(ref).max()
+
+
+def test_node_gradients_match_finite_differences():
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    coefs = nfw_multipole(lmax=4, n_nodes=25, seed=5, amp=0.3)
+    pot = agb.MultipolePotentialGPU(coefs)
+    xyz = _pts(4000, 23, 0.05, 200.0)
+    rng = np.random.default_rng(24)
+    gphi, gf = rng.normal(size=len(xyz)), rng.normal(size=(len(xyz), 3))
+    x = torch.from_numpy(xyz).cuda()
+
+    def loss(c):
+        p = agb.MultipolePotentialGPU(c)
+        ph, f, _, _ = p._launch(x, 0.0, 1, True, precision="fp64")
+        return float((ph.cpu().numpy() * gphi).sum() + (f.cpu().numpy() * gf).sum())
+
+    gpoly = pot.table_vjp(x, 0.0, torch.from_numpy(gphi).cuda(), torch.from_numpy(gf).cuda())
+    gnp, gnd = (a.cpu().numpy() for a in pot.node_gradients(gpoly))
+    lab = coefs.lm_labels
+    checks = [(2, lab.index((0, 0))), (10, lab.index((0, 0))), (7, lab.index((2, 1))),
+              (15, lab.index((4, -3))), (20, lab.index((2, 0)))]
+    for i, c in checks:
+        for which, G in (("phi", gnp), ("dphi", gnd)):
+            tab = coefs.phi if which == "phi" else coefs.dphi_dr
+            h = 1e-5 * np.abs(tab[:, c]).max()       # step on the column's scale
+            cp_ = agb.MultipoleCoefs(coefs.R_grid, coefs.phi.copy(), coefs.dphi_dr.copy(), lab)
+            cm_ = agb.MultipoleCoefs(coefs.R_grid, coefs.phi.copy(), coefs.dphi_dr.copy(), lab)
+            (cp_.phi if which == "phi" else cp_.dphi_dr)[i, c] += h
+            (cm_.phi if which == "phi" else cm_.dphi_dr)[i, c] -= h
+            fd = (loss(cp_) - loss(cm_)) / (2 * h)
+            assert abs(G[i, c] - fd) <= 1e-5 * max(abs(fd), 1e-4 * np.abs(G).max()), (which, i, c, G[i, c], fd)
+
+
+def test_leapfrog_table_gradients():
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    coefs = nfw_multipole(lmax=4, n_nodes=30, seed=8, amp=0.3)
+    mn = agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3)
+    x0, v0 = _disk_ics(24, 12)
+    target = x0 * 1.1
+
+    def run(c, want=False):
+        mp = agb.MultipolePotentialGPU(c)
+        integ = Leapfrog(mp + mn, 0.002, precision="fp64")
+        xT, vT, ck = integ.run(x0, v0, 60, checkpoint_every=16)
+        Lv = float(((xT - target) ** 2).sum())
+        if not want:
+            return Lv
+        lx, lv, tg = integ.adjoint(ck, 60, 2 * (xT - target), torch.zeros_like(vT), table_grads=True)
+        return Lv, mp, tg[mp]
+
+    _, mp, gpoly = run(coefs, True)
+    gnp, gnd = (a.cpu().numpy() for a in mp.node_gradients(gpoly))
+    lab = coefs.lm_labels
+    for i, c in [(12, lab.index((0, 0))), (14, lab.index((2, 2))), (9, lab.index((4, 0)))]:
+        for which, G in (("phi", gnp), ("dphi", gnd)):
+            tab = coefs.phi if which == "phi" else coefs.dphi_dr
+            h = 1e-5 * np.abs(tab[:, c]).max()
+            cp_ = agb.MultipoleCoefs(coefs.R_grid, coefs.phi.copy(), coefs.dphi_dr.copy(), lab)
+            cm_ = agb.MultipoleCoefs(coefs.R_grid, coefs.phi.copy(), coefs.dphi_dr.copy(), lab)
+            (cp_.phi if which == "phi" else cp_.dphi_dr)[i, c] += h
+            (cm_.phi if which == "phi" else cm_.dphi_dr)[i, c] -= h
+            fd = (run(cp_) - run(cm_)) / (2 * h)
+            assert abs(G[i, c] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(G).max()), (which, i, c, G[i, c], fd)
