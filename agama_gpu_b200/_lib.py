@@ -98,6 +98,11 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
         ctypes.c_void_p]
+    lib.agb_multipole_adjoint.restype = ctypes.c_int
+    lib.agb_multipole_adjoint.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_eval_static.restype = ctypes.c_int
     lib.agb_eval_static.argtypes = lib.agb_eval.argtypes
     lib.agb_eval_workspace_bytes.restype = ctypes.c_size_t
@@ -120,6 +125,7 @@ EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
+    "agb_multipole_adjoint",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
     "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
 ]

@@ -8,6 +8,7 @@
 // of one launch per component plus CuPy elementwise passes for shifts, scales,
 // negation, lerps and sums (gpu_potential.py:1439-1918).
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdio.h>
 #include <string.h>
 #include <stdarg.h>
@@ -498,6 +499,83 @@ extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf
     if (!rc) {
         mp_grad_kernel<<<grid_for(n), 256, 0, st>>>(g);
         rc = check_launch("mp_grad_kernel");
+    }
+    if (need && own) cudaFreeAsync(ws, st);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// fused adjoint of one Multipole leaf (position VJP + coefficient gradient)
+// ---------------------------------------------------------------------------
+extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
+                                     const double* xyz, int64_t n, int precision,
+                                     const double* g_phi, const double* g_force, double* g_xyz,
+                                     double* g_table, void* workspace, size_t workspace_bytes,
+                                     void* stream)
+{
+    if (!comp || !leaf || !g_table || !g_xyz)
+        return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: null argument");
+    if (comp->kind != AGB_KIND_MULTIPOLE || comp->layout != AGB_LAYOUT_INTERVAL_MAJOR ||
+        comp->structure == AGB_STRUCT_LIST)
+        return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: needs an interval-major Multipole "
+                       "table with a regular column structure");
+    if (precision != AGB_PREC_FP64 && precision != AGB_PREC_MIXED)
+        return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: unknown precision %d", precision);
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: negative point count");
+    if (n == 0) return AGB_OK;
+    if (!xyz) return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: xyz is null");
+    static thread_local MPAdjArgs g;
+    memset(&g, 0, sizeof(g));
+    int rc = comp_to_dev(*comp, g.c, precision);
+    if (rc) return rc;
+    g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
+    g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
+    g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force;
+    g.gx = g_xyz; g.grad = g_table;
+    cudaStream_t st = (cudaStream_t)stream;
+    agb_leaf l = *leaf;
+    l.comp = 0;
+    const BinPlan b = plan_binning(comp, &l, 1, n, 0);
+    const size_t need = ws_bytes(b, n);
+    void* ws = workspace;
+    const bool own = (workspace == nullptr);
+    if (need) {
+        if (own) {
+            if (cudaMallocAsync(&ws, need, st) != cudaSuccess)
+                return set_err(AGB_ERR_DEVICE, "agb_multipole_adjoint: cannot allocate scratch");
+        } else if (workspace_bytes < need || ((uintptr_t)ws & 255u)) {
+            return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: workspace too small or misaligned");
+        }
+        static thread_local EvalArgs tmp;
+        memset(&tmp, 0, sizeof(tmp));
+        rc = run_binning(tmp, b, xyz, n, (char*)ws, st);
+        g.xyz = tmp.xyz;
+        g.perm = tmp.perm;
+    }
+    if (!rc) {
+        // staged accumulation when 8 warps' slices of n_lm x 6 doubles fit in shared memory
+        int grid = grid_for(n);
+        size_t smem = (size_t)8 * (size_t)g.c.n_lm * 6 * sizeof(double);
+        if (smem <= (size_t)AGB_ADJ_SMEM_MAX) {
+            const long long blocks = std::min<long long>((long long)g_num_sms * 2, (n + 255) / 256);
+            const long long warps = blocks * 8, groups = (n + 31) / 32;
+            g.chunk = ((groups + warps - 1) / warps) * 32;
+            grid = (int)blocks;
+        } else {
+            smem = 0;
+            g.chunk = 0;
+        }
+        const void* fn = precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
+                                                     : (const void*)mp_adjoint_kernel<double>;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            rc = set_err(AGB_ERR_DEVICE, "agb_multipole_adjoint: cannot reserve %zu bytes of shared "
+                         "memory", smem);
+        if (!rc) {
+            if (precision == AGB_PREC_MIXED) mp_adjoint_kernel<float><<<grid, 256, smem, st>>>(g);
+            else mp_adjoint_kernel<double><<<grid, 256, smem, st>>>(g);
+            rc = check_launch("mp_adjoint_kernel");
+        }
     }
     if (need && own) cudaFreeAsync(ws, st);
     return rc;

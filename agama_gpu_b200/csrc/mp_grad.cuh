@@ -52,6 +52,7 @@ struct MPGradArgs {
     const double* gphi;       // [N] or null
     const double* gforce;     // [N,3] or null
     double* grad;             // [n_int][n_lm][6], accumulated
+    long long chunk;          // > 0: points per warp, staged in shared memory
     DevComp c;
     DevLeaf leaf;
 };
@@ -255,4 +256,335 @@ mp_grad_kernel(const __grid_constant__ MPGradArgs a)
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Fused adjoint of one Multipole leaf: position VJP and coefficient gradient in
+// one walk over the harmonics (regular column structures).
+// ---------------------------------------------------------------------------
+
+// Warp reduce-scatter of eight values: lane L returns the warp sum of value
+// 4*b4 + 2*b3 + b2 (b = bits of L); 9 shuffles instead of 40 for eight
+// independent butterflies.
+template <typename T>
+__device__ __forceinline__ T warp_rs8(const T v[8], int lane)
+{
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    T w[4], u[2];
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const T keep = h16 ? v[q + 4] : v[q];
+        const T send = h16 ? v[q] : v[q + 4];
+        w[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    #pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const T keep = h8 ? w[q + 2] : w[q];
+        const T send = h8 ? w[q] : w[q + 2];
+        u[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    T z = (h4 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, h4 ? u[0] : u[1], 4);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    return z;
+}
+
+// add six per-lane gradient values of one column into gk[col][0..5]; when the
+// warp is uniform and sk (the warp's shared-memory accumulator for this
+// interval) is given, the reduced values go there instead of to global memory
+template <typename T>
+__device__ __forceinline__ void grad_emit6(double* __restrict__ gk, double* sk, int col,
+                                           const T v6[6], bool uniform, int lane, bool active)
+{
+    if (uniform) {
+        const T v[8] = {active ? v6[0] : T(0), active ? v6[1] : T(0), active ? v6[2] : T(0),
+                        active ? v6[3] : T(0), active ? v6[4] : T(0), active ? v6[5] : T(0),
+                        T(0), T(0)};
+        const T z = warp_rs8<T>(v, lane);
+        const int idx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+        if ((lane & 3) == 0 && idx < 6) {
+            if (sk) sk[col * 6 + idx] += (double)z;
+            else if (gk) atomicAdd(gk + (long long)col * 6 + idx, (double)z);
+        }
+    } else if (active && gk) {
+        #pragma unroll
+        for (int j = 0; j < 6; ++j) atomicAdd(gk + (long long)col * 6 + j, (double)v6[j]);
+    }
+}
+
+// largest shared-memory reservation of the staged adjoint (8 warps' slices)
+#define AGB_ADJ_SMEM_MAX (200 * 1024)
+
+struct MPAdjArgs {
+    long long n;
+    const double* xyz;        // sorted copy when perm != null
+    const int* perm;
+    const double* gphi;       // [N] or null
+    const double* gforce;     // [N,3] or null
+    double* gx;               // [N,3], accumulated (+=)
+    double* grad;             // [n_int][n_lm][6], accumulated
+    long long chunk;          // > 0: points per warp, staged in shared memory
+    DevComp c;
+    DevLeaf leaf;
+};
+
+template <typename R, int PAR>
+__device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, double cth_d,
+                                            double sth_d, double cph, double sph, R P1, R P2,
+                                            R P3, R P4, double* gbase, double* sk, bool uniform,
+                                            int lane, bool active, MPSums& tot)
+{
+    constexpr int MODE = AGB_MODE_HESS;
+    const bool near_pole = sth_d < 1.0e-10;
+    R sp[6], dw[6], ew[6];
+    sp[0] = R(1); sp[1] = s; sp[2] = s * s; sp[3] = sp[2] * s; sp[4] = sp[2] * sp[2]; sp[5] = sp[4] * s;
+    dw[0] = R(0); dw[1] = R(1); dw[2] = R(2) * s; dw[3] = R(3) * sp[2]; dw[4] = R(4) * sp[3]; dw[5] = R(5) * sp[4];
+    ew[0] = R(0); ew[1] = R(0); ew[2] = R(2); ew[3] = R(6) * s; ew[4] = R(12) * sp[2]; ew[5] = R(20) * sp[3];
+    const R cth = (R)cth_d, sth = (R)sth_d;
+    const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
+    const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
+    const R np1 = near_pole ? R(0) : R(1);
+    const R* rec = MPPtr<R>::base(c, kw) + MPPtr<R>::REC;
+    double cm = 1.0, sm = 0.0, sinpow = 1.0, sinpow_m1 = 0.0;
+    int col = 1;
+    for (int m = 0; m <= c.lmax; ++m) {
+        if (m > 0) {
+            const double t = cm * cph - sm * sph;
+            sm = sm * cph + cm * sph;
+            cm = t;
+            sinpow_m1 = sinpow;
+            sinpow *= sth_d;
+        }
+        int l0 = (PAR == 2) ? (m + (m & 1)) : m;
+        if (m == 0) l0 = PAR;
+        if (l0 > c.lmax) continue;
+        const R q1 = (near_pole && m == 1) ? R(1) : R(0);
+        const R m2 = R(m * m) * inv_sth * inv_sth;
+        const R Tc = (R)cm, Ts = (R)sm, dTc = -R(m) * Ts, dTs = R(m) * Tc;
+        R Pc = (R)(AGB_SEED[m] * sinpow), Pp = R(0), dPp = R(0);
+        R dPc = (m == 0) ? R(0) : ((m == 1) ? (R)(AGB_SEED[1] * cth_d)
+                : (near_pole ? R(0) : (R)((double)m * AGB_SEED[m] * sinpow_m1 * cth_d)));
+        MPCol<R> gc, gs;
+        gc.zero();
+        gs.zero();
+        const int tb = m * AGB_LEG_N;
+        auto step = [&](int L) {
+            const R a = MPConst<R>::alpha(tb + L), b = MPConst<R>::beta(tb + L);
+            const R Pn = fma(a * cth, Pc, -b * Pp);
+            const R dPn = fma(a, fma(cth, dPc, -sth * Pc), -b * dPp);
+            dPp = dPc; dPc = dPn; Pp = Pc; Pc = Pn;
+        };
+        auto acc = [&](int L) {
+            const R ll1 = R(L * (L + 1));
+            const R Pos = fma(Pc, inv_sth, q1 * dPc);
+            const R d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
+            const R base = fma(P3, dPc, P1 * Pc);
+            const R Pq = P4 * Pos;
+            R a[6], v[6];
+            MPPtr<R>::load(rec, a);
+            rec += MPPtr<R>::REC;
+            mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            {
+                const R U = fma(Tc, base, dTc * Pq), V = P2 * Pc * Tc;
+                #pragma unroll
+                for (int j = 0; j < 6; ++j) v[j] = fma(sp[j], U, dw[j] * V);
+                grad_emit6<R>(gbase, sk, col, v, uniform, lane, active);
+                ++col;
+            }
+            if (m > 0) {
+                MPPtr<R>::load(rec, a);
+                rec += MPPtr<R>::REC;
+                mp_col_acc<MODE, R>(gs, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+                const R U = fma(Ts, base, dTs * Pq), V = P2 * Pc * Ts;
+                #pragma unroll
+                for (int j = 0; j < 6; ++j) v[j] = fma(sp[j], U, dw[j] * V);
+                grad_emit6<R>(gbase, sk, col, v, uniform, lane, active);
+                ++col;
+            }
+        };
+        int l = m;
+        while (l < l0) step(++l);
+        acc(l);
+        for (l = l0 + PAR; l <= c.lmax; l += PAR) {
+            if (PAR == 2) step(l - 1);
+            step(l);
+            acc(l);
+        }
+        const double md = (double)m;
+        const double ddTc = -md * sm, ddTs = md * cm;
+        tot.A += (double)gc.V * cm + (double)gs.V * sm;
+        tot.B += (double)gc.VR * cm + (double)gs.VR * sm;
+        tot.D += (double)gc.VRR * cm + (double)gs.VRR * sm;
+        tot.Th += (double)gc.VT * cm + (double)gs.VT * sm;
+        tot.Pos += (double)gc.VP * ddTc + (double)gs.VP * ddTs;
+        tot.Thth += (double)gc.VTT * cm + (double)gs.VTT * sm;
+        tot.BTh += (double)gc.VRT * cm + (double)gs.VRT * sm;
+        tot.Ph += (double)gc.V * ddTc + (double)gs.V * ddTs;
+        tot.Phph += -md * md * ((double)gc.V * cm + (double)gs.V * sm);
+        tot.BPh += (double)gc.VR * ddTc + (double)gs.VR * ddTs;
+        tot.ThPh += (double)gc.VT * ddTc + (double)gs.VT * ddTs;
+    }
+}
+
+// Two ways to schedule the points.  Plain (chunk == 0): grid-stride over warps
+// of 32 points, every uniform warp adding its 6 x n_lm reduced values to the
+// interval's gradient with global atomics.  Staged (chunk > 0): each warp owns
+// `chunk` consecutive (interval-sorted) points and a slice of shared memory of
+// n_lm x 6 doubles; while its points stay in one interval it adds into the
+// slice with plain stores, and it flushes the slice to global memory (one
+// atomic per value) only when the interval changes and at the end.
+template <typename R>
+__global__ void __launch_bounds__(256, 1)
+mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
+{
+    extern __shared__ double agb_adj_smem[];
+    const DevComp& c = a.c;
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const bool staged = a.chunk > 0;
+    const int nval = c.n_lm * 6;
+    double* swarp = staged ? agb_adj_smem + (long long)(threadIdx.x >> 5) * nval : nullptr;
+    long long lo, hi, step;
+    if (staged) {
+        lo = gwarp * a.chunk;
+        hi = lo + a.chunk < a.n ? lo + a.chunk : a.n;
+        step = 32;
+        for (int q = lane; q < nval; q += 32) swarp[q] = 0.0;
+    } else {
+        lo = gwarp * 32;
+        hi = a.n;
+        step = (long long)gridDim.x * blockDim.x;
+    }
+    int cur_k = -1;                      // interval held in swarp
+    auto flush = [&]() {
+        __syncwarp();
+        if (cur_k >= 0) {
+            double* g = a.grad + (long long)cur_k * nval;
+            for (int q = lane; q < nval; q += 32) {
+                const double v = swarp[q];
+                if (v != 0.0) atomicAdd(g + q, v);
+                swarp[q] = 0.0;
+            }
+        }
+        cur_k = -1;
+        __syncwarp();
+    };
+    const double logr_min = c.p[0], dlogr = c.p[1], inv_dlogr = c.p[2], invPhi0 = c.p[3];
+    const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
+    const double A = a.leaf.ampl, sg = a.leaf.sigma;
+    for (long long base = lo; base < hi; base += step) {
+        const long long pos = base + lane;
+        const bool valid = pos < hi;
+        long long i = pos;
+        double px = 0.0, py = 0.0, pz = 1.0, gp = 0.0, gf0 = 0.0, gf1 = 0.0, gf2 = 0.0;
+        if (valid) {
+            i = a.perm ? (long long)a.perm[pos] : pos;
+            px = sg * a.xyz[3 * pos] - a.leaf.g0;
+            py = sg * a.xyz[3 * pos + 1] - a.leaf.g1;
+            pz = sg * a.xyz[3 * pos + 2] - a.leaf.g2;
+            gp = a.gphi ? a.gphi[i] : 0.0;
+            if (a.gforce) { gf0 = a.gforce[3 * i]; gf1 = a.gforce[3 * i + 1]; gf2 = a.gforce[3 * i + 2]; }
+        }
+        const double r2 = px * px + py * py + pz * pz;
+        const double r = sqrt(r2);
+        const double Rc = sqrt(px * px + py * py);
+        int k = -1;
+        double s = 0.0;
+        if (valid && r >= 1.0e-300) {
+            const double logr = log(r);
+            if (logr >= logr_min) {
+                int kk = (int)((logr - logr_min) * inv_dlogr);
+                if (kk < 0) kk = 0;
+                if (kk < c.n_int) {
+                    k = kk;
+                    s = fmin(fmax((logr - (logr_min + kk * dlogr)) * inv_dlogr, 0.0), 1.0);
+                }
+            }
+        }
+        const bool inside = k >= 0;
+        const int kw = inside ? k : 0;
+        const double inv_r = inside ? 1.0 / r : 0.0;
+        const double cth = inside ? pz * inv_r : 1.0;
+        const double sth = inside ? Rc * inv_r : 0.0;
+        const double cph = (Rc > 1.0e-300) ? px / Rc : 1.0;
+        const double sph = (Rc > 1.0e-300) ? py / Rc : 0.0;
+        // monopole and log-scaling factor
+        double c0, c0s, c0ss;
+        mp_quintic0(c, kw, s, c0, c0s, c0ss);
+        const double dc0 = c0s * inv_dlogr, d2c0 = c0ss * inv_dlogr * inv_dlogr;
+        double F = 1.0, dF = 0.0, d2F = 0.0, F1 = 0.0, ex = 0.0, mono, dmono, d2mono;
+        if (c.log_scaling) {
+            ex = exp(c0);
+            F = 1.0 / (invPhi0 - ex);
+            F1 = F * F * ex;
+            dF = F1 * dc0;
+            d2F = F1 * (d2c0 + dc0 * dc0 * F * (invPhi0 + ex));
+            mono = MP0 * F; dmono = MP0 * dF; d2mono = MP0 * d2F;
+        } else {
+            mono = MP0 * c0; dmono = MP0 * dc0; d2mono = MP0 * d2c0;
+        }
+        // weights of the coefficient gradient
+        const double w0 = -A * sg * gf0, w1 = -A * sg * gf1, w2 = -A * sg * gf2;
+        const double inv_r2 = inv_r * inv_r;
+        const double alpha = inside ? gp * A : 0.0;
+        const double br = inside ? (w0 * px + w1 * py + w2 * pz) * inv_r2 : 0.0;
+        const double bt = inside ? (w0 * cth * cph + w1 * cth * sph - w2 * sth) * inv_r : 0.0;
+        const double bp = inside ? (-w0 * sph + w1 * cph) * inv_r : 0.0;
+        const R P1 = (R)(alpha * F + br * dF), P2 = (R)(br * F * inv_dlogr);
+        const R P3 = (R)(bt * F), P4 = (R)(bp * F);
+        const int kmax = __reduce_max_sync(0xffffffffu, k);
+        const bool uniform = __all_sync(0xffffffffu, k == kmax || k < 0);
+        const int kk = uniform ? kmax : k;
+        double* gbase = (kk >= 0) ? a.grad + (long long)kk * c.n_lm * 6 : nullptr;
+        double* sk = nullptr;
+        if (staged && uniform && kk >= 0) {
+            if (kk != cur_k) {
+                flush();
+                cur_k = kk;
+            }
+            sk = swarp;
+        }
+        MPSums t = {};
+        if (c.structure == AGB_STRUCT_EVEN)
+            mp_adj_walk<R, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, sk, uniform, lane, inside, t);
+        else
+            mp_adj_walk<R, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, sk, uniform, lane, inside, t);
+        // monopole column of the coefficient gradient
+        {
+            const double Bp = t.B * inv_dlogr;
+            double v[6];
+            const double sp[6] = {1.0, s, s * s, s * s * s, s * s * s * s, s * s * s * s * s};
+            const double dw[6] = {0.0, 1.0, 2.0 * s, 3.0 * s * s, 4.0 * s * s * s, 5.0 * s * s * s * s};
+            if (c.log_scaling) {
+                const double QF = alpha * (MP0 + t.A) + br * Bp + bt * t.Th + bp * t.Pos;
+                const double QdF = br * (MP0 + t.A);
+                const double dFdc0 = F1 * (1.0 + 2.0 * F * ex) * dc0;
+                #pragma unroll
+                for (int j = 0; j < 6; ++j)
+                    v[j] = QF * F1 * sp[j] + QdF * (dFdc0 * sp[j] + F1 * inv_dlogr * dw[j]);
+            } else {
+                #pragma unroll
+                for (int j = 0; j < 6; ++j) v[j] = alpha * MP0 * sp[j] + br * MP0 * inv_dlogr * dw[j];
+            }
+            grad_emit6<double>(gbase, sk, 0, v, uniform, lane, inside);
+        }
+        if (!valid) continue;
+        // position VJP of this leaf: A sigma (gPhi grad - sigma H gF)
+        PointOut o;
+        o.phi = 0.0; o.rho = 0.0;
+        o.g[0] = o.g[1] = o.g[2] = 0.0;
+        #pragma unroll
+        for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
+        if (inside)
+            mp_finish<AGB_MODE_HESS>(t, inv_dlogr, F, dF, d2F, mono, dmono, d2mono, px, py, pz,
+                                     inv_r, Rc, cth, sth, cph, sph, o);
+        else
+            multipole_point<AGB_MODE_HESS, R>(c, px, py, pz, o);
+        const double As = A * sg, s2 = sg;
+        const double* h = o.h;
+        a.gx[3 * i]     += As * (gp * o.g[0] - s2 * (h[0] * gf0 + h[3] * gf1 + h[5] * gf2));
+        a.gx[3 * i + 1] += As * (gp * o.g[1] - s2 * (h[3] * gf0 + h[1] * gf1 + h[4] * gf2));
+        a.gx[3 * i + 2] += As * (gp * o.g[2] - s2 * (h[5] * gf0 + h[4] * gf1 + h[2] * gf2));
+    }
+    if (staged) flush();
 }

@@ -415,6 +415,88 @@ __device__ __forceinline__ void mp_extrap_out(int MODE_, double p0, double d1, d
     }
 }
 
+// Phi, gradient, Hessian or density of one Multipole point from its harmonic
+// sums, the log-scaling factor F(log r) with its log-r derivatives, the
+// monopole terms and the point's geometry (the conversion of
+// _multipole_potential_kernel.cu:388-409 and :713-799).
+template <int MODE>
+__device__ __forceinline__ void mp_finish(const MPSums& t, double inv_dlogr, double F, double dF,
+                                          double d2F, double mono, double dmono, double d2mono,
+                                          double px, double py, double pz, double inv_r,
+                                          double Rc, double cth, double sth, double cph,
+                                          double sph, PointOut& o)
+{
+    const double Bp = t.B * inv_dlogr;
+    const double Dp = t.D * inv_dlogr * inv_dlogr;
+    o.phi = mono + F * t.A;
+    if (MODE == AGB_MODE_POT) return;
+
+    const double Pr = dmono + F * Bp + dF * t.A;
+    if (MODE == AGB_MODE_DENS) {
+        const double inv_r2 = inv_r * inv_r;
+        const double lap = (d2mono + dmono) * inv_r2
+            + (F * (Dp + Bp - t.L) + dF * (2.0 * Bp + t.A) + d2F * t.A) * inv_r2;
+        o.rho = lap * AGB_INV_4PIG;
+        return;
+    }
+    const double Pth = F * t.Th;
+    const double Pos = F * t.Pos;
+    const double inv_r2 = inv_r * inv_r;
+    o.g[0] = Pr * (px * inv_r2) + Pth * (cth * cph * inv_r) + Pos * (-sph * inv_r);
+    o.g[1] = Pr * (py * inv_r2) + Pth * (cth * sph * inv_r) + Pos * (cph * inv_r);
+    o.g[2] = Pr * (pz * inv_r2) + Pth * (-sth * inv_r);
+    if (MODE != AGB_MODE_HESS) return;
+
+    // second derivatives in (log r, theta, phi)
+    const double Prr = d2mono + F * Dp + 2.0 * dF * Bp + d2F * t.A;
+    const double Pthth = F * t.Thth;
+    const double Prth = F * (t.BTh * inv_dlogr) + dF * t.Th;
+    const double Pph = F * t.Ph;
+    const double Pphph = F * t.Phph;
+    const double Prph = F * (t.BPh * inv_dlogr) + dF * t.Ph;
+    const double Pthph = F * t.ThPh;
+
+    // first and second derivatives of (log r, theta, phi) w.r.t. x, y, z
+    const double inv_R = (Rc > 1.0e-300) ? 1.0 / Rc : 0.0;
+    const double X[3] = {px, py, pz};
+    const double dlr[3] = {px * inv_r2, py * inv_r2, pz * inv_r2};
+    const double dth[3] = {cth * cph * inv_r, cth * sph * inv_r, -sth * inv_r};
+    const double dph[3] = {-sph * inv_R, cph * inv_R, 0.0};
+    const double inv_r3 = inv_r2 * inv_r, inv_r4 = inv_r2 * inv_r2, inv_r5 = inv_r4 * inv_r;
+    const double inv_s = (sth > 1.0e-14) ? 1.0 / sth : 0.0;
+    const double cos3 = cth * inv_s * inv_s * inv_s;
+    // f = cos(theta) = z / r
+    const double df[3] = {-pz * px * inv_r3, -pz * py * inv_r3, inv_r - pz * pz * inv_r3};
+    double d2ph_xx = 0.0, d2ph_xy = 0.0, d2ph_yy = 0.0;
+    if (Rc > 1.0e-14) {
+        const double iR4 = inv_R * inv_R * inv_R * inv_R;
+        d2ph_xx = 2.0 * px * py * iR4;
+        d2ph_xy = (py * py - px * px) * iR4;
+        d2ph_yy = -2.0 * px * py * iR4;
+    }
+    #pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        const int i = hess_i(p), j = hess_j(p);
+        const double dij = (i == j) ? 1.0 : 0.0;
+        const double d2lr = dij * inv_r2 - 2.0 * X[i] * X[j] * inv_r4;
+        // d2 f / dx_i dx_j = -(delta_ij z + delta_iz x_j + delta_jz x_i)/r^3 + 3 z x_i x_j / r^5
+        const double d2f = -(dij * pz + (i == 2 ? X[j] : 0.0) + (j == 2 ? X[i] : 0.0)) * inv_r3
+                         + 3.0 * pz * X[i] * X[j] * inv_r5;
+        const double d2th = -d2f * inv_s - df[i] * df[j] * cos3;
+        double d2ph = 0.0;
+        if (p == 0) d2ph = d2ph_xx;
+        else if (p == 1) d2ph = d2ph_yy;
+        else if (p == 3) d2ph = d2ph_xy;
+        o.h[p] = Prr * dlr[i] * dlr[j]
+               + Prth * (dlr[i] * dth[j] + dlr[j] * dth[i])
+               + Prph * (dlr[i] * dph[j] + dlr[j] * dph[i])
+               + Pthth * dth[i] * dth[j]
+               + Pthph * (dth[i] * dph[j] + dth[j] * dph[i])
+               + Pphph * dph[i] * dph[j]
+               + Pr * d2lr + Pth * d2th + Pph * d2ph;
+    }
+}
+
 template <int MODE, typename R>
 __device__ __forceinline__ void multipole_point(const DevComp& c, double px, double py,
                                                 double pz, PointOut& o)
@@ -498,73 +580,6 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
     else
         mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
 
-    const double Bp = t.B * inv_dlogr;
-    const double Dp = t.D * inv_dlogr * inv_dlogr;
-    o.phi = mono + F * t.A;
-    if (MODE == AGB_MODE_POT) return;
-
-    const double Pr = dmono + F * Bp + dF * t.A;
-    if (MODE == AGB_MODE_DENS) {
-        const double inv_r2 = inv_r * inv_r;
-        const double lap = (d2mono + dmono) * inv_r2
-            + (F * (Dp + Bp - t.L) + dF * (2.0 * Bp + t.A) + d2F * t.A) * inv_r2;
-        o.rho = lap * AGB_INV_4PIG;
-        return;
-    }
-    const double Pth = F * t.Th;
-    const double Pos = F * t.Pos;
-    const double inv_r2 = inv_r * inv_r;
-    o.g[0] = Pr * (px * inv_r2) + Pth * (cth * cph * inv_r) + Pos * (-sph * inv_r);
-    o.g[1] = Pr * (py * inv_r2) + Pth * (cth * sph * inv_r) + Pos * (cph * inv_r);
-    o.g[2] = Pr * (pz * inv_r2) + Pth * (-sth * inv_r);
-    if (MODE != AGB_MODE_HESS) return;
-
-    // second derivatives in (log r, theta, phi)
-    const double Prr = d2mono + F * Dp + 2.0 * dF * Bp + d2F * t.A;
-    const double Pthth = F * t.Thth;
-    const double Prth = F * (t.BTh * inv_dlogr) + dF * t.Th;
-    const double Pph = F * t.Ph;
-    const double Pphph = F * t.Phph;
-    const double Prph = F * (t.BPh * inv_dlogr) + dF * t.Ph;
-    const double Pthph = F * t.ThPh;
-
-    // first and second derivatives of (log r, theta, phi) w.r.t. x, y, z
-    const double inv_R = (Rc > 1.0e-300) ? 1.0 / Rc : 0.0;
-    const double X[3] = {px, py, pz};
-    const double dlr[3] = {px * inv_r2, py * inv_r2, pz * inv_r2};
-    const double dth[3] = {cth * cph * inv_r, cth * sph * inv_r, -sth * inv_r};
-    const double dph[3] = {-sph * inv_R, cph * inv_R, 0.0};
-    const double inv_r3 = inv_r2 * inv_r, inv_r4 = inv_r2 * inv_r2, inv_r5 = inv_r4 * inv_r;
-    const double inv_s = (sth > 1.0e-14) ? 1.0 / sth : 0.0;
-    const double cos3 = cth * inv_s * inv_s * inv_s;
-    // f = cos(theta) = z / r
-    const double df[3] = {-pz * px * inv_r3, -pz * py * inv_r3, inv_r - pz * pz * inv_r3};
-    double d2ph_xx = 0.0, d2ph_xy = 0.0, d2ph_yy = 0.0;
-    if (Rc > 1.0e-14) {
-        const double iR4 = inv_R * inv_R * inv_R * inv_R;
-        d2ph_xx = 2.0 * px * py * iR4;
-        d2ph_xy = (py * py - px * px) * iR4;
-        d2ph_yy = -2.0 * px * py * iR4;
-    }
-    #pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        const int i = hess_i(p), j = hess_j(p);
-        const double dij = (i == j) ? 1.0 : 0.0;
-        const double d2lr = dij * inv_r2 - 2.0 * X[i] * X[j] * inv_r4;
-        // d2 f / dx_i dx_j = -(delta_ij z + delta_iz x_j + delta_jz x_i)/r^3 + 3 z x_i x_j / r^5
-        const double d2f = -(dij * pz + (i == 2 ? X[j] : 0.0) + (j == 2 ? X[i] : 0.0)) * inv_r3
-                         + 3.0 * pz * X[i] * X[j] * inv_r5;
-        const double d2th = -d2f * inv_s - df[i] * df[j] * cos3;
-        double d2ph = 0.0;
-        if (p == 0) d2ph = d2ph_xx;
-        else if (p == 1) d2ph = d2ph_yy;
-        else if (p == 3) d2ph = d2ph_xy;
-        o.h[p] = Prr * dlr[i] * dlr[j]
-               + Prth * (dlr[i] * dth[j] + dlr[j] * dth[i])
-               + Prph * (dlr[i] * dph[j] + dlr[j] * dph[i])
-               + Pthth * dth[i] * dth[j]
-               + Pthph * (dth[i] * dph[j] + dth[j] * dph[i])
-               + Pphph * dph[i] * dph[j]
-               + Pr * d2lr + Pth * d2th + Pph * d2ph;
-    }
+    mp_finish<MODE>(t, inv_dlogr, F, dF, d2F, mono, dmono, d2mono, px, py, pz, inv_r, Rc,
+                    cth, sth, cph, sph, o);
 }

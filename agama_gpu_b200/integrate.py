@@ -172,21 +172,25 @@ class Leapfrog:
                 gF = lv * self.h
                 if pending is not None:
                     gF.add_(pending)
-                self.pot._vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
-                              precision=self.precision, out=gx)
-                if tg is not None:
-                    self.pot._table_vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF, tg)
+                if tg is None:
+                    self.pot._vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
+                                  precision=self.precision, out=gx)
+                else:
+                    self.pot._adjoint_vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
+                                          tg, precision=self.precision, out=gx)
                 lx.add_(gx)
                 lv.add_(lx, alpha=self.dt)
                 pending = lv * self.h
         if pending is not None:
             _, x0, _ = ckpts[0]
-            self.pot._vjp(x0, self.t0, None, pending, precision=self.precision, out=gx)
-            if tg is not None:
-                self.pot._table_vjp(x0, self.t0, None, pending, tg)
+            if tg is None:
+                self.pot._vjp(x0, self.t0, None, pending, precision=self.precision, out=gx)
+            else:
+                self.pot._adjoint_vjp(x0, self.t0, None, pending, tg, precision=self.precision,
+                                      out=gx)
             lx.add_(gx)
         if tg is not None:
-            return lx, lv, tg
+            return lx, lv, self.pot._table_grads_from_device(tg)
         return lx, lv
 
 

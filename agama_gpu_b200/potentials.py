@@ -142,9 +142,11 @@ class _GPUPotBase:
         return self
 
     # -- evaluation core ----------------------------------------------------
-    def _c_args(self, t: float, dev: torch.device):
-        """(component array, n_comps, leaf array, n_leaves) of the tree at time t."""
-        leaves = self._leaves(float(t))
+    def _c_args(self, t: float, dev: torch.device, leaves=None):
+        """(component array, n_comps, leaf array, n_leaves) of the tree at time t
+        (or of the given leaves)."""
+        if leaves is None:
+            leaves = self._leaves(float(t))
         if not leaves:
             raise ValueError("potential has no components")
         if len(leaves) > _lib.MAX_LEAVES:
@@ -206,7 +208,7 @@ class _GPUPotBase:
 
     def _vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
              g_force: Optional[torch.Tensor], precision: Optional[str] = None,
-             out: Optional[torch.Tensor] = None) -> torch.Tensor:
+             out: Optional[torch.Tensor] = None, leaves=None) -> torch.Tensor:
         """dL/dx = g_phi * grad(Phi) - H g_force for cotangents of (Phi, force)."""
         n = arr.shape[0]
         dev = arr.device
@@ -214,7 +216,7 @@ class _GPUPotBase:
         gx = out if out is not None else torch.empty((n, 3), dtype=torch.float64, device=dev)
         if n == 0:
             return gx
-        cargs = self._c_args(t, dev)
+        cargs = self._c_args(t, dev, leaves)
         gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
         gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
@@ -224,6 +226,73 @@ class _GPUPotBase:
                                    ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
         _lib.check(rc, "agb_eval_vjp")
         return gx
+
+    def _adjoint_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
+                     g_force: Optional[torch.Tensor], acc_dev: dict,
+                     precision: Optional[str] = None, out: Optional[torch.Tensor] = None):
+        """Position VJP of the tree and, fused into the same walk, the coefficient
+        gradients of its (regular-layout) Multipoles, accumulated into ``acc_dev``
+        as device-layout buffers {component: (n_int, n_cols, 6)}; convert them with
+        ``_table_grads_from_device``.  Other Multipoles use the separate passes."""
+        n = arr.shape[0]
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        leaves = self._leaves(float(t))
+        fused = [lf for lf in leaves
+                 if lf[0].kind == _lib.KIND_MULTIPOLE and getattr(lf[0], "_structure", 0) != 0]
+        rest = [lf for lf in leaves if not any(lf is f for f in fused)]
+        gx = out if out is not None else torch.empty((n, 3), dtype=torch.float64, device=dev)
+        if rest:
+            self._vjp(arr, t, g_phi, g_force, precision=precision, out=gx, leaves=rest)
+            for comp, sigma, gamma, ampl in rest:
+                if comp.kind == _lib.KIND_MULTIPOLE:
+                    g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
+                    key = ("poly", comp)
+                    if key in acc_dev:
+                        acc_dev[key].add_(g)
+                    else:
+                        acc_dev[key] = g
+        else:
+            gx.zero_()
+        if n == 0:
+            return gx
+        gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
+        gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        for comp, sigma, gamma, ampl in fused:
+            c = comp._device_component(dev)
+            lf = _lib.AgbLeaf()
+            lf.comp, lf.sigma, lf.ampl = 0, float(sigma), float(ampl)
+            lf.gamma[0], lf.gamma[1], lf.gamma[2] = (float(v) for v in gamma)
+            buf = acc_dev.get(comp)
+            if buf is None:
+                buf = torch.zeros((comp.tables.n_int, comp._n_cols, 6), dtype=torch.float64,
+                                  device=dev)
+                acc_dev[comp] = buf
+            nws = int(_lib.lib.agb_multipole_table_vjp_workspace_bytes(ctypes.byref(c),
+                                                                       ctypes.byref(lf), n))
+            ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
+            rc = _lib.lib.agb_multipole_adjoint(ctypes.byref(c), ctypes.byref(lf), arr.data_ptr(),
+                                                n, prec, ptr(gp), ptr(gf), gx.data_ptr(),
+                                                buf.data_ptr(), ptr(ws), nws, stream)
+            _lib.check(rc, "agb_multipole_adjoint")
+        return gx
+
+    @staticmethod
+    def _table_grads_from_device(acc_dev: dict) -> dict:
+        """{component: dL/dpoly in the layout of component.tables.poly}."""
+        out = {}
+        for key, g in acc_dev.items():
+            if isinstance(key, tuple):              # already in poly layout
+                comp = key[1]
+                out[comp] = out[comp] + g if comp in out else g
+                continue
+            comp = key
+            cols = torch.from_numpy(comp._col_of).to(g.device)
+            gp = g.index_select(1, cols).permute(1, 0, 2).contiguous()
+            out[comp] = out[comp] + gp if comp in out else gp
+        return out
 
     def _table_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
                    g_force: Optional[torch.Tensor], acc: Optional[dict] = None) -> dict:

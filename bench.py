@@ -150,6 +150,55 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision: str,
+                  checkpoint_every: int = 64):
+    """Adjoint / forward time of the stream workload: Gaussian clouds (0.1 kpc, 1 km/s)
+    on circular orbits at 10-60 kpc in an lmax=16 x 64-node Multipole + Miyamoto-Nagai,
+    leapfrog dt = 1e-3 Gyr; loss = sum |x_T - target|^2; the backward returns dL/dx0,
+    dL/dv0 and dL/d(quintic coefficients) of the Multipole."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
+    from agama_gpu_b200.synthetic import nfw_multipole
+    rng = np.random.default_rng(77)
+    mp = agb.MultipolePotentialGPU(nfw_multipole(lmax=16, n_nodes=64, seed=16))
+    pot = mp + agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3)
+    R0 = rng.uniform(10.0, 60.0, n_streams)
+    ph0 = rng.uniform(0, 2 * np.pi, n_streams)
+    inc = rng.uniform(0, np.pi, n_streams)
+    c0 = np.stack([R0 * np.cos(ph0), R0 * np.sin(ph0) * np.cos(inc), R0 * np.sin(ph0) * np.sin(inc)], 1)
+    vc = np.sqrt(np.maximum(-(pot.force(c0).cpu().numpy() * c0).sum(1), 1.0))
+    t_hat = np.stack([-np.sin(ph0), np.cos(ph0) * np.cos(inc), np.cos(ph0) * np.sin(inc)], 1)
+    v0c = t_hat * vc[:, None]
+    x0 = np.repeat(c0, per_stream, 0) + rng.normal(0, 0.1, (n_streams * per_stream, 3))
+    v0 = np.repeat(v0c, per_stream, 0) + rng.normal(0, 1.0, (n_streams * per_stream, 3))
+    x0t = torch.from_numpy(x0).to(dev)
+    v0t = torch.from_numpy(v0).to(dev)
+    target = x0t + torch.from_numpy(rng.normal(0, 1.0, x0.shape)).to(dev)
+    integ = Leapfrog(pot, gyr_to_time(1e-3), precision=precision)
+    integ.run(x0t, v0t, 2 * integ.graph_steps, checkpoint_every)      # capture + warm up
+    torch.cuda.synchronize()
+    e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+    e0.record()
+    xT, vT, ck = integ.run(x0t, v0t, n_steps, checkpoint_every)
+    e1.record()
+    lx, lv, tg = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT), table_grads=True)
+    gnodes = mp.node_gradients(tg[mp])
+    e2.record()
+    lx2, _ = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT))
+    e3.record()
+    torch.cuda.synchronize()
+    fwd, adj, adj_x = e0.elapsed_time(e1), e1.elapsed_time(e2), e2.elapsed_time(e3)
+    ok = bool(torch.isfinite(lx).all() and torch.isfinite(gnodes[0]).all()
+              and torch.isfinite(lx2).all())
+    return {"forward_ms": fwd, "adjoint_ms": adj, "ratio": adj / fwd,
+            "adjoint_phase_space_only_ms": adj_x, "ratio_phase_space_only": adj_x / fwd,
+            "steps": n_steps,
+            "particles": n_streams * per_stream, "checkpoint_every": checkpoint_every,
+            "precision": precision, "finite": ok,
+            "backward_returns": "dL/dx0, dL/dv0, dL/dPhi_nodes, dL/d(dPhi/dr)_nodes (17^2 x 64)"}
+
+
 def cpu_baseline_leg(pot, xyz: np.ndarray, t: float, n_sample: int):
     from oracle import cpu
     threads = os.cpu_count() or 1
@@ -174,6 +223,8 @@ def main():
     ap.add_argument("--n", type=int, default=4_000_000, help="points per GPU")
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=256,
+                    help="leapfrog steps of the adjoint/forward measurement (0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -296,6 +347,11 @@ def main():
     e2e_ms = max_over_ranks(e_tot / args.steps)
     pot.set_precision(None)
 
+    adj = None
+    if args.adj_steps > 0:
+        adj = adjoint_ratio(dev, 1024, 2048, args.adj_steps, "mixed")
+        adj["ratio"] = max_over_ranks(adj["ratio"])
+
     # roofline of the dominant (only) kernel
     pk64 = ctypes_peak(_lib, 0)
     pk32 = ctypes_peak(_lib, 1)
@@ -321,7 +377,8 @@ def main():
                               "interval_sort_mixed": ms32 - k32,
                               "mixed_unsorted_points_no_sort": u32},
         "mixed_vs_fp64_error": {"force_max_rel": err_f, "phi_max_rel": err_p, "gate": 1e-6},
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": None if adj is None else adj["ratio"],
+        "adjoint": adj,
         "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
                 "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,
                 "ms_per_step": e2e_ms},

@@ -228,6 +228,21 @@ int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
                             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Fused adjoint of one Multipole leaf: one walk over the harmonics per point
+ * ADDS this leaf's position VJP, A sigma (g_phi grad Phi - sigma H g_force),
+ * into g_xyz [N,3] and accumulates the coefficient gradient into g_table as
+ * agb_multipole_table_vjp does.  Needs a regular column structure
+ * (AGB_STRUCT_ALL/EVEN).  precision: AGB_PREC_FP64 or AGB_PREC_MIXED (FP32
+ * walk and warp reductions, FP64 accumulation).  Same workspace rules and size
+ * as agb_multipole_table_vjp.  No counterpart in the reference.
+ */
+int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
+                          const double* xyz, int64_t n, int precision,
+                          const double* g_phi, const double* g_force, double* g_xyz,
+                          double* g_table, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
+/*
  * agb_eval_static -- agb_eval that allocates nothing.  No counterpart in the
  * reference: it exists for callers that may not allocate device memory (a
  * code that reserved the GPU for its own pools, a loop that must not pay

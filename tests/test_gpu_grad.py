@@ -299,3 +299,36 @@ def test_leapfrog_table_gradients():
             (cm_.phi if which == "phi" else cm_.dphi_dr)[i, c] -= h
             fd = (run(cp_) - run(cm_)) / (2 * h)
             assert abs(G[i, c] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(G).max()), (which, i, c, G[i, c], fd)
+
+
+@pytest.mark.parametrize("lmax", [6, 32])
+@pytest.mark.parametrize("prec,tol_x,tol_g", [("fp64", 1e-12, 1e-11), ("mixed", 2e-5, 2e-5)])
+def test_fused_adjoint_matches_separate_passes(prec, tol_x, tol_g, lmax):
+    """agb_multipole_adjoint (one harmonic walk for the position VJP and the
+    coefficient gradients) against agb_eval_vjp + agb_multipole_table_vjp.
+    lmax=6 runs the shared-memory staged accumulation, lmax=32 (561 columns)
+    the direct global atomics."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    mp = agb.MultipolePotentialGPU(nfw_multipole(lmax=lmax, n_nodes=30, seed=31, amp=0.3))
+    assert mp._structure != 0
+    pot = agb.CompositePotentialGPU([
+        agb.ScaledPotentialGPU(agb.ShiftedPotentialGPU(mp, [0.3, -0.2, 0.1]), 1.3, 0.8),
+        agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3),
+        agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))])
+    xyz = _pts(20000, 32, 0.02, 2000.0)
+    rng = np.random.default_rng(33)
+    x = torch.from_numpy(xyz).cuda()
+    gphi = torch.from_numpy(rng.normal(size=len(xyz))).cuda()
+    gf = torch.from_numpy(rng.normal(size=(len(xyz), 3))).cuda()
+    ref_x = pot._vjp(x, 0.0, gphi, gf, precision="fp64")
+    ref_g = pot._table_vjp(x, 0.0, gphi, gf)[mp]
+    acc = {}
+    gx = pot._adjoint_vjp(x, 0.0, gphi, gf, acc, precision=prec)
+    gx = pot._adjoint_vjp(x, 0.0, gphi, gf, acc, precision=prec, out=torch.empty_like(gx))
+    tg = pot._table_grads_from_device(acc)[mp]
+    ex = ((gx - ref_x).abs().max() / ref_x.abs().max()).item()
+    eg = ((tg - 2 * ref_g).abs().max() / ref_g.abs().max()).item()
+    assert ex <= tol_x, ex
+    assert eg <= tol_g, eg
