@@ -553,21 +553,26 @@ extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* 
         g.perm = tmp.perm;
     }
     if (!rc) {
-        // staged accumulation when 8 warps' slices of n_lm x 6 doubles fit in shared memory
-        int grid = grid_for(n);
-        size_t smem = (size_t)8 * (size_t)g.c.n_lm * 6 * sizeof(double);
-        if (smem <= (size_t)AGB_ADJ_SMEM_MAX) {
-            const long long blocks = std::min<long long>((long long)g_num_sms * 2, (n + 255) / 256);
-            const long long warps = blocks * 8, groups = (n + 31) / 32;
-            g.chunk = ((groups + warps - 1) / warps) * 32;
-            grid = (int)blocks;
-        } else {
-            smem = 0;
-            g.chunk = 0;
-        }
+        // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
+        (void)grid_for(n);               // reads the SM count once
+        const int grid = (int)std::min<long long>((long long)g_num_sms * 2, (n + 255) / 256);
+        const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
+        g.chunk = ((groups + warps - 1) / warps) * 32;
+        const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
+        const size_t acc = (size_t)g.c.n_lm * 6 * sizeof(double);
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            optin = 48 * 1024;
+        g.staged = (size_t)8 * (tile + acc) <= (size_t)optin;
+        g.warp_smem = g.staged ? (int)(tile + acc) : tile;
+        const size_t smem = (size_t)8 * g.warp_smem;
         const void* fn = precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
                                                      : (const void*)mp_adjoint_kernel<double>;
-        if (smem > 48 * 1024 &&
+        if (smem > (size_t)optin)
+            rc = set_err(AGB_ERR_UNSUPPORTED, "agb_multipole_adjoint: needs %zu bytes of shared "
+                         "memory per block, more than %d", smem, optin);
+        else if (smem > 48 * 1024 &&
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             rc = set_err(AGB_ERR_DEVICE, "agb_multipole_adjoint: cannot reserve %zu bytes of shared "
                          "memory", smem);

@@ -52,7 +52,6 @@ struct MPGradArgs {
     const double* gphi;       // [N] or null
     const double* gforce;     // [N,3] or null
     double* grad;             // [n_int][n_lm][6], accumulated
-    long long chunk;          // > 0: points per warp, staged in shared memory
     DevComp c;
     DevLeaf leaf;
 };
@@ -312,9 +311,6 @@ __device__ __forceinline__ void grad_emit6(double* __restrict__ gk, double* sk, 
     }
 }
 
-// largest shared-memory reservation of the staged adjoint (8 warps' slices)
-#define AGB_ADJ_SMEM_MAX (200 * 1024)
-
 struct MPAdjArgs {
     long long n;
     const double* xyz;        // sorted copy when perm != null
@@ -323,16 +319,97 @@ struct MPAdjArgs {
     const double* gforce;     // [N,3] or null
     double* gx;               // [N,3], accumulated (+=)
     double* grad;             // [n_int][n_lm][6], accumulated
-    long long chunk;          // > 0: points per warp, staged in shared memory
+    long long chunk;          // points per warp (multiple of 32)
+    int warp_smem;            // bytes of dynamic shared memory per warp
+    int staged;               // 1: interval sums staged in shared memory
     DevComp c;
     DevLeaf leaf;
 };
 
+// Coefficient gradient of one interval k for a warp whose 32 points all lie
+// in k: dL/da_{c,j} = sum_p (s_p^j U_c(p) + j s_p^(j-1) V_c(p)).  Instead of
+// reducing 6 values across the warp for every column, the walk writes each
+// point's (U, V) of the column into a shared tile [point][column], and every
+// 32 columns the lanes switch roles: lane q takes column q of the tile and
+// contracts it with the points' powers of s (broadcast reads), 10 FMAs per
+// point, then adds its 6 sums to the interval's accumulator.
+template <typename R> struct AdjVec;
+template <> struct AdjVec<float> { typedef float2 T2; };
+template <> struct AdjVec<double> { typedef double2 T2; };
+
+#define AGB_ADJ_TILE_STRIDE 33          // tile row length (columns + 1: no bank conflicts)
+#define AGB_ADJ_SPW 12                  // per-point powers: s..s^5, 2s, 3s^2, 4s^3, 5s^4, pad
+
+template <typename R>
+__host__ __device__ constexpr int adj_tile_bytes()
+{
+    return (32 * AGB_ADJ_TILE_STRIDE * 2 + 32 * AGB_ADJ_SPW) * (int)sizeof(R);
+}
+
+template <typename R>
+struct AdjTile {
+    typename AdjVec<R>::T2* uv;   // [32 points][AGB_ADJ_TILE_STRIDE]
+    R* spw;                       // [32 points][AGB_ADJ_SPW]
+    double* acc;                  // interval accumulator [n_lm][6]: shared (staged) or global
+    int nb, col0;
+    bool on;                      // warp-uniform: this warp's points share one interval
+    bool shared_acc;
+};
+
+template <typename R>
+__device__ __forceinline__ void adj_contract(AdjTile<R>& T, int lane)
+{
+    __syncwarp();
+    if (lane < T.nb) {
+        R g0 = R(0), g1 = R(0), g2 = R(0), g3 = R(0), g4 = R(0), g5 = R(0);
+        #pragma unroll 4
+        for (int p = 0; p < 32; ++p) {
+            const typename AdjVec<R>::T2 uv = T.uv[p * AGB_ADJ_TILE_STRIDE + lane];
+            const R* w = T.spw + p * AGB_ADJ_SPW;
+            g0 += uv.x;
+            g1 = fma(w[0], uv.x, g1 + uv.y);
+            g2 = fma(w[1], uv.x, fma(w[5], uv.y, g2));
+            g3 = fma(w[2], uv.x, fma(w[6], uv.y, g3));
+            g4 = fma(w[3], uv.x, fma(w[7], uv.y, g4));
+            g5 = fma(w[4], uv.x, fma(w[8], uv.y, g5));
+        }
+        double* d = T.acc + (long long)(T.col0 + lane) * 6;
+        if (T.shared_acc) {
+            d[0] += (double)g0; d[1] += (double)g1; d[2] += (double)g2;
+            d[3] += (double)g3; d[4] += (double)g4; d[5] += (double)g5;
+        } else {
+            atomicAdd(d, (double)g0); atomicAdd(d + 1, (double)g1); atomicAdd(d + 2, (double)g2);
+            atomicAdd(d + 3, (double)g3); atomicAdd(d + 4, (double)g4); atomicAdd(d + 5, (double)g5);
+        }
+    }
+    __syncwarp();
+    T.col0 += T.nb;
+    T.nb = 0;
+}
+
+// one column's (U, V) of this lane's point
+template <typename R>
+__device__ __forceinline__ void adj_put(AdjTile<R>& T, double* __restrict__ gk, int col,
+                                        const R sp[6], const R dw[6], R U, R V, int lane,
+                                        bool active)
+{
+    if (T.on) {
+        typename AdjVec<R>::T2 uv;
+        uv.x = U;
+        uv.y = V;
+        T.uv[lane * AGB_ADJ_TILE_STRIDE + T.nb] = uv;
+        if (++T.nb == 32) adj_contract(T, lane);
+    } else if (active && gk) {
+        #pragma unroll
+        for (int j = 0; j < 6; ++j) atomicAdd(gk + (long long)col * 6 + j, (double)fma(sp[j], U, dw[j] * V));
+    }
+}
+
 template <typename R, int PAR>
 __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, double cth_d,
                                             double sth_d, double cph, double sph, R P1, R P2,
-                                            R P3, R P4, double* gbase, double* sk, bool uniform,
-                                            int lane, bool active, MPSums& tot)
+                                            R P3, R P4, double* gbase, AdjTile<R>& T, int lane,
+                                            bool active, MPSums& tot)
 {
     constexpr int MODE = AGB_MODE_HESS;
     const bool near_pole = sth_d < 1.0e-10;
@@ -380,26 +457,17 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
             const R d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
             const R base = fma(P3, dPc, P1 * Pc);
             const R Pq = P4 * Pos;
-            R a[6], v[6];
+            R a[6];
             MPPtr<R>::load(rec, a);
             rec += MPPtr<R>::REC;
             mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
-            {
-                const R U = fma(Tc, base, dTc * Pq), V = P2 * Pc * Tc;
-                #pragma unroll
-                for (int j = 0; j < 6; ++j) v[j] = fma(sp[j], U, dw[j] * V);
-                grad_emit6<R>(gbase, sk, col, v, uniform, lane, active);
-                ++col;
-            }
+            adj_put<R>(T, gbase, col++, sp, dw, fma(Tc, base, dTc * Pq), P2 * Pc * Tc, lane, active);
             if (m > 0) {
                 MPPtr<R>::load(rec, a);
                 rec += MPPtr<R>::REC;
                 mp_col_acc<MODE, R>(gs, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
-                const R U = fma(Ts, base, dTs * Pq), V = P2 * Pc * Ts;
-                #pragma unroll
-                for (int j = 0; j < 6; ++j) v[j] = fma(sp[j], U, dw[j] * V);
-                grad_emit6<R>(gbase, sk, col, v, uniform, lane, active);
-                ++col;
+                adj_put<R>(T, gbase, col++, sp, dw, fma(Ts, base, dTs * Pq), P2 * Pc * Ts, lane,
+                           active);
             }
         };
         int l = m;
@@ -424,37 +492,34 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
         tot.BPh += (double)gc.VR * ddTc + (double)gs.VR * ddTs;
         tot.ThPh += (double)gc.VT * ddTc + (double)gs.VT * ddTs;
     }
+    if (T.on && T.nb) adj_contract(T, lane);
 }
 
-// Two ways to schedule the points.  Plain (chunk == 0): grid-stride over warps
-// of 32 points, every uniform warp adding its 6 x n_lm reduced values to the
-// interval's gradient with global atomics.  Staged (chunk > 0): each warp owns
-// `chunk` consecutive (interval-sorted) points and a slice of shared memory of
-// n_lm x 6 doubles; while its points stay in one interval it adds into the
-// slice with plain stores, and it flushes the slice to global memory (one
-// atomic per value) only when the interval changes and at the end.
+// Each warp owns `chunk` consecutive (interval-sorted) points and a slice of
+// dynamic shared memory: the (U, V) tile and powers of s above, and when
+// `staged`, an accumulator of n_lm x 6 doubles for the interval its points are
+// in, flushed to global memory (one atomic per value) only when the interval
+// changes and at the end.  Without `staged` the tile contractions add to
+// global memory directly.  Warps whose points straddle intervals add each
+// lane's six values with atomics.
 template <typename R>
 __global__ void __launch_bounds__(256, 1)
 mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
 {
-    extern __shared__ double agb_adj_smem[];
+    extern __shared__ __align__(16) unsigned char agb_adj_smem[];
     const DevComp& c = a.c;
     const int lane = threadIdx.x & 31;
     const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const bool staged = a.chunk > 0;
     const int nval = c.n_lm * 6;
-    double* swarp = staged ? agb_adj_smem + (long long)(threadIdx.x >> 5) * nval : nullptr;
-    long long lo, hi, step;
-    if (staged) {
-        lo = gwarp * a.chunk;
-        hi = lo + a.chunk < a.n ? lo + a.chunk : a.n;
-        step = 32;
+    unsigned char* wbase = agb_adj_smem + (size_t)(threadIdx.x >> 5) * a.warp_smem;
+    AdjTile<R> T;
+    T.uv = reinterpret_cast<typename AdjVec<R>::T2*>(wbase);
+    T.spw = reinterpret_cast<R*>(wbase + 32 * AGB_ADJ_TILE_STRIDE * sizeof(typename AdjVec<R>::T2));
+    double* swarp = a.staged ? reinterpret_cast<double*>(wbase + adj_tile_bytes<R>()) : nullptr;
+    const long long lo = gwarp * a.chunk;
+    const long long hi = lo + a.chunk < a.n ? lo + a.chunk : a.n;
+    if (swarp)
         for (int q = lane; q < nval; q += 32) swarp[q] = 0.0;
-    } else {
-        lo = gwarp * 32;
-        hi = a.n;
-        step = (long long)gridDim.x * blockDim.x;
-    }
     int cur_k = -1;                      // interval held in swarp
     auto flush = [&]() {
         __syncwarp();
@@ -472,7 +537,7 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
     const double logr_min = c.p[0], dlogr = c.p[1], inv_dlogr = c.p[2], invPhi0 = c.p[3];
     const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
     const double A = a.leaf.ampl, sg = a.leaf.sigma;
-    for (long long base = lo; base < hi; base += step) {
+    for (long long base = lo; base < hi; base += 32) {
         const long long pos = base + lane;
         const bool valid = pos < hi;
         long long i = pos;
@@ -537,18 +602,33 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
         const int kk = uniform ? kmax : k;
         double* gbase = (kk >= 0) ? a.grad + (long long)kk * c.n_lm * 6 : nullptr;
         double* sk = nullptr;
-        if (staged && uniform && kk >= 0) {
-            if (kk != cur_k) {
-                flush();
-                cur_k = kk;
+        T.on = uniform && kk >= 0;
+        T.nb = 0;
+        T.col0 = 1;
+        T.shared_acc = false;
+        T.acc = gbase;
+        if (T.on) {
+            if (swarp) {
+                if (kk != cur_k) {
+                    flush();
+                    cur_k = kk;
+                }
+                sk = swarp;
+                T.acc = swarp;
+                T.shared_acc = true;
             }
-            sk = swarp;
+            // this lane's powers of s (zeros for points outside the grid)
+            const R sr = inside ? (R)s : R(0);
+            const R s2 = sr * sr, s3 = s2 * sr, s4 = s2 * s2;
+            R* w = T.spw + lane * AGB_ADJ_SPW;
+            w[0] = sr; w[1] = s2; w[2] = s3; w[3] = s4; w[4] = s4 * sr;
+            w[5] = R(2) * sr; w[6] = R(3) * s2; w[7] = R(4) * s3; w[8] = R(5) * s4;
         }
         MPSums t = {};
         if (c.structure == AGB_STRUCT_EVEN)
-            mp_adj_walk<R, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, sk, uniform, lane, inside, t);
+            mp_adj_walk<R, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
         else
-            mp_adj_walk<R, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, sk, uniform, lane, inside, t);
+            mp_adj_walk<R, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
         // monopole column of the coefficient gradient
         {
             const double Bp = t.B * inv_dlogr;
@@ -586,5 +666,5 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
         a.gx[3 * i + 1] += As * (gp * o.g[1] - s2 * (h[3] * gf0 + h[1] * gf1 + h[4] * gf2));
         a.gx[3 * i + 2] += As * (gp * o.g[2] - s2 * (h[5] * gf0 + h[4] * gf1 + h[2] * gf2));
     }
-    if (staged) flush();
+    if (swarp) flush();
 }

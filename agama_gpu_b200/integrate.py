@@ -10,11 +10,13 @@ next):
     v_n+1 = v_h + h F(x_n+1, t_n+1)
 
 The adjoint runs the steps backwards.  Positions are re-computed segment by
-segment from checkpoints stored every ``checkpoint_every`` steps, and each
-backward step needs ONE vector-Jacobian product of the force
+segment from checkpoints stored every ``checkpoint_every`` steps (and at the
+end), and each backward step needs ONE vector-Jacobian product of the force
 (``agb_eval_vjp``: (dF/dx)^T g = -H g) because the two half-kicks that use
 F(x_n) are merged into one cotangent.  Total cost: the forward (n+1
-evaluations), a re-computation (n+segments evaluations) and n+1 VJPs.
+evaluations), a re-computation (n evaluations; none when every step is a
+checkpoint, which is what ``checkpoint_every=None`` picks whenever the
+positions of every step fit in 60% of the free device memory) and n+1 VJPs.
 
 For potentials that do not depend on time, steps are captured into CUDA
 graphs (``graph_steps`` per graph) and replayed.
@@ -49,6 +51,23 @@ def is_static(pot) -> bool:
     if isinstance(pot, ScaledPotentialGPU):
         return pot._is_static and is_static(pot._inner)
     return False
+
+
+def auto_checkpoint_every(like: torch.Tensor, n_steps: int, fraction: float = 0.6) -> int:
+    """Checkpoint interval for ``n_steps`` steps of the particles in ``like`` within
+    ``fraction`` of the free device memory: 1 (every step's positions, no
+    re-computation in the adjoint) when they fit, else the smallest k whose (x, v)
+    checkpoints fit."""
+    row = like.numel() * 8
+    try:
+        free, _ = torch.cuda.mem_get_info(like.device)
+    except (RuntimeError, AssertionError):
+        return 64
+    budget = int(free * fraction)
+    if (int(n_steps) + 2) * row <= budget:
+        return 1
+    fit = max(1, budget // max(2 * row, 1))
+    return max(2, -(-int(n_steps) // fit))
 
 
 class Leapfrog:
@@ -115,20 +134,47 @@ class Leapfrog:
 
     # -- forward with checkpoints ------------------------------------------------------
     def run(self, x0: torch.Tensor, v0: torch.Tensor, n_steps: int,
-            checkpoint_every: int = 64) -> Tuple[torch.Tensor, torch.Tensor, List]:
-        """Returns (x_T, v_T, checkpoints); checkpoints = [(step, x, v)] every k steps."""
+            checkpoint_every: Optional[int] = 64) -> Tuple[torch.Tensor, torch.Tensor, List]:
+        """Returns (x_T, v_T, checkpoints); checkpoints = [(step, x, v)] every k steps and
+        at the end.  k = 1 keeps every step's positions (v is None except at the end) and
+        the adjoint then re-computes nothing; checkpoint_every=None picks k with
+        ``auto_checkpoint_every`` (1 whenever the trajectory fits in 60% of the free
+        device memory)."""
         x, v, F = self._buffers(x0)
         x.copy_(x0.detach())
         v.copy_(v0.detach())
         self._force_into(x, self.t0, F)
-        k = max(1, int(checkpoint_every))
+        k = auto_checkpoint_every(x, n_steps) if checkpoint_every is None else int(checkpoint_every)
+        k = max(1, k)
+        if k == 1:
+            # every step's positions in one allocation [step][particle][3]; the adjoint
+            # re-computes nothing and needs no velocities
+            store = torch.empty((int(n_steps) + 1,) + tuple(x.shape), dtype=torch.float64,
+                                device=x.device)
+            for n in range(n_steps):
+                store[n].copy_(x)
+                self._step(x, v, F, self.t0 + n * self.dt)
+            store[n_steps].copy_(x)
+            ckpts = [(n, store[n], None) for n in range(n_steps)]
+            ckpts.append((n_steps, store[n_steps], v.clone()))
+            return x.clone(), v.clone(), ckpts
+        # one allocation for all checkpoints: [checkpoint][x|v][particle][3]
+        store = torch.empty((-(-int(n_steps) // k) + 1, 2) + tuple(x.shape), dtype=torch.float64,
+                            device=x.device)
         ckpts = []
         n = 0
         while n < n_steps:
-            ckpts.append((n, x.clone(), v.clone()))
+            j = len(ckpts)
+            store[j, 0].copy_(x)
+            store[j, 1].copy_(v)
+            ckpts.append((n, store[j, 0], store[j, 1]))
             m = min(k, n_steps - n)
             self._advance(x, v, F, n, m)
             n += m
+        j = len(ckpts)
+        store[j, 0].copy_(x)
+        store[j, 1].copy_(v)
+        ckpts.append((n_steps, store[j, 0], store[j, 1]))
         return x.clone(), v.clone(), ckpts
 
     def _buffers(self, like: torch.Tensor):
@@ -155,34 +201,41 @@ class Leapfrog:
         lv = lam_v.detach().to(torch.float64).contiguous().clone()
         pending = None                      # cotangent on F(x_n) from the later half-kick
         gx = torch.empty_like(lx)
-        bounds = [c[0] for c in ckpts] + [n_steps]
-        for seg in range(len(ckpts) - 1, -1, -1):
+        at = {c[0]: c for c in ckpts}
+        starts = sorted(c[0] for c in ckpts if c[0] < n_steps)
+        bounds = starts + [n_steps]
+        for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
-            _, xs, vs = ckpts[seg]
-            # re-compute the segment's positions
-            X = torch.empty((e - s + 1,) + tuple(xs.shape), dtype=torch.float64, device=xs.device)
-            x, v = xs.clone(), vs.clone()
-            F = torch.empty_like(x)
-            self._force_into(x, self.t0 + s * self.dt, F)
-            X[0].copy_(x)
-            for n in range(s, e):
-                self._step(x, v, F, self.t0 + n * self.dt)
-                X[n - s + 1].copy_(x)
+            _, xs, vs = at[s]
+            # the segment's positions: x_s and x_e from checkpoints, the others re-computed
+            pos = {s: xs}
+            if e in at:
+                pos[e] = at[e][1]
+            last = e - 1 if e in at else e
+            if last > s:
+                X = torch.empty((last - s,) + tuple(xs.shape), dtype=torch.float64, device=xs.device)
+                x, v = xs.clone(), vs.clone()
+                F = torch.empty_like(x)
+                self._force_into(x, self.t0 + s * self.dt, F)
+                for n in range(s, last):
+                    self._step(x, v, F, self.t0 + n * self.dt)
+                    X[n - s].copy_(x)
+                    pos[n + 1] = X[n - s]
             for n in range(e - 1, s - 1, -1):
                 gF = lv * self.h
                 if pending is not None:
                     gF.add_(pending)
                 if tg is None:
-                    self.pot._vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
+                    self.pot._vjp(pos[n + 1], self.t0 + (n + 1) * self.dt, None, gF,
                                   precision=self.precision, out=gx)
                 else:
-                    self.pot._adjoint_vjp(X[n + 1 - s], self.t0 + (n + 1) * self.dt, None, gF,
+                    self.pot._adjoint_vjp(pos[n + 1], self.t0 + (n + 1) * self.dt, None, gF,
                                           tg, precision=self.precision, out=gx)
                 lx.add_(gx)
                 lv.add_(lx, alpha=self.dt)
                 pending = lv * self.h
         if pending is not None:
-            _, x0, _ = ckpts[0]
+            _, x0, _ = at[0]
             if tg is None:
                 self.pot._vjp(x0, self.t0, None, pending, precision=self.precision, out=gx)
             else:
@@ -212,9 +265,10 @@ class _LeapfrogFn(torch.autograd.Function):
 
 
 def leapfrog(pot, x0: torch.Tensor, v0: torch.Tensor, dt: float, n_steps: int, t0: float = 0.0,
-             checkpoint_every: int = 64, precision: Optional[str] = None,
+             checkpoint_every: Optional[int] = 64, precision: Optional[str] = None,
              use_graph: Optional[bool] = None):
     """(x_T, v_T) after n_steps leapfrog steps; differentiable w.r.t. (x0, v0) through the
     checkpointed adjoint."""
     integ = Leapfrog(pot, dt, t0=t0, precision=precision, use_graph=use_graph)
-    return _LeapfrogFn.apply(x0, v0, integ, int(n_steps), int(checkpoint_every))
+    k = None if checkpoint_every is None else int(checkpoint_every)
+    return _LeapfrogFn.apply(x0, v0, integ, int(n_steps), k)

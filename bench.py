@@ -151,14 +151,15 @@ def run_reference(args):
 
 
 def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision: str,
-                  checkpoint_every: int = 64):
-    """Adjoint / forward time of the stream workload: Gaussian clouds (0.1 kpc, 1 km/s)
+                  checkpoint_every=None):
+    """Adjoint / forward time of the stream workload (1024 clouds x 2048 particles, 2000
+    steps by default): Gaussian clouds (0.1 kpc, 1 km/s)
     on circular orbits at 10-60 kpc in an lmax=16 x 64-node Multipole + Miyamoto-Nagai,
     leapfrog dt = 1e-3 Gyr; loss = sum |x_T - target|^2; the backward returns dL/dx0,
     dL/dv0 and dL/d(quintic coefficients) of the Multipole."""
     import torch
     import agama_gpu_b200 as agb
-    from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
+    from agama_gpu_b200.integrate import Leapfrog, auto_checkpoint_every, gyr_to_time
     from agama_gpu_b200.synthetic import nfw_multipole
     rng = np.random.default_rng(77)
     mp = agb.MultipolePotentialGPU(nfw_multipole(lmax=16, n_nodes=64, seed=16))
@@ -176,18 +177,30 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
     v0t = torch.from_numpy(v0).to(dev)
     target = x0t + torch.from_numpy(rng.normal(0, 1.0, x0.shape)).to(dev)
     integ = Leapfrog(pot, gyr_to_time(1e-3), precision=precision)
-    integ.run(x0t, v0t, 2 * integ.graph_steps, checkpoint_every)      # capture + warm up
+    if checkpoint_every is None:
+        checkpoint_every = auto_checkpoint_every(x0t, n_steps)
+    # warm-up: graph capture, every kernel of the adjoint, and the allocator's blocks
+    nw = 2 * integ.graph_steps
+    xw, vw, ck = integ.run(x0t, v0t, nw, checkpoint_every)
+    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw), table_grads=True)
+    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw))
+    mp.node_gradients(mp.table_vjp(x0t[:1024], 0.0, None, torch.ones_like(x0t[:1024])))
+    del ck
+    xw, vw, ck = integ.run(x0t, v0t, n_steps, checkpoint_every)
+    del ck
     torch.cuda.synchronize()
     e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     e0.record()
     xT, vT, ck = integ.run(x0t, v0t, n_steps, checkpoint_every)
     e1.record()
-    lx, lv, tg = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT), table_grads=True)
+    lx, lv, tg = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT),
+                               table_grads=True)
     gnodes = mp.node_gradients(tg[mp])
     e2.record()
     lx2, _ = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT))
     e3.record()
     torch.cuda.synchronize()
+    del ck
     fwd, adj, adj_x = e0.elapsed_time(e1), e1.elapsed_time(e2), e2.elapsed_time(e3)
     ok = bool(torch.isfinite(lx).all() and torch.isfinite(gnodes[0]).all()
               and torch.isfinite(lx2).all())
@@ -223,7 +236,7 @@ def main():
     ap.add_argument("--n", type=int, default=4_000_000, help="points per GPU")
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--adj-steps", type=int, default=256,
+    ap.add_argument("--adj-steps", type=int, default=2000,
                     help="leapfrog steps of the adjoint/forward measurement (0: skip)")
     args = ap.parse_args()
 
@@ -349,8 +362,14 @@ def main():
 
     adj = None
     if args.adj_steps > 0:
+        # checkpoint interval from free memory (every step: no re-computation), then k = 64
         adj = adjoint_ratio(dev, 1024, 2048, args.adj_steps, "mixed")
         adj["ratio"] = max_over_ranks(adj["ratio"])
+        torch.cuda.empty_cache()
+        r64 = adjoint_ratio(dev, 1024, 2048, args.adj_steps, "mixed", checkpoint_every=64)
+        adj["recompute_k64"] = {q: r64[q] for q in ("forward_ms", "adjoint_ms", "ratio",
+                                                    "adjoint_phase_space_only_ms",
+                                                    "ratio_phase_space_only")}
 
     # roofline of the dominant (only) kernel
     pk64 = ctypes_peak(_lib, 0)

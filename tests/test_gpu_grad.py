@@ -157,6 +157,28 @@ def test_leapfrog_adjoint_matches_finite_differences(static):
             assert abs(an - fd) <= 1e-5 * max(abs(fd), 1e-3 * float(lam.abs().max())), (which, an, fd)
 
 
+@pytest.mark.parametrize("static", [True, False])
+def test_leapfrog_adjoint_independent_of_checkpoint_interval(static):
+    """Every interval (1: the stored trajectory, no re-computation; None: chosen
+    from free memory) gives the gradients of the default interval."""
+    import torch
+    from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
+    pot = _composite(static=static)
+    x0, v0 = _disk_ics(300, 17)
+    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64")
+    n_steps = 45
+    ref = None
+    for k in (16, 1, 7, 45, 200, None):
+        xT, vT, ck = integ.run(x0, v0, n_steps, checkpoint_every=k)
+        lx, lv = integ.adjoint(ck, n_steps, xT - x0, 0.1 * vT)
+        if ref is None:
+            ref = (xT, lx, lv)
+            continue
+        assert torch.equal(xT, ref[0]), k
+        assert torch.allclose(lx, ref[1], rtol=1e-13, atol=0), k
+        assert torch.allclose(lv, ref[2], rtol=1e-13, atol=0), k
+
+
 def test_leapfrog_graph_replay_equals_eager():
     import torch
     from agama_gpu_b200.integrate import Leapfrog
