@@ -45,6 +45,7 @@ struct EvalArgs {
     int out_flags;
     int soa;                 // 1: x, y, z separate arrays (kernel-signature entries)
     int pad;
+    long long chunk;         // points per block: block b evaluates [b*chunk, (b+1)*chunk)
     const double* xyz;       // AoS N x 3 when !soa (sorted copy when perm != null)
     const int* perm;         // binned order: point pos is input point perm[pos]
     const double* x;

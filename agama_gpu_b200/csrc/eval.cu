@@ -79,8 +79,11 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
     // the VJP mode evaluates every component with its Hessian and contracts at the end
     constexpr int CM = (MODE == AGB_MODE_VJP) ? AGB_MODE_HESS : MODE;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < a.n; pos += stride) {
+    // a contiguous range of (interval-sorted) points per block: consecutive
+    // iterations of a block reuse the same interval's table records from L1
+    const long long lo = (long long)blockIdx.x * a.chunk;
+    const long long hi = lo + a.chunk < a.n ? lo + a.chunk : a.n;
+    for (long long pos = lo + threadIdx.x; pos < hi; pos += blockDim.x) {
         double x, y, z;
         if (a.soa) {
             x = a.x[pos]; y = a.y[pos]; z = a.z[pos];
@@ -162,13 +165,30 @@ static int grid_for(long long n)
     return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
+#ifndef AGB_EVAL_WAVES
+#define AGB_EVAL_WAVES 4      // blocks per resident slot: balances the cost spread along r
+#endif
+
 template <int MODE, typename R>
-static void launch_eval(const EvalArgs& a, cudaStream_t st)
+static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
-    agb_eval_kernel<MODE, R><<<grid_for(a.n), 256, 0, st>>>(a);
+    static int per_sm = 0;    // resident blocks per SM of this instantiation
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_eval_kernel<MODE, R>, 256, 0)
+            != cudaSuccess || b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    (void)grid_for(a.n);      // reads the SM count once
+    const long long want = (a.n + 255) / 256;
+    const long long slots = (long long)g_num_sms * per_sm * AGB_EVAL_WAVES;
+    const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
+    a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
+    agb_eval_kernel<MODE, R><<<(int)grid, 256, 0, st>>>(a);
 }
 
-static int launch_mode(int mode, int precision, const EvalArgs& a, cudaStream_t st)
+static int launch_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
 {
     const bool mixed = precision == AGB_PREC_MIXED;
     switch (mode) {
