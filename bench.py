@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--n", type=int, default=4_000_000, help="points per GPU")
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adj-clouds", type=int, default=1024,
+                    help="clouds of 2048 particles in the adjoint/forward measurement")
     ap.add_argument("--adj-steps", type=int, default=2000,
                     help="leapfrog steps of the adjoint/forward measurement (0: skip)")
     args = ap.parse_args()
@@ -363,10 +365,10 @@ def main():
     adj = None
     if args.adj_steps > 0:
         # checkpoint interval from free memory (every step: no re-computation), then k = 64
-        adj = adjoint_ratio(dev, 1024, 2048, args.adj_steps, "mixed")
+        adj = adjoint_ratio(dev, args.adj_clouds, 2048, args.adj_steps, "mixed")
         adj["ratio"] = max_over_ranks(adj["ratio"])
         torch.cuda.empty_cache()
-        r64 = adjoint_ratio(dev, 1024, 2048, args.adj_steps, "mixed", checkpoint_every=64)
+        r64 = adjoint_ratio(dev, args.adj_clouds, 2048, args.adj_steps, "mixed", checkpoint_every=64)
         adj["recompute_k64"] = {q: r64[q] for q in ("forward_ms", "adjoint_ms", "ratio",
                                                     "adjoint_phase_space_only_ms",
                                                     "ratio_phase_space_only")}
