@@ -33,6 +33,19 @@ WORKLOAD = ("time-dependent composite: Multipole lmax=32 x 100 nodes + MiyamotoN
             "DiskAnsatz + Shifted NFW on (1000,4) track + Evolving 16 x lmax=16 snapshots; "
             "isotropic Hernquist a=10 kpc points")
 G = 4.30091727067736e-06
+# DRAM bytes (read + write) per point of one mixed-precision launch on this workload:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum = 52.20 MB + 21.63 MB at 1M points
+# (profiles/eval_kernel_composite_1M_full.txt), scaled linearly with the point count
+TRAFFIC_BYTES_PER_POINT = 73.83
+
+
+def measured_hbm_peak():
+    """Copy bandwidth in GB/s measured on this machine's GPUs, when a record is present."""
+    try:
+        with open(ROOT / "MEASURED_PEAKS.json") as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
 
 
 def step_times(k_total: int):
@@ -41,7 +54,7 @@ def step_times(k_total: int):
 
 
 def flops_per_step(pot, xyz: np.ndarray, t: float) -> tuple:
-    """Algorithmic FLOPs of one Phi+F evaluation (convention of DESIGN.md):
+    """Algorithmic FLOPs of one Phi+F evaluation (the roofline's fixed convention):
     Multipole 48*n_harm + 64 per point inside its grid (64 outside), analytic 30
     per component.  Returns (fp32-eligible harmonic flops, fp64 flops)."""
     from agama_gpu_b200 import _lib as L
@@ -384,6 +397,7 @@ def main():
     eff_peak32 = (fh + fp) / t_roof_mixed / 1e12
 
     value = world * N / (ms32 * 1e-3)
+    hbm_peak = measured_hbm_peak()
     line = {
         "metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
@@ -406,13 +420,18 @@ def main():
         "gpu_launches": int(l32),
         "roofline": {
             "bound": "fp32+fp64 pipes (mixed); fp64 pipe (plain)", "unit": "TFLOP/s",
+            "note": "FP32/FP64 ALU-bound: the peaks are measured live (FMA chains) because the "
+                    "pool's measured peaks cover only HBM copy and bf16 GEMM",
             "achieved": achieved32, "peak": eff_peak32, "frac": achieved32 / eff_peak32,
-            "traffic": None,
+            "traffic": TRAFFIC_BYTES_PER_POINT * N,
+            "traffic_source": "ncu DRAM read+write of the mixed launch at 1M points, scaled to N",
             "fp64_kernel": {"achieved": achieved64, "peak": pk64, "frac": achieved64 / pk64},
             "timing": "eval kernel alone, CUDA events on its stream, points pre-sorted by interval",
             "flops_per_step": fh + fp, "fp32_eligible_flops": fh,
             "peak_source": f"measured live: FMA-chain kernel, fp64 {pk64:.1f} / fp32 {pk32:.1f} TFLOP/s",
-            "hbm": {"bytes_per_step": N * (24 + 32), "achieved_gbs": N * 56 / (ms32 * 1e-3) / 1e9},
+            "hbm": {"bytes_per_step": N * (24 + 32), "achieved_gbs": N * 56 / (ms32 * 1e-3) / 1e9,
+                    "peak_gbs": hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
+                    if hbm_peak else "unavailable"},
         },
         "clocks": clocks,
     }
