@@ -9,6 +9,7 @@ from . import _lib  # noqa: F401  (fails loudly when libagb.so is missing)
 from .analytic import (DehnenSphericalPotentialGPU, DiskAnsatzPotentialGPU, HernquistPotentialGPU,
                        IsochronePotentialGPU, LogHaloPotentialGPU, MiyamotoNagaiPotentialGPU,
                        NFWPotentialGPU, PlummerPotentialGPU, UniformAccelerationGPU)
+from .batch import BatchedPotentialGPU
 from .coefs import CylSplineCoefs, MultipoleCoefs, read_coefs, write_coefs
 from .factory import PotentialGPU
 from .potentials import (G_AGAMA, INV_4PIG, CompositePotentialGPU, CylSplinePotentialGPU,
@@ -16,7 +17,7 @@ from .potentials import (G_AGAMA, INV_4PIG, CompositePotentialGPU, CylSplinePote
                          ShiftedPotentialGPU, prep_xyz, set_default_precision)
 
 __all__ = [
-    "PotentialGPU", "MultipolePotentialGPU", "CylSplinePotentialGPU", "CompositePotentialGPU",
+    "PotentialGPU", "BatchedPotentialGPU", "MultipolePotentialGPU", "CylSplinePotentialGPU", "CompositePotentialGPU",
     "EvolvingPotentialGPU", "ShiftedPotentialGPU", "ScaledPotentialGPU", "NFWPotentialGPU",
     "PlummerPotentialGPU", "HernquistPotentialGPU", "DehnenSphericalPotentialGPU",
     "IsochronePotentialGPU", "MiyamotoNagaiPotentialGPU", "LogHaloPotentialGPU",

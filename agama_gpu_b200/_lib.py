@@ -115,6 +115,21 @@ def _load():
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_batch_create.restype = ctypes.c_int
+    lib.agb_batch_create.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf),
+        ctypes.POINTER(ctypes.c_int32), ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+        ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.agb_batch_eval.restype = ctypes.c_int
+    lib.agb_batch_eval.argtypes = [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.agb_batch_points.restype = ctypes.c_int64
+    lib.agb_batch_points.argtypes = [ctypes.c_void_p]
+    lib.agb_batch_tiles.restype = ctypes.c_int
+    lib.agb_batch_tiles.argtypes = [ctypes.c_void_p]
+    lib.agb_batch_destroy.restype = None
+    lib.agb_batch_destroy.argtypes = [ctypes.c_void_p]
     return lib
 
 
@@ -126,6 +141,8 @@ EXPORTED = [
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
     "agb_multipole_adjoint",
+    "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
+    "agb_batch_destroy",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
     "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
 ]

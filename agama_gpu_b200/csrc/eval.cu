@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <stdarg.h>
+#include <stdlib.h>
 #include "agb_dev.cuh"
 #include "multipole.cuh"
 #include "cylspline.cuh"
@@ -775,3 +776,8 @@ extern "C" int agb_cylspl_hess(CS_SIG, double* phi_out, double* grad_out, double
     if (!phi_out || !grad_out || !hess_out) return set_err(AGB_ERR_ARG, "output pointer is null");
     return cs_compat(AGB_MODE_HESS, CS_FWD, phi_out, grad_out, hess_out, N, stream);
 }
+
+// ---------------------------------------------------------------------------
+// batched work units (device work queue)
+// ---------------------------------------------------------------------------
+#include "batch.cuh"

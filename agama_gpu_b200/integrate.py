@@ -40,8 +40,9 @@ def is_static(pot) -> bool:
     """True when the potential tree does not depend on time."""
     from .potentials import (CompositePotentialGPU, EvolvingPotentialGPU, ScaledPotentialGPU,
                              ShiftedPotentialGPU, _Component)
-    if isinstance(pot, _Component):
-        return True
+    from .batch import BatchedPotentialGPU
+    if isinstance(pot, (_Component, BatchedPotentialGPU)):
+        return True      # batches hold only static units
     if isinstance(pot, CompositePotentialGPU):
         return all(is_static(c) for c in pot._components)
     if isinstance(pot, EvolvingPotentialGPU):

@@ -225,6 +225,85 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
             "backward_returns": "dL/dx0, dL/dv0, dL/dPhi_nodes, dL/d(dPhi/dr)_nodes (17^2 x 64)"}
 
 
+def batched_units(dev, n_units: int, steps: int, warmup: int, lf_steps: int, precision: str):
+    """Many independent potentials in one launch: n_units NFW-based Multipoles
+    (lmax ~ U{2..32}, nodes ~ U[30,120], M ~ logU[1e10,1e12], rs ~ U[2,30]) with
+    N_i ~ logU[1e3, 5e5] Hernquist(a = rs) particles each, stacked.  Times the
+    batched force evaluation (one work-queue launch), the same work as one call per
+    unit, and lf_steps leapfrog steps captured in one CUDA graph."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    rng = np.random.default_rng(4)
+    units, counts, xs, flops = [], [], [], 0.0
+    for u in range(n_units):
+        lmax = int(rng.integers(2, 33))
+        rs = rng.uniform(2.0, 30.0)
+        mp = agb.MultipolePotentialGPU(nfw_multipole(
+            lmax=lmax, n_nodes=int(rng.integers(30, 121)), M=10 ** rng.uniform(10, 12), rs=rs,
+            seed=u, amp=0.05))
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        units.append(mp)
+        counts.append(n)
+        xs.append(hernquist_points(n, rs, 1000 + u))
+        flops += n * (48.0 * mp.tables.n_lm + 64.0)
+    batch = agb.BatchedPotentialGPU(units, counts, precision=precision)
+    x = torch.from_numpy(np.concatenate(xs)).to(dev)
+    del xs
+    N = batch.n_points
+    F = torch.empty_like(x)
+    ev = lambda: batch._launch(x, 0.0, 1, False, out=(None, F, None, None))  # noqa: E731
+    rows = [batch.unit_rows(u) for u in range(n_units)]
+    xu = [x[r] for r in rows]
+    Fu = [torch.empty_like(a) for a in xu]
+
+    def loop():
+        for u in range(n_units):
+            units[u]._launch(xu[u], 0.0, 1, False, precision=precision, out=(None, Fu[u], None, None))
+
+    def timed(fn, k):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+    t_batch = timed(ev, steps)
+    t_loop = timed(loop, max(1, steps // 2))
+    err = max(float((F[r] - f).abs().max()) / max(float(f.abs().max()), 1e-300)
+              for r, f in zip(rows, Fu) if r.stop > r.start)
+    del Fu, xu
+    # leapfrog: circular-ish velocities from the batched force, lf_steps steps per graph
+    vc = (F * x).sum(1, keepdim=True).neg().clamp_min(1.0).sqrt()
+    e = torch.zeros_like(x)
+    e[:, 2] = 1.0
+    t_hat = torch.linalg.cross(e, x)
+    t_hat = t_hat / t_hat.norm(dim=1, keepdim=True).clamp_min(1e-12)
+    v = t_hat * vc
+    integ = Leapfrog(batch, 0.001, precision=precision, graph_steps=lf_steps)
+    integ.run(x, v, lf_steps, checkpoint_every=lf_steps)        # capture + warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    xT, vT, _ = integ.run(x, v, lf_steps, checkpoint_every=lf_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    t_lf = e0.elapsed_time(e1)
+    return {"units": n_units, "points": N, "tiles": batch.tiles(precision), "precision": precision,
+            "eval_ms": t_batch, "pts_per_s": N / (t_batch * 1e-3),
+            "tflops": flops / (t_batch * 1e-3) / 1e12,
+            "per_unit_calls_ms": t_loop, "speedup_vs_per_unit_calls": t_loop / t_batch,
+            "max_rel_diff_vs_per_unit_calls": err,
+            "leapfrog_graph_steps": lf_steps, "leapfrog_ms": t_lf,
+            "leapfrog_particle_steps_per_s": N * lf_steps / (t_lf * 1e-3),
+            "finite": bool(torch.isfinite(xT).all())}
+
+
 def cpu_baseline_leg(pot, xyz: np.ndarray, t: float, n_sample: int):
     from oracle import cpu
     threads = os.cpu_count() or 1
@@ -249,6 +328,8 @@ def main():
     ap.add_argument("--n", type=int, default=4_000_000, help="points per GPU")
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-units", type=int, default=512,
+                    help="independent potentials of the batched measurement (0: skip)")
     ap.add_argument("--adj-clouds", type=int, default=1024,
                     help="clouds of 2048 particles in the adjoint/forward measurement")
     ap.add_argument("--adj-steps", type=int, default=2000,
@@ -386,6 +467,12 @@ def main():
                                                     "adjoint_phase_space_only_ms",
                                                     "ratio_phase_space_only")}
 
+    batched = None
+    if args.batch_units > 0:
+        torch.cuda.empty_cache()
+        batched = batched_units(dev, args.batch_units, 3, 2, 100, "mixed")
+        torch.cuda.empty_cache()
+
     # roofline of the dominant (only) kernel
     pk64 = ctypes_peak(_lib, 0)
     pk32 = ctypes_peak(_lib, 1)
@@ -414,6 +501,7 @@ def main():
         "mixed_vs_fp64_error": {"force_max_rel": err_f, "phi_max_rel": err_p, "gate": 1e-6},
         "adjoint_over_forward": None if adj is None else adj["ratio"],
         "adjoint": adj,
+        "batched": batched,
         "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
                 "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,
                 "ms_per_step": e2e_ms},

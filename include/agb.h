@@ -263,6 +263,35 @@ int agb_eval_static(const agb_component* comps, int n_comps,
                     int out_flags, void* stream);
 
 /*
+ * Batched evaluation of many independent work units in ONE launch: unit u is a
+ * potential (its leaves [unit_leaf_offsets[u], unit_leaf_offsets[u+1]) of
+ * `leaves`, which index `comps`) evaluated at its own points, rows
+ * [point_offsets[u], point_offsets[u+1]) of one shared xyz array.  The plan
+ * uploads the descriptors once (it owns that device memory until
+ * agb_batch_destroy) and cuts the units into tiles of at most tile_points
+ * points (0: 2048), ordered by estimated cost, largest first.  agb_batch_eval
+ * then launches one persistent kernel whose blocks take tiles from a device
+ * work queue (an atomic counter reset by a memset node before the launch), so
+ * a call makes no host-side copies or allocations.  One plan serves one stream
+ * at a time (the queue counter is per plan).  Modes POT/GRAD/HESS/DENS; the
+ * precision is fixed per plan.  Results equal per-unit agb_eval calls point by
+ * point.  Replaces the per-potential launch loop a caller of the reference
+ * writes around gpu_potential.py:826-935 (one call per potential and point
+ * set); the reference has no batched entry point.
+ */
+typedef struct agb_batch agb_batch;
+int agb_batch_create(const agb_component* comps, int n_comps,
+                     const agb_leaf* leaves, const int32_t* unit_leaf_offsets, int n_units,
+                     const int64_t* point_offsets, int precision, int tile_points,
+                     agb_batch** out);
+int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode,
+                   double* phi, double* grad, double* hess, double* rho,
+                   int out_flags, void* stream);
+int64_t agb_batch_points(const agb_batch* plan);
+int     agb_batch_tiles(const agb_batch* plan);
+void    agb_batch_destroy(agb_batch* plan);
+
+/*
  * Kernel-signature entries.  Arguments are those of the reference kernels, in
  * order, with SoA x, y, z device arrays, the reference's harmonic-major poly
  * layout and lm_l/lm_m arrays sorted as gpu_potential.py:516 sorts them.

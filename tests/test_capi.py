@@ -83,3 +83,47 @@ int main(void) {{
     C, L = _lib.AgbComponent, _lib.AgbLeaf
     assert got == [ctypes.sizeof(C), C.table.offset, C.p.offset, ctypes.sizeof(L),
                    L.sigma.offset, L.gamma.offset, L.ampl.offset]
+
+
+def test_batch_plan_argument_errors_need_no_gpu():
+    """agb_batch_create validates everything on the host before touching a device."""
+    from agama_gpu_b200 import _lib
+    comps = (_lib.AgbComponent * 1)()
+    comps[0].kind = _lib.KIND_NFW
+    leaves = (_lib.AgbLeaf * 2)()
+    h = ctypes.c_void_p()
+    uoff = (ctypes.c_int32 * 3)(0, 1, 2)
+    poff = (ctypes.c_int64 * 3)(0, 10, 5)
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff, 2, poff, 0, 0, ctypes.byref(h))
+    assert rc == -1 and "decrease" in _lib.last_error() and not h.value
+    uoff2 = (ctypes.c_int32 * 3)(0, 1, 1)
+    poff2 = (ctypes.c_int64 * 3)(0, 10, 20)
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff2, 2, poff2, 0, 0, ctypes.byref(h))
+    assert rc == -1 and "no leaves" in _lib.last_error()
+    leaves[1].comp = 4
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff, 2, poff2, 0, 0, ctypes.byref(h))
+    assert rc == -1 and "refers to component" in _lib.last_error()
+    leaves[1].comp = 0
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff, 2, poff2, 7, 0, ctypes.byref(h))
+    assert rc == -1 and "precision" in _lib.last_error()
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff, 2, poff2, 0, 8, ctypes.byref(h))
+    assert rc == -1 and "tile_points" in _lib.last_error()
+    comps[0].kind = 99
+    rc = _lib.lib.agb_batch_create(comps, 1, leaves, uoff, 2, poff2, 0, 0, ctypes.byref(h))
+    assert rc == -1 and "unknown component kind" in _lib.last_error()
+    assert _lib.lib.agb_batch_eval(None, None, 1, None, None, None, None, 0, None) == -1
+    assert _lib.lib.agb_batch_points(None) == -1
+
+
+def test_batch_class_validation_needs_no_gpu():
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import circular_track
+    nfw = agb.NFWPotentialGPU(mass=1e12, scaleRadius=20.0)
+    with pytest.raises(ValueError):
+        agb.BatchedPotentialGPU([nfw, nfw], [10])
+    with pytest.raises(ValueError):
+        agb.BatchedPotentialGPU([agb.ShiftedPotentialGPU(nfw, circular_track(T=50))], [10])
+    b = agb.BatchedPotentialGPU([nfw, nfw], [3, 4])
+    assert b.n_points == 7 and b.unit_rows(1) == slice(3, 7)
+    with pytest.raises(TypeError):
+        b + nfw

@@ -1,0 +1,124 @@
+"""Batched work units (one launch, device work queue) against per-unit calls."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from helpers import cs_coefs
+
+pytestmark = pytest.mark.gpu
+
+
+def _units():
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    rng = np.random.default_rng(5)
+    cs = agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))
+    units = []
+    for u in range(37):
+        k = u % 6
+        if k == 0:
+            lmax = int(rng.integers(2, 17))
+            units.append(agb.MultipolePotentialGPU(nfw_multipole(
+                lmax=lmax, n_nodes=int(rng.integers(30, 90)), M=10 ** rng.uniform(10, 12),
+                rs=rng.uniform(2, 30), seed=u, amp=0.3)))
+        elif k == 1:
+            units.append(agb.NFWPotentialGPU(mass=10 ** rng.uniform(10, 12), scaleRadius=rng.uniform(2, 30)))
+        elif k == 2:
+            units.append(agb.MultipolePotentialGPU(nfw_multipole(lmax=6, n_nodes=40, seed=u, amp=0.3))
+                         + agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3))
+        elif k == 3:
+            units.append(agb.ShiftedPotentialGPU(
+                agb.MultipolePotentialGPU(nfw_multipole(lmax=4, n_nodes=30, seed=u, amp=0.3)),
+                [1.0, -2.0, 0.5]))
+        elif k == 4:
+            units.append(cs)                      # the same component in several units
+        else:
+            units.append(agb.ScaledPotentialGPU(agb.HernquistPotentialGPU(mass=1e11, scaleRadius=4.0),
+                                                1.5, 0.7))
+    counts = rng.integers(0, 3000, len(units))
+    counts[3] = 0
+    counts[10] = 1
+    counts[11] = 256
+    return units, counts
+
+
+def _points(n, seed):
+    rng = np.random.default_rng(seed)
+    r = np.exp(rng.uniform(np.log(0.05), np.log(500.0), n))
+    u = rng.normal(size=(n, 3))
+    return u / np.linalg.norm(u, axis=1)[:, None] * r[:, None]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_batch_matches_per_unit_calls(prec, mode):
+    import torch
+    import agama_gpu_b200 as agb
+    units, counts = _units()
+    batch = agb.BatchedPotentialGPU(units, counts, tile_points=256)
+    x = torch.from_numpy(_points(batch.n_points, 6)).cuda()
+    got = batch._launch(x, 0.0, mode, True, precision=prec)
+    assert batch.tiles(prec) == int(sum((c + 255) // 256 for c in counts))
+    for u, pot in enumerate(units):
+        rows = batch.unit_rows(u)
+        if rows.stop == rows.start:
+            continue
+        want = pot._launch(x[rows].contiguous(), 0.0, mode, True, precision=prec)
+        for g, w in zip(got, want):
+            if w is None:
+                continue
+            g = g[rows]
+            scale = float(w.abs().max()) or 1.0
+            err = float((g - w).abs().max()) / scale
+            assert err <= 1e-14, (u, err)
+
+
+def test_batch_many_small_units_and_two_calls():
+    import torch
+    import agama_gpu_b200 as agb
+    rng = np.random.default_rng(9)
+    units = [agb.PlummerPotentialGPU(mass=10 ** rng.uniform(9, 11), scaleRadius=rng.uniform(0.5, 5))
+             for _ in range(600)]
+    counts = rng.integers(1, 50, 600)
+    batch = agb.BatchedPotentialGPU(units, counts, tile_points=32)
+    x = torch.from_numpy(_points(batch.n_points, 10)).cuda()
+    f1 = batch.force(x)
+    f2 = batch.force(x)
+    assert torch.equal(f1, f2)                 # the work queue is reset between calls
+    for u in (0, 17, 599):
+        rows = batch.unit_rows(u)
+        w = units[u].force(x[rows])
+        assert float((f1[rows] - w).abs().max()) <= 1e-14 * float(w.abs().max())
+
+
+def test_batch_leapfrog_graph_matches_per_unit():
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    rng = np.random.default_rng(12)
+    units = [agb.MultipolePotentialGPU(nfw_multipole(lmax=int(l), n_nodes=50, seed=int(l), amp=0.3))
+             for l in (2, 6, 10)]
+    counts = [500, 1200, 700]
+    batch = agb.BatchedPotentialGPU(units, counts)
+    n = batch.n_points
+    R = rng.uniform(5, 30, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    x0 = torch.from_numpy(np.stack([R * np.cos(ph), R * np.sin(ph), rng.normal(0, 1, n)], 1)).cuda()
+    v0 = torch.from_numpy(np.stack([-150 * np.sin(ph), 150 * np.cos(ph), rng.normal(0, 5, n)], 1)).cuda()
+    integ = Leapfrog(batch, 0.002, graph_steps=10)
+    assert integ.use_graph
+    xT, vT, _ = integ.run(x0, v0, 40, checkpoint_every=64)
+    for u, pot in enumerate(units):
+        rows = batch.unit_rows(u)
+        xu, vu, _ = Leapfrog(pot, 0.002, use_graph=False).run(x0[rows], v0[rows], 40, checkpoint_every=64)
+        assert float((xT[rows] - xu).abs().max()) <= 1e-10 * float(xu.abs().max())
+        assert float((vT[rows] - vu).abs().max()) <= 1e-10 * float(vu.abs().max())
+
+
+def test_batch_rejects_wrong_size():
+    import torch
+    import agama_gpu_b200 as agb
+    batch = agb.BatchedPotentialGPU([agb.NFWPotentialGPU(mass=1e12, scaleRadius=20.0)], [10])
+    with pytest.raises(ValueError):
+        batch.force(torch.zeros((11, 3), dtype=torch.float64, device="cuda"))
