@@ -12,6 +12,13 @@
 // finishing a cheap tile immediately takes the next, so the expensive units
 // (high lmax, many points) start first and the tail is made of small tiles.
 
+// Within a tile the points are counting-sorted in shared memory by the radial
+// interval of the unit's heaviest Multipole (the per-call binning of agb_eval,
+// done here per tile with no global scratch), so a warp's lanes read the same
+// interval's coefficients.
+#define AGB_BATCH_SORT_MAX 4096        // largest tile that is sorted
+#define AGB_BATCH_MAX_BINS 256         // most intervals (+2) of a sorted unit
+
 struct BatchTile {
     long long start;          // first point (row of xyz)
     int unit;
@@ -23,6 +30,7 @@ struct BatchArgs {
     const DevLeaf* leaves;    // device [n_leaves], comp indexes comps
     const int* unit_leaf;     // device [n_units + 1]
     const BatchTile* tiles;   // device [n_tiles], largest cost first
+    const BinKey* ukey;       // device [n_units]: sort key of the unit (n_int < 0: none)
     int* counter;             // device, zero at launch
     int n_tiles;
     int out_flags;
@@ -38,6 +46,8 @@ __global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS) ? 1 : 2)
 agb_batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ int s_tile;
+    __shared__ int s_hist[AGB_BATCH_MAX_BINS], s_cur[AGB_BATCH_MAX_BINS];
+    __shared__ unsigned short s_key[AGB_BATCH_SORT_MAX], s_order[AGB_BATCH_SORT_MAX];
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(a.counter, 1);
         __syncthreads();
@@ -46,8 +56,43 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         if (t >= a.n_tiles) return;
         const BatchTile T = a.tiles[t];
         const int l0 = a.unit_leaf[T.unit], l1 = a.unit_leaf[T.unit + 1];
+        const BinKey K = a.ukey[T.unit];
+        const int nb = K.n_int + 2;
+        const bool sorted = K.n_int >= 0 && nb <= AGB_BATCH_MAX_BINS && T.count <= AGB_BATCH_SORT_MAX;
+        if (sorted) {
+            for (int q = threadIdx.x; q < nb; q += blockDim.x) s_hist[q] = 0;
+            __syncthreads();
+            for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
+                const long long i = T.start + j;
+                const int k = bin_of(K, a.xyz[3 * i], a.xyz[3 * i + 1], a.xyz[3 * i + 2]);
+                s_key[j] = (unsigned short)k;
+                atomicAdd(&s_hist[k], 1);
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {        // exclusive scan of <= 256 bins by one warp
+                const int lane = threadIdx.x, b0 = lane * (AGB_BATCH_MAX_BINS / 32);
+                int loc = 0;
+                for (int q = 0; q < AGB_BATCH_MAX_BINS / 32; ++q)
+                    loc += (b0 + q < nb) ? s_hist[b0 + q] : 0;
+                int inc = loc;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, inc, d);
+                    if (lane >= d) inc += v;
+                }
+                int run = inc - loc;
+                for (int q = 0; q < AGB_BATCH_MAX_BINS / 32; ++q)
+                    if (b0 + q < nb) {
+                        s_cur[b0 + q] = run;
+                        run += s_hist[b0 + q];
+                    }
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < T.count; j += blockDim.x)
+                s_order[atomicAdd(&s_cur[s_key[j]], 1)] = (unsigned short)j;
+            __syncthreads();
+        }
         for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
-            const long long i = T.start + j;
+            const long long i = T.start + (sorted ? (int)s_order[j] : j);
             const double x = a.xyz[3 * i], y = a.xyz[3 * i + 1], z = a.xyz[3 * i + 2];
             double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
             double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -100,11 +145,12 @@ struct agb_batch {
     int n_units;
     int n_tiles;
     int64_t n_points;
-    void* mem;                // one device allocation: comps | leaves | unit_leaf | tiles | counter
+    void* mem;                // one device allocation: comps, leaves, unit_leaf, tiles, keys, counter
     const DevComp* comps;
     const DevLeaf* leaves;
     const int* unit_leaf;
     const BatchTile* tiles;
+    const BinKey* ukey;
     int* counter;
 };
 
@@ -152,8 +198,9 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
     DevComp* hc = (DevComp*)calloc((size_t)n_comps, sizeof(DevComp));
     DevLeaf* hl = (DevLeaf*)calloc((size_t)n_leaves, sizeof(DevLeaf));
     double* ucost = (double*)calloc((size_t)n_units, sizeof(double));
-    if (!hc || !hl || !ucost) {
-        free(hc); free(hl); free(ucost);
+    BinKey* hk = (BinKey*)calloc((size_t)n_units, sizeof(BinKey));
+    if (!hc || !hl || !ucost || !hk) {
+        free(hc); free(hl); free(ucost); free(hk);
         return set_err(AGB_ERR_DEVICE, "agb_batch_create: host allocation failed");
     }
     int rc = AGB_OK;
@@ -166,8 +213,24 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
     }
     long long n_tiles = 0;
     for (int u = 0; u < n_units && !rc; ++u) {
-        for (int L = unit_leaf_offsets[u]; L < unit_leaf_offsets[u + 1]; ++L)
-            ucost[u] += leaf_cost(comps[leaves[L].comp]);
+        int best = -1;
+        for (int L = unit_leaf_offsets[u]; L < unit_leaf_offsets[u + 1]; ++L) {
+            const agb_component& c = comps[leaves[L].comp];
+            ucost[u] += leaf_cost(c);
+            if (c.kind == AGB_KIND_MULTIPOLE && c.n_lm >= 2 &&
+                (best < 0 || c.n_lm > comps[leaves[best].comp].n_lm))
+                best = L;
+        }
+        hk[u].n_int = -1;
+        if (best >= 0) {
+            const agb_component& c = comps[leaves[best].comp];
+            hk[u].sigma = leaves[best].sigma;
+            hk[u].g0 = leaves[best].gamma[0]; hk[u].g1 = leaves[best].gamma[1];
+            hk[u].g2 = leaves[best].gamma[2];
+            hk[u].logr_min = c.p[0];
+            hk[u].inv_dlogr = c.p[2];
+            hk[u].n_int = c.n_int;
+        }
         n_tiles += (point_offsets[u + 1] - point_offsets[u] + tile_points - 1) / tile_points;
     }
     if (!rc && n_tiles > 0x7fffffffLL)
@@ -194,7 +257,8 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
     const size_t o_l = al256(o_c + sizeof(DevComp) * (size_t)n_comps);
     const size_t o_u = al256(o_l + sizeof(DevLeaf) * (size_t)n_leaves);
     const size_t o_t = al256(o_u + sizeof(int) * (size_t)(n_units + 1));
-    const size_t o_k = al256(o_t + sizeof(BatchTile) * (size_t)(n_tiles > 0 ? n_tiles : 1));
+    const size_t o_y = al256(o_t + sizeof(BatchTile) * (size_t)(n_tiles > 0 ? n_tiles : 1));
+    const size_t o_k = al256(o_y + sizeof(BinKey) * (size_t)n_units);
     const size_t bytes = o_k + 256;
     agb_batch* p = nullptr;
     if (!rc) {
@@ -217,6 +281,8 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
         if (n_tiles > 0)
             ok = ok && cudaMemcpy(m + o_t, ht, sizeof(BatchTile) * (size_t)n_tiles,
                                   cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && cudaMemcpy(m + o_y, hk, sizeof(BinKey) * (size_t)n_units,
+                              cudaMemcpyHostToDevice) == cudaSuccess;
         ok = ok && cudaMemset(m + o_k, 0, 256) == cudaSuccess;
         if (!ok) rc = set_err(AGB_ERR_DEVICE, "agb_batch_create: upload of the plan failed");
         p->precision = precision;
@@ -227,9 +293,10 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
         p->leaves = (const DevLeaf*)(m + o_l);
         p->unit_leaf = (const int*)(m + o_u);
         p->tiles = (const BatchTile*)(m + o_t);
+        p->ukey = (const BinKey*)(m + o_y);
         p->counter = (int*)(m + o_k);
     }
-    free(hc); free(hl); free(ucost); free(ht);
+    free(hc); free(hl); free(ucost); free(hk); free(ht);
     if (rc) {
         if (p) {
             if (p->mem) cudaFree(p->mem);
@@ -295,7 +362,8 @@ extern "C" int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode
     cudaStream_t st = (cudaStream_t)stream;
     BatchArgs a;
     a.comps = plan->comps; a.leaves = plan->leaves; a.unit_leaf = plan->unit_leaf;
-    a.tiles = plan->tiles; a.counter = plan->counter; a.n_tiles = plan->n_tiles;
+    a.tiles = plan->tiles; a.ukey = plan->ukey; a.counter = plan->counter;
+    a.n_tiles = plan->n_tiles;
     a.out_flags = out_flags; a.xyz = xyz;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
     if (cudaMemsetAsync(plan->counter, 0, sizeof(int), st) != cudaSuccess)
