@@ -16,6 +16,9 @@ MODE_POT, MODE_GRAD, MODE_HESS, MODE_DENS, MODE_VJP = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 OUT_NEGATE = 1
 OUT_NO_BINNING = 2
+OUT_BIN_ALWAYS = 4
+OUT_GRID_SHIFT = 8
+BIN_MIN_POINTS = 16384
 
 KIND_MULTIPOLE = 1
 KIND_CYLSPLINE = 2

@@ -137,7 +137,8 @@ class BatchedPotentialGPU(_GPUPotBase):
     def _leaves(self, t: float):
         raise TypeError("a batch is not one potential tree; evaluate it as a whole")
 
-    def __del__(self):
+    def _release_plans(self) -> None:
+        """Destroy the device plans (after the device has finished using them)."""
         plans = getattr(self, "_plans", {})
         for (dev_index, _), h in plans.items():
             try:
@@ -147,6 +148,11 @@ class BatchedPotentialGPU(_GPUPotBase):
             except Exception:   # interpreter shutdown
                 pass
         self._plans = {}
+        # CUDA graphs captured over the old plans must not replay them
+        self.plan_generation = getattr(self, "plan_generation", 0) + 1
+
+    def __del__(self):
+        self._release_plans()
 
 
 def _default() -> str:

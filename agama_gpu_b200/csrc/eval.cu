@@ -183,7 +183,8 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
     }
     (void)grid_for(a.n);      // reads the SM count once
     const long long want = (a.n + 255) / 256;
-    const long long slots = (long long)g_num_sms * per_sm * AGB_EVAL_WAVES;
+    const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
+    const long long slots = (long long)g_num_sms * per_sm * (w ? w : AGB_EVAL_WAVES);
     const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
     a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
     agb_eval_kernel<MODE, R><<<(int)grid, 256, 0, st>>>(a);
@@ -264,7 +265,8 @@ static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, 
 {
     BinPlan b;
     memset(&b, 0, sizeof(b));
-    if ((out_flags & AGB_OUT_NO_BINNING) || n < AGB_BIN_MIN_POINTS || n > 0x7fffffffLL) return b;
+    if ((out_flags & AGB_OUT_NO_BINNING) || n > 0x7fffffffLL) return b;
+    if (n < AGB_BIN_MIN_POINTS && !(out_flags & AGB_OUT_BIN_ALWAYS)) return b;
     int best = -1, best_lm = 0;
     for (int L = 0; L < n_leaves; ++L) {
         const agb_component& c = comps[leaves[L].comp];

@@ -106,7 +106,8 @@ class Leapfrog:
             for k in range(n_steps):
                 self._step(x, v, F, self.t0 + (n0 + k) * self.dt)
             return
-        key = (x.data_ptr(), v.data_ptr(), F.data_ptr(), x.shape[0])
+        key = (x.data_ptr(), v.data_ptr(), F.data_ptr(), x.shape[0],
+               getattr(self.pot, "plan_generation", 0))
         if self._graph is None or self._graph_key != key:
             self._capture(x, v, F)
             self._graph_key = key

@@ -167,12 +167,16 @@ class _GPUPotBase:
             lf.ampl = ampl
         return (_lib.AgbComponent * len(comps))(*comps), len(comps), leaf_arr, len(leaves)
 
-    def _flags(self) -> int:
-        return _lib.OUT_NEGATE | (0 if self.binning else _lib.OUT_NO_BINNING)
+    def _flags(self, mode: int = -1, prec: int = -1, n: int = 0) -> int:
+        f = _lib.OUT_NEGATE | (0 if self.binning else _lib.OUT_NO_BINNING)
+        tuned = self.__dict__.get("_tuned")
+        if tuned:                   # launch shape chosen by autotune.autotune()
+            f |= tuned.get((mode, prec, int(n).bit_length()), 0)
+        return f
 
-    def _workspace(self, cargs, n: int, dev: torch.device):
+    def _workspace(self, cargs, n: int, dev: torch.device, flags: int):
         nws = int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3], n,
-                                                    self._flags()))
+                                                    flags))
         return (torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None), nws
 
     def _launch(self, arr: torch.Tensor, t: float, mode: int, want_phi: bool,
@@ -199,9 +203,10 @@ class _GPUPotBase:
             return phi, grad, hess, rho
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         stream = torch.cuda.current_stream(dev).cuda_stream
-        ws, nws = self._workspace(cargs, n, dev)
+        flags = self._flags(mode, prec, n)
+        ws, nws = self._workspace(cargs, n, dev, flags)
         rc = _lib.lib.agb_eval_ws(*cargs, arr.data_ptr(), n, mode, prec, ptr(phi), ptr(grad),
-                                  ptr(hess), ptr(rho), self._flags(), ptr(ws), nws,
+                                  ptr(hess), ptr(rho), flags, ptr(ws), nws,
                                   ctypes.c_void_p(stream))
         _lib.check(rc, "agb_eval_ws")
         return phi, grad, hess, rho
@@ -220,7 +225,7 @@ class _GPUPotBase:
         gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
         gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
-        ws, nws = self._workspace(cargs, n, dev)
+        ws, nws = self._workspace(cargs, n, dev, 0)       # agb_eval_vjp sorts by default
         rc = _lib.lib.agb_eval_vjp(*cargs, arr.data_ptr(), n, prec, ptr(gp), ptr(gf), gx.data_ptr(),
                                    ptr(ws), nws,
                                    ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))

@@ -58,6 +58,12 @@ extern "C" {
 /* output flags for agb_eval */
 #define AGB_OUT_NEGATE     1   /* write -grad (force) and -Hessian (forceDeriv layout) */
 #define AGB_OUT_NO_BINNING 2   /* evaluate the points in input order (no scratch memory) */
+#define AGB_OUT_BIN_ALWAYS 4   /* sort by interval even below AGB_BIN_MIN_POINTS points */
+/* bits 8-11: blocks per resident slot of the evaluation kernel's grid, 1-15
+   (0: the default, 4).  Results do not depend on it: a launch-shape knob for
+   the autotuner (agama_gpu_b200/autotune.py).  No counterpart in the reference. */
+#define AGB_OUT_GRID_SHIFT 8
+#define AGB_OUT_GRID(w)    (((w) & 15) << AGB_OUT_GRID_SHIFT)
 
 /* agb_eval sorts the points by the radial interval of its heaviest Multipole
    leaf (a counting sort in device scratch) when there are at least this many */

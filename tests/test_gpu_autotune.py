@@ -1,0 +1,59 @@
+"""Autotuner: every launch shape gives the same results; the choice is kept and cached."""
+import json
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _pot():
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    return (agb.MultipolePotentialGPU(nfw_multipole(lmax=10, n_nodes=60, seed=3, amp=0.3))
+            + agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3))
+
+
+@pytest.mark.parametrize("n", [5000, 70000])
+def test_launch_shapes_agree(n, tmp_path, monkeypatch):
+    import torch
+    from agama_gpu_b200 import _lib, autotune
+    monkeypatch.setenv("AGB_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    pot = _pot()
+    from agama_gpu_b200.synthetic import hernquist_points
+    x = torch.from_numpy(hernquist_points(n, 10.0, 4)).cuda()
+    ref = pot.force(x)
+    for prec in ("fp64", "mixed"):
+        base = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
+        for name, flags in autotune._candidates(n):
+            autotune._set(pot, _lib.MODE_GRAD, _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED,
+                          n, flags)
+            got = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
+            for g, b in zip(got[:2], base[:2]):
+                assert float((g - b).abs().max()) <= 1e-14 * float(b.abs().max()), (prec, name)
+        pot.__dict__.pop("_tuned", None)
+    res = autotune.autotune(pot, x, mode="force", precision="mixed", reps=2)
+    assert res["best"] in res["ms"] and len(res["ms"]) == 2 * len(autotune.GRIDS)
+    assert (_lib.MODE_GRAD, _lib.PREC_MIXED, n.bit_length()) in pot._tuned
+    assert torch.equal(pot.force(x), ref)                 # fp64 calls keep their own shape
+    rec = json.loads((tmp_path / "cache.json").read_text())
+    assert len(rec) == 1
+    fresh = _pot()
+    assert autotune.apply_cached(fresh, n, mode="force", precision="mixed")
+    assert fresh._tuned == pot._tuned
+
+
+def test_tune_batch_keeps_results():
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import autotune
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    units = [agb.MultipolePotentialGPU(nfw_multipole(lmax=l, n_nodes=40, seed=l, amp=0.3))
+             for l in (2, 8, 14)]
+    batch = agb.BatchedPotentialGPU(units, [3000, 9000, 500])
+    x = torch.from_numpy(hernquist_points(batch.n_points, 8.0, 5)).cuda()
+    f0 = batch.force(x)
+    res = autotune.tune_batch(batch, x, tiles=(256, 2048, 8192))
+    assert batch.tile_points == res["best"]
+    f1 = batch.force(x)
+    assert float((f1 - f0).abs().max()) <= 1e-14 * float(f0.abs().max())
