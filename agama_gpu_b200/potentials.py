@@ -361,6 +361,91 @@ class _GPUPotBase:
             res.append(_sq(d, single))
         return res[0] if len(res) == 1 else tuple(res)
 
+    def eval_host(self, xyz, pot: bool = False, acc: bool = False, der: bool = False,
+                  t: float = 0.0, chunk_points: Optional[int] = None, out=None, device=None):
+        """``eval`` for positions and results in HOST memory, pipelined.
+
+        The points go through the GPU in chunks of ``chunk_points`` (default: N/6,
+        clamped to [2^17, 2^20] points, so a chunk still fills the GPU): while chunk i
+        is evaluated, chunk i+1 is copied in and chunk i-1's results are copied
+        out (three CUDA streams, two device buffers per stream stage), so the
+        PCIe transfers hide behind the kernel.  xyz: (N,3) float64 CPU tensor or
+        NumPy array -- pinned memory (``tensor.pin_memory()``) makes the copies
+        asynchronous; pageable memory works, without the overlap.  Returns CPU
+        tensors in eval()'s order (pinned unless ``out`` gives the buffers:
+        a tuple matching the requested outputs).  The host waits for the
+        results before returning.  No counterpart in the reference (its API
+        returns device arrays only).
+        """
+        if not (pot or acc or der):
+            raise ValueError("eval_host(): at least one of pot, acc, der must be True.")
+        src = xyz if isinstance(xyz, torch.Tensor) else torch.from_numpy(
+            np.ascontiguousarray(xyz, dtype=np.float64))
+        if src.device.type != "cpu":
+            raise ValueError("eval_host() takes host (CPU) positions; use eval() for device arrays")
+        src = src.to(torch.float64).contiguous()
+        if src.dim() != 2 or src.shape[1] != 3:
+            raise ValueError(f"xyz must have shape (N,3), got {tuple(src.shape)}")
+        n = src.shape[0]
+        dev = _cuda_device(device)
+        mode = _lib.MODE_HESS if der else (_lib.MODE_GRAD if acc else _lib.MODE_POT)
+        want = [(pot, (n,), 0), (acc, (n, 3), 1), (der, (n, 6), 2)]
+        if out is None:
+            host = [torch.empty(shape, dtype=torch.float64, pin_memory=True) if w else None
+                    for w, shape, _ in want]
+        else:
+            outs = list(out) if isinstance(out, (tuple, list)) else [out]
+            host = []
+            for w, shape, _ in want:
+                host.append(outs.pop(0) if w else None)
+            for h, (w, shape, _) in zip(host, want):
+                if w and (h is None or tuple(h.shape) != shape or h.dtype != torch.float64
+                          or h.device.type != "cpu" or not h.is_contiguous()):
+                    raise ValueError(f"out buffer must be a contiguous float64 CPU tensor {shape}")
+        if chunk_points is None:
+            chunk_points = min(1 << 20, max(1 << 17, -(-n // 6)))
+        chunk = max(1, min(int(chunk_points), max(n, 1)))
+        cur = torch.cuda.current_stream(dev)
+        s_in, s_cmp, s_out = (torch.cuda.Stream(device=dev) for _ in range(3))
+        for s in (s_in, s_cmp, s_out):
+            s.wait_stream(cur)
+        f64 = dict(dtype=torch.float64, device=dev)
+        with torch.cuda.device(dev):
+            xb = [torch.empty((chunk, 3), **f64) for _ in range(2)]
+            ob = [[torch.empty((chunk,) + shape[1:], **f64) if w else None
+                   for w, shape, _ in want] for _ in range(2)]
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_cmp = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [torch.cuda.Event() for _ in range(2)]
+        started = [False, False]
+        for i, lo in enumerate(range(0, n, chunk)):
+            b = i & 1
+            hi = min(n, lo + chunk)
+            m = hi - lo
+            with torch.cuda.stream(s_in):
+                if started[b]:
+                    s_in.wait_event(ev_cmp[b])          # the kernel is done with xb[b]
+                xb[b][:m].copy_(src[lo:hi], non_blocking=True)
+                ev_in[b].record(s_in)
+            with torch.cuda.stream(s_cmp):
+                s_cmp.wait_event(ev_in[b])
+                if started[b]:
+                    s_cmp.wait_event(ev_out[b])      # the results of chunk i-2 are out
+                p_, f_, d_ = (ob[b][k][:m] if ob[b][k] is not None else None for k in range(3))
+                self._launch(xb[b][:m], t, mode, pot, out=(p_, f_, d_, None))
+                ev_cmp[b].record(s_cmp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_cmp[b])
+                for k in range(3):
+                    if host[k] is not None:
+                        host[k][lo:hi].copy_(ob[b][k][:m], non_blocking=True)
+                ev_out[b].record(s_out)
+            started[b] = True
+        cur.wait_stream(s_out)          # later work on the caller's stream sees the results
+        s_out.synchronize()
+        res = [h for h in host if h is not None]
+        return res[0] if len(res) == 1 else tuple(res)
+
 
 class _Component(_GPUPotBase):
     """A leaf: one component with device tables."""
