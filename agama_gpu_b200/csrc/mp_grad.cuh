@@ -454,21 +454,23 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
         auto acc = [&](int L) {
             const R ll1 = R(L * (L + 1));
             const R Pos = fma(Pc, inv_sth, q1 * dPc);
-            const R d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
             const R base = fma(P3, dPc, P1 * Pc);
             const R Pq = P4 * Pos;
-            R a[6];
-            MPPtr<R>::load(rec, a);
-            rec += MPPtr<R>::REC;
-            mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            // FP32 m>0 records are interleaved (cos, sin): both come in one load;
+            // FP64 loads the sin record only when it is needed (register pressure)
+            constexpr bool F32 = std::is_same<R, float>::value;
+            R a[6], b[6];
+            if (F32 && m > 0) MPPtr<R>::load_cs(rec, a, b);
+            else MPPtr<R>::load(rec, a);
+            mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, ll1);
             adj_put<R>(T, gbase, col++, sp, dw, fma(Tc, base, dTc * Pq), P2 * Pc * Tc, lane, active);
             if (m > 0) {
-                MPPtr<R>::load(rec, a);
-                rec += MPPtr<R>::REC;
-                mp_col_acc<MODE, R>(gs, a, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+                if (!F32) MPPtr<R>::load(rec + MPPtr<R>::REC, b);
+                mp_col_acc<MODE, R>(gs, b, sp, dw, ew, Pc, dPc, ll1);
                 adj_put<R>(T, gbase, col++, sp, dw, fma(Ts, base, dTs * Pq), P2 * Pc * Ts, lane,
                            active);
             }
+            rec += (m > 0 ? 2 : 1) * MPPtr<R>::REC;
         };
         int l = m;
         while (l < l0) step(++l);
@@ -478,6 +480,8 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
             step(l);
             acc(l);
         }
+        mp_col_finish<MODE, R>(gc, inv_sth, q1, np1, cot, m2);
+        mp_col_finish<MODE, R>(gs, inv_sth, q1, np1, cot, m2);
         const double md = (double)m;
         const double ddTc = -md * sm, ddTs = md * cm;
         tot.A += (double)gc.V * cm + (double)gs.V * sm;

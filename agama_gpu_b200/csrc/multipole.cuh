@@ -233,6 +233,12 @@ template <> struct MPPtr<double> {
         const double2 v0 = __ldg(q), v1 = __ldg(q + 1), v2 = __ldg(q + 2);
         a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y; a[4] = v2.x; a[5] = v2.y;
     }
+    // the cos and sin records of an m>0 harmonic (consecutive columns)
+    static __device__ __forceinline__ void load_cs(const double* p, double c[6], double s[6])
+    {
+        load(p, c);
+        load(p + REC, s);
+    }
 };
 template <> struct MPPtr<float> {
     static constexpr int REC = 8;
@@ -246,6 +252,16 @@ template <> struct MPPtr<float> {
         const float4 v0 = __ldg(q), v1 = __ldg(q + 1);
         a[0] = v0.x; a[1] = v0.y; a[2] = v0.z; a[3] = v0.w; a[4] = v1.x; a[5] = v1.y;
     }
+    // an m>0 harmonic's cos and sin records, stored interleaved in the FP32
+    // table of a regular structure: c0 s0 c1 s1 ... c5 s5 (+4 pads)
+    static __device__ __forceinline__ void load_cs(const float* p, float c[6], float s[6])
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        const float4 v0 = __ldg(q), v1 = __ldg(q + 1), v2 = __ldg(q + 2);
+        c[0] = v0.x; s[0] = v0.y; c[1] = v0.z; s[1] = v0.w;
+        c[2] = v1.x; s[2] = v1.y; c[3] = v1.z; s[3] = v1.w;
+        c[4] = v2.x; s[4] = v2.y; c[5] = v2.z; s[5] = v2.w;
+    }
 };
 
 template <typename R> struct MPCol {         // per-group sums of one trig column (cos or sin)
@@ -253,10 +269,15 @@ template <typename R> struct MPCol {         // per-group sums of one trig colum
     __device__ __forceinline__ void zero() { V = VR = VRR = VT = VTT = VRT = VP = L = R(0); }
 };
 
+// Per l the walk accumulates C*Y, C'*Y, C*dY (and C''*Y, C'*dY, l(l+1) C*Y for
+// the second derivatives); the two angular sums that need Y/sin(theta) and
+// d2Y/dtheta2 follow from those once per |m| group, because inside a group
+//   Y/sin         = Y inv_sth + q1 dY              (q1: the m=1 pole rule)
+//   d2Y/dtheta2   = np1 (-cot dY - (l(l+1) - m^2/sin^2) Y)
+// (the Legendre equation) have coefficients that do not depend on l.
 template <int MODE, typename R>
 __device__ __forceinline__ void mp_col_acc(MPCol<R>& g, const R a[6], const R sp[6],
-                                           const R dw[6], const R ew[6], R Y, R dY, R d2Y,
-                                           R Pos, R ll1)
+                                           const R dw[6], const R ew[6], R Y, R dY, R ll1)
 {
     constexpr bool NEED_B = MODE != AGB_MODE_POT;
     constexpr bool NEED_D = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
@@ -273,12 +294,16 @@ __device__ __forceinline__ void mp_col_acc(MPCol<R>& g, const R a[6], const R sp
         const R d2C = fma(a[3], ew[3], R(2) * a[2]) + fma(a[5], ew[5], a[4] * ew[4]);
         g.VRR = fma(d2C, Y, g.VRR);
     }
-    if (MODE == AGB_MODE_DENS) g.L = fma(ll1 * C, Y, g.L);
-    if (NEED_ANG) {
-        g.VT = fma(C, dY, g.VT);
-        g.VP = fma(C, Pos, g.VP);
-        if (MODE == AGB_MODE_HESS) g.VTT = fma(C, d2Y, g.VTT);
-    }
+    if (MODE == AGB_MODE_DENS || MODE == AGB_MODE_HESS) g.L = fma(ll1 * C, Y, g.L);
+    if (NEED_ANG) g.VT = fma(C, dY, g.VT);
+}
+
+// the group's Y/sin and d2Y/dtheta2 sums from its accumulators (see above)
+template <int MODE, typename R>
+__device__ __forceinline__ void mp_col_finish(MPCol<R>& g, R inv_sth, R q1, R np1, R cot, R m2)
+{
+    if (MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS) g.VP = fma(g.V, inv_sth, q1 * g.VT);
+    if (MODE == AGB_MODE_HESS) g.VTT = np1 * (fma(-cot, g.VT, m2 * g.V) - g.L);
 }
 
 template <int MODE, typename R, int PAR>
@@ -338,15 +363,12 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
         // the loads of a loop body issue together (no branch inside the body)
         auto acc = [&](int L, auto has_sin) {
             R ac[6], as[6];
-            MPPtr<R>::load(rec, ac);
-            if (has_sin) MPPtr<R>::load(rec + MPPtr<R>::REC, as);
+            if (has_sin) MPPtr<R>::load_cs(rec, ac, as);
+            else MPPtr<R>::load(rec, ac);
             rec += has_sin ? 2 * MPPtr<R>::REC : MPPtr<R>::REC;
             const R ll1 = R(L * (L + 1));
-            R Pos = R(0), d2Y = R(0);
-            if (NEED_ANG) Pos = fma(Pc, inv_sth, q1 * dPc);
-            if (NEED_ANG2) d2Y = np1 * fma(-cot, dPc, -(ll1 - m2) * Pc);
-            mp_col_acc<MODE, R>(gc, ac, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
-            if (has_sin) mp_col_acc<MODE, R>(gs, as, sp, dw, ew, Pc, dPc, d2Y, Pos, ll1);
+            mp_col_acc<MODE, R>(gc, ac, sp, dw, ew, Pc, dPc, ll1);
+            if (has_sin) mp_col_acc<MODE, R>(gs, as, sp, dw, ew, Pc, dPc, ll1);
         };
         auto walk = [&](auto has_sin) {
             int l = m;
@@ -361,6 +383,8 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
         };
         if (m == 0) walk(std::false_type());
         else walk(std::true_type());
+        mp_col_finish<MODE, R>(gc, inv_sth, q1, np1, cot, m2);
+        mp_col_finish<MODE, R>(gs, inv_sth, q1, np1, cot, m2);
         // combine the group's cos and sin sums with cos/sin(m phi) in FP64
         const double md = (double)m;
         const double dTc = -md * sm, dTs = md * cm;

@@ -512,6 +512,18 @@ class MultipolePotentialGPU(_Component):
         self._poly_im = np.ascontiguousarray(poly.transpose(1, 0, 2))
         p32 = np.zeros((t.n_int, self._n_cols, 8), dtype=np.float32)
         p32[:, :, :6] = self._poly_im.astype(np.float32)
+        if reg is not None:
+            # FP32 table of a regular structure: each m>0 (cos, sin) column pair as one
+            # 16-float record, c0 s0 c1 s1 ... c5 s5 + 4 pads (the mixed kernel reads
+            # the pair with packed two-lane loads); m=0 columns keep 8-float records
+            flat = p32.reshape(t.n_int, self._n_cols * 8)
+            for (l, m), c in cols.items():
+                if m > 0:
+                    rec = np.zeros((t.n_int, 16), dtype=np.float32)
+                    rec[:, 0:12:2] = p32[:, c, :6]
+                    rec[:, 1:12:2] = p32[:, c + 1, :6]
+                    flat[:, c * 8:(c + 2) * 8] = rec
+            p32 = flat.reshape(t.n_int, self._n_cols, 8)
         self._poly32 = p32
         self._lm = t.lm_packed()
 

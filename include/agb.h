@@ -101,7 +101,10 @@ extern "C" {
  *
  * MULTIPOLE  (tables from the quintic-spline builder, gpu_potential.py:408-631)
  *   table      FP64 poly, layout per `layout`
- *   table32    FP32 copy of the same polynomials (needed for AGB_PREC_MIXED)
+ *   table32    FP32 copy of the same polynomials (needed for AGB_PREC_MIXED),
+ *              interval-major with 8-float records (a0..a5, 2 pads); with a
+ *              regular structure each m>0 (cos, sin) column pair is one 16-float
+ *              record, cos and sin interleaved: c0 s0 c1 s1 ... c5 s5, 4 pads
  *   lm         packed harmonic list, lm[c] = (l << 16) | (m & 0xffff), sorted by
  *              (|m|, l, cos before sin), lm[0] = (0,0)
  *   n_lm, n_int, lmax, log_scaling, layout
