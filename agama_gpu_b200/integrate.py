@@ -71,6 +71,19 @@ def auto_checkpoint_every(like: torch.Tensor, n_steps: int, fraction: float = 0.
     return max(2, -(-int(n_steps) // fit))
 
 
+def allreduce_table_grads(tg: dict, group=None) -> dict:
+    """Sum the coefficient gradients of every rank (particles sharded across ranks,
+    the potential replicated): one all-reduce per Multipole, in a fixed order so
+    that every rank issues the same collectives.  A no-op without an initialised
+    process group of more than one rank."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) < 2:
+        return tg
+    for key in sorted(tg, key=lambda c: c._sync_order):
+        dist.all_reduce(tg[key], op=dist.ReduceOp.SUM, group=group)
+    return tg
+
+
 class Leapfrog:
     """Integrate N particles; keeps x, v, F as device buffers updated in place."""
 
@@ -191,12 +204,14 @@ class Leapfrog:
 
     # -- adjoint -----------------------------------------------------------------------
     def adjoint(self, ckpts: List, n_steps: int, lam_x: torch.Tensor,
-                lam_v: torch.Tensor, table_grads: bool = False):
+                lam_v: torch.Tensor, table_grads: bool = False, group=None):
         """(dL/dx0, dL/dv0) from (dL/dx_T, dL/dv_T) and the forward's checkpoints.
 
         With table_grads=True also returns {Multipole component: dL/dpoly}, the
         gradient with respect to each Multipole's quintic coefficients summed over
         all force evaluations (component.node_gradients() carries it to the nodes).
+        Under torch.distributed (each rank integrating its own particles in the same
+        potential) the table gradients are summed over the ranks of ``group``.
         """
         tg = {} if table_grads else None
         lx = lam_x.detach().to(torch.float64).contiguous().clone()
@@ -245,7 +260,7 @@ class Leapfrog:
                                       out=gx)
             lx.add_(gx)
         if tg is not None:
-            return lx, lv, self.pot._table_grads_from_device(tg)
+            return lx, lv, allreduce_table_grads(self.pot._table_grads_from_device(tg), group)
         return lx, lv
 
 

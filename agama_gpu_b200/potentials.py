@@ -19,6 +19,7 @@ reference's ``cp.asarray`` does.  Outputs are torch CUDA float64 tensors.
 from __future__ import annotations
 
 import ctypes
+import itertools
 import math
 import os
 import tempfile
@@ -39,6 +40,7 @@ G_AGAMA = 4.30091727067736e-06                    # kpc (km/s)^2 / Msol
 INV_4PIG = 1.0 / (4.0 * math.pi * G_AGAMA)
 
 _PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_MULTIPOLE_SERIAL = itertools.count()
 _default_precision = os.environ.get("AGB_PRECISION", "fp64")
 
 
@@ -489,6 +491,9 @@ class MultipolePotentialGPU(_Component):
     kind = _lib.KIND_MULTIPOLE
 
     def __init__(self, coefs, prune_threshold: float = 1e-16) -> None:
+        # construction order: ranks that build the same potentials in the same order
+        # agree on it, which fixes the order of the gradient all-reduces
+        self._sync_order = next(_MULTIPOLE_SERIAL)
         self.tables = build_multipole_tables(coefs, prune_threshold=prune_threshold)
         self._n_file_cols = len(coefs.lm_labels)
         t = self.tables
