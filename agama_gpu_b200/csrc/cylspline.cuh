@@ -16,6 +16,7 @@
 // (kernel-signature entries) and a cell-major one where the 16 values a
 // harmonic needs in one cell are contiguous (the fused path).
 #pragma once
+#include <type_traits>
 #include "agb_dev.cuh"
 
 __device__ __forceinline__ int cs_cell(double x, const double* __restrict__ g, int n)
@@ -30,15 +31,36 @@ __device__ __forceinline__ int cs_cell(double x, const double* __restrict__ g, i
 }
 
 // Cubic Hermite on [xl, xh] from end values and end slopes (Agama's form).
-__device__ __forceinline__ void cs_hermite(double t, double T, double tT, double h,
-                                           double fl, double fh, double f1l, double f1h,
-                                           double* f, double* df, double* d2f)
+template <typename T>
+__device__ __forceinline__ void cs_hermite(T t, T Tm, T tT, T h, T fl, T fh, T f1l, T f1h,
+                                           T* f, T* df, T* d2f)
 {
-    const double dif = fh - fl;
-    const double Q = 3.0 * (f1l + f1h) - 6.0 * dif / h;
-    if (f) *f = fl * T + fh * t + (dif * (t - T) + (f1l * T - f1h * t) * h) * tT;
-    if (df) *df = f1l * T + f1h * t - Q * tT;
-    if (d2f) *d2f = (f1h - f1l + Q * (t - T)) / h;
+    const T dif = fh - fl;
+    const T Q = T(3) * (f1l + f1h) - T(6) * dif / h;
+    if (f) *f = fl * Tm + fh * t + (dif * (t - Tm) + (f1l * Tm - f1h * t) * h) * tT;
+    if (df) *df = f1l * Tm + f1h * t - Q * tT;
+    if (d2f) *d2f = (f1h - f1l + Q * (t - Tm)) / h;
+}
+
+// One harmonic's bicubic Hermite in a cell: value and lR/lz derivatives from the
+// 16 node values v (layout of cs_load), first along z, then along R.
+template <typename T, bool DO_G, bool DO_H>
+__device__ __forceinline__ void cs_bicubic(const T v[16], T tR, T TR, T tTR, T hR, T tz, T Tz,
+                                           T tTz, T hz, T& val, T& vR, T& vRR, T& vz, T& vRz,
+                                           T& vzz)
+{
+    T F[4], dF[4], d2F[4];
+    const int lo_i[4] = {0, 2, 4, 6}, hi_i[4] = {1, 3, 5, 7};
+    #pragma unroll
+    for (int q = 0; q < 4; ++q)
+        cs_hermite<T>(tz, Tz, tTz, hz, v[lo_i[q]], v[hi_i[q]], v[8 + lo_i[q]], v[8 + hi_i[q]],
+                      &F[q], DO_G ? &dF[q] : nullptr, DO_H ? &d2F[q] : nullptr);
+    cs_hermite<T>(tR, TR, tTR, hR, F[0], F[1], F[2], F[3], &val, DO_G ? &vR : nullptr,
+                  DO_H ? &vRR : nullptr);
+    if (DO_G)
+        cs_hermite<T>(tR, TR, tTR, hR, dF[0], dF[1], dF[2], dF[3], &vz, DO_H ? &vRz : nullptr, nullptr);
+    if (DO_H)
+        cs_hermite<T>(tR, TR, tTR, hR, d2F[0], d2F[1], d2F[2], d2F[3], &vzz, nullptr, nullptr);
 }
 
 // Outer PowerLaw multipole (W_outer, r0) evaluated with the reference's
@@ -153,10 +175,27 @@ __device__ __forceinline__ void cs_load(const DevComp& c, int h, int iR, int iz,
 // which the reference's conversion omits (_cylspl_potential_kernel.cu:836-852);
 // used for derivatives (the VJP), not for forceDeriv, which keeps the
 // reference's values.
-template <int MODE, bool EXACT = false>
+// Mixed precision: the FP32 record (see prep_cylspline.cell_major_f32) holds the
+// corner value f00 in FP64 and the rest relative to it in FP32; the Hermite runs
+// in FP32 and f00 is added back in FP64.
+__device__ __forceinline__ double cs_load32(const DevComp& c, int h, int iR, int iz, float v[16])
+{
+    const float4* p = reinterpret_cast<const float4*>(
+        c.table32 + (((long long)iR * (c.nz - 1) + iz) * c.n_lm + h) * 20);
+    const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2), q3 = __ldg(p + 3),
+                 q4 = __ldg(p + 4);
+    v[0] = 0.0f; v[1] = q0.z; v[2] = q0.w; v[3] = q1.x;
+    v[4] = q1.y; v[5] = q1.z; v[6] = q1.w; v[7] = q2.x;
+    v[8] = q2.y; v[9] = q2.z; v[10] = q2.w; v[11] = q3.x;
+    v[12] = q3.y; v[13] = q3.z; v[14] = q3.w; v[15] = q4.x;
+    return __hiloint2double(__float_as_int(q0.y), __float_as_int(q0.x));
+}
+
+template <int MODE, bool EXACT = false, typename RT = double>
 __device__ __forceinline__ void cylspline_point(const DevComp& c, double px, double py,
                                                 double pz, PointOut& o)
 {
+    constexpr bool F32 = std::is_same<RT, float>::value;   // mixed precision
     constexpr bool DO_G = MODE != AGB_MODE_POT;
     constexpr bool DO_H = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
     const double Rs = c.p[0];
@@ -199,26 +238,25 @@ __device__ __forceinline__ void cylspline_point(const DevComp& c, double px, dou
     double cm = 1.0, sm = 0.0;
     for (int h = 0; h < c.n_lm; ++h) {
         const int m = __ldg(c.lm + h);
-        double v[16];
-        cs_load(c, h, iR, iz, v);
-        const double off = R_at_hi ? (z_at_hi ? v[3] : v[2]) : (z_at_hi ? v[1] : v[0]);
-        v[0] -= off; v[1] -= off; v[2] -= off; v[3] -= off;
-        // in z: the four R-node functions {f(lo), f(hi), fx(lo), fx(hi)} along z
-        double F[4], dF[4], d2F[4];
-        const int lo_i[4] = {0, 2, 4, 6}, hi_i[4] = {1, 3, 5, 7};
-        #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            cs_hermite(tz, Tz, tTz, hz, v[lo_i[q]], v[hi_i[q]], v[8 + lo_i[q]], v[8 + hi_i[q]],
-                       &F[q], DO_G ? &dF[q] : nullptr, DO_H ? &d2F[q] : nullptr);
-        }
         double val, vR = 0.0, vRR = 0.0, vz = 0.0, vRz = 0.0, vzz = 0.0;
-        cs_hermite(tR, TR, tTR, hR, F[0], F[1], F[2], F[3], &val, DO_G ? &vR : nullptr,
-                   DO_H ? &vRR : nullptr);
-        val += off;
-        if (DO_G)
-            cs_hermite(tR, TR, tTR, hR, dF[0], dF[1], dF[2], dF[3], &vz, DO_H ? &vRz : nullptr, nullptr);
-        if (DO_H)
-            cs_hermite(tR, TR, tTR, hR, d2F[0], d2F[1], d2F[2], d2F[3], &vzz, nullptr, nullptr);
+        if (F32 && c.table32) {
+            float w[16];
+            const double f00 = cs_load32(c, h, iR, iz, w);
+            float a, aR = 0.0f, aRR = 0.0f, az = 0.0f, aRz = 0.0f, azz = 0.0f;
+            cs_bicubic<float, DO_G, DO_H>(w, (float)tR, (float)TR, (float)tTR, (float)hR,
+                                          (float)tz, (float)Tz, (float)tTz, (float)hz,
+                                          a, aR, aRR, az, aRz, azz);
+            val = f00 + (double)a;
+            vR = aR; vRR = aRR; vz = az; vRz = aRz; vzz = azz;
+        } else {
+            double v[16];
+            cs_load(c, h, iR, iz, v);
+            const double off = R_at_hi ? (z_at_hi ? v[3] : v[2]) : (z_at_hi ? v[1] : v[0]);
+            v[0] -= off; v[1] -= off; v[2] -= off; v[3] -= off;
+            cs_bicubic<double, DO_G, DO_H>(v, tR, TR, tTR, hR, tz, Tz, tTz, hz, val, vR, vRR, vz,
+                                           vRz, vzz);
+            val += off;
+        }
 
         double T = 1.0, dT = 0.0, d2T = 0.0;
         if (m != 0) {

@@ -58,7 +58,7 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 {
     switch (c.kind) {
     case AGB_KIND_MULTIPOLE:     multipole_point<MODE, R>(c, x, y, z, o); break;
-    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE, EXACT>(c, x, y, z, o); break;
+    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE, EXACT, R>(c, x, y, z, o); break;
     case AGB_KIND_NFW:           nfw_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_PLUMMER:       plummer_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_HERNQUIST:     hernquist_point<MODE>(c.p, x, y, z, o); break;
@@ -247,6 +247,8 @@ static int comp_to_dev(const agb_component& s, DevComp& d, int precision)
             return set_err(AGB_ERR_ARG, "cylspline table must be 16-byte aligned");
         if (s.lmax > AGB_MAX_LMAX || (int)s.p[2] > s.lmax)
             return set_err(AGB_ERR_ARG, "cylspline outer multipole orders out of range");
+        if (precision == AGB_PREC_MIXED && s.table32 && !aligned16(s.table32))
+            return set_err(AGB_ERR_ARG, "cylspline FP32 table must be 16-byte aligned");
     } else if (s.kind < AGB_KIND_NFW || s.kind > AGB_KIND_UNIFORMACC) {
         return set_err(AGB_ERR_ARG, "unknown component kind %d", s.kind);
     }

@@ -646,6 +646,7 @@ class CylSplinePotentialGPU(_Component):
         self.tables = build_cylspline_tables(coefs)
         t = self.tables
         self._cells = t.cell_major()
+        self._cells32 = t.cell_major_f32()
         self._m = t.m_sorted()
 
     @classmethod
@@ -655,6 +656,7 @@ class CylSplinePotentialGPU(_Component):
     def _upload(self, dev):
         t = self.tables
         cells = torch.from_numpy(self._cells).to(dev)
+        cells32 = torch.from_numpy(self._cells32).to(dev)
         m = torch.from_numpy(self._m).to(dev)
         lR = torch.from_numpy(np.ascontiguousarray(t.lR_grid)).to(dev)
         lz = torch.from_numpy(np.ascontiguousarray(t.lz_grid)).to(dev)
@@ -668,6 +670,7 @@ class CylSplinePotentialGPU(_Component):
         c.log_scaling = t.log_scaling
         c.layout = 1
         c.table = cells.data_ptr()
+        c.table32 = cells32.data_ptr()
         c.lm = m.data_ptr()
         c.grid_a = lR.data_ptr()
         c.grid_b = lz.data_ptr()
@@ -675,7 +678,7 @@ class CylSplinePotentialGPU(_Component):
         c.p[0] = t.Rscale
         c.p[1] = t.r0_outer
         c.p[2] = float(t.mmax_outer)
-        return c, (cells, m, lR, lz, W)
+        return c, (cells, cells32, m, lR, lz, W)
 
 
 # ---------------------------------------------------------------------------

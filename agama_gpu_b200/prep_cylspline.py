@@ -66,6 +66,19 @@ class CylSplineTables:
         c = c.transpose(1, 2, 0, 4, 3)                  # (nR-1, nz-1, H, 4q, 4c)
         return np.ascontiguousarray(c.reshape(-1))
 
+    def cell_major_f32(self) -> np.ndarray:
+        """FP32 cell-major records for the mixed-precision kernel, 20 floats (80 bytes)
+        per (cell, harmonic): the (lo,lo) corner value f00 as one FP64 in the first 8
+        bytes, then f - f00 at the (lo,hi), (hi,lo), (hi,hi) corners, f_R, f_z and
+        f_Rz at the four corners (FP32), 3 pads.  Values relative to the corner keep
+        FP32's 24 bits for the variation across the cell, which the derivatives need."""
+        rec64 = self.cell_major().reshape(-1, 16)
+        out = np.zeros((rec64.shape[0], 20), dtype=np.float32)
+        out.view(np.float64)[:, 0] = rec64[:, 0]
+        out[:, 2:5] = (rec64[:, 1:4] - rec64[:, 0:1]).astype(np.float32)
+        out[:, 5:17] = rec64[:, 4:16].astype(np.float32)
+        return np.ascontiguousarray(out.reshape(-1))
+
     def m_sorted(self) -> np.ndarray:
         return np.ascontiguousarray(self.m_arr[self.harmonic_order()].astype(np.int32))
 

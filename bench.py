@@ -274,7 +274,10 @@ def batched_units(dev, n_units: int, steps: int, warmup: int, lf_steps: int, pre
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / k
     t_batch = timed(ev, steps)
+    t_batch64 = timed(lambda: batch._launch(x, 0.0, 1, False, precision="fp64",
+                                            out=(None, F, None, None)), steps)
     t_loop = timed(loop, max(1, steps // 2))
+    ev()
     err = max(float((F[r] - f).abs().max()) / max(float(f.abs().max()), 1e-300)
               for r, f in zip(rows, Fu) if r.stop > r.start)
     del Fu, xu
@@ -296,12 +299,49 @@ def batched_units(dev, n_units: int, steps: int, warmup: int, lf_steps: int, pre
     t_lf = e0.elapsed_time(e1)
     return {"units": n_units, "points": N, "tiles": batch.tiles(precision), "precision": precision,
             "eval_ms": t_batch, "pts_per_s": N / (t_batch * 1e-3),
+            "fp64_eval_ms": t_batch64, "fp64_pts_per_s": N / (t_batch64 * 1e-3),
             "tflops": flops / (t_batch * 1e-3) / 1e12,
             "per_unit_calls_ms": t_loop, "speedup_vs_per_unit_calls": t_loop / t_batch,
             "max_rel_diff_vs_per_unit_calls": err,
             "leapfrog_graph_steps": lf_steps, "leapfrog_ms": t_lf,
             "leapfrog_particle_steps_per_s": N * lf_steps / (t_lf * 1e-3),
             "finite": bool(torch.isfinite(xT).all())}
+
+
+def cylspline_leg(dev, n: int, steps: int, warmup: int):
+    """CylSpline bar (mmax 6: m=0 Miyamoto-Nagai + m=2,4,6 with seeded phases, 32x32
+    sinh grid), 1M exponential-disk points (Rd 3, hz 0.3): Phi+F in FP64 and mixed."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    from agama_gpu_b200.synthetic import bar_cylspline, disk_points
+    cs = agb.CylSplinePotentialGPU(bar_cylspline())
+    x = torch.from_numpy(disk_points(n, 3.0, 0.3, 21)).to(dev)
+    phi = torch.empty(n, dtype=torch.float64, device=dev)
+    F = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        run = lambda: cs._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec,  # noqa: E731
+                                 out=(phi, F, None, None))
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        res[prec] = {"ms": e0.elapsed_time(e1) / steps, "F": F.clone()}
+    # inside the grid (R >= 0.1 kpc); the outer asymptote below it is FP64 in both modes
+    inside = torch.hypot(x[:, 0], x[:, 1]) >= 0.1
+    fm, fd = res["mixed"]["F"][inside], res["fp64"]["F"][inside]
+    err = float((fm - fd).abs().max() / fd.abs().max())
+    return {"points": n, "harmonics": int(cs.tables.n_harm),
+            "points_below_grid_R0.1": int((~inside).sum()),
+            "fp64_ms": res["fp64"]["ms"], "fp64_pts_per_s": n / (res["fp64"]["ms"] * 1e-3),
+            "mixed_ms": res["mixed"]["ms"], "mixed_pts_per_s": n / (res["mixed"]["ms"] * 1e-3),
+            "mixed_force_max_rel_in_grid": err}
 
 
 def cpu_baseline_leg(pot, xyz: np.ndarray, t: float, n_sample: int):
@@ -432,6 +472,16 @@ def main():
     device_step(t_chk, "mixed")
     err_f = float((frc - f64).abs().max() / f64.abs().max())
     err_p = float((phi - p64).abs().max() / p64.abs().max())
+    del f64, p64
+    # second derivatives on the first 1M points: forceDeriv and density, same convention
+    sub = xyz[: min(N, 1_000_000)]
+    _, _, h64, _ = pot._launch(sub, t_chk, _lib.MODE_HESS, False, precision="fp64")
+    _, _, h32, _ = pot._launch(sub, t_chk, _lib.MODE_HESS, False, precision="mixed")
+    err_h = float((h32 - h64).abs().max() / h64.abs().max())
+    _, _, _, r64 = pot._launch(sub, t_chk, _lib.MODE_DENS, False, precision="fp64")
+    _, _, _, r32 = pot._launch(sub, t_chk, _lib.MODE_DENS, False, precision="mixed")
+    err_r = float((r32 - r64).abs().max() / r64.abs().max())
+    del h64, h32, r64, r32
 
     # end to end through the public API from pinned host memory
     pot.set_precision("mixed")
@@ -466,6 +516,7 @@ def main():
                                                     "adjoint_phase_space_only_ms",
                                                     "ratio_phase_space_only")}
 
+    cyl = cylspline_leg(dev, 1_000_000, max(3, args.steps), 3)
     batched = None
     if args.batch_units > 0:
         torch.cuda.empty_cache()
@@ -497,10 +548,12 @@ def main():
         "step_breakdown_ms": {"eval_kernel_mixed": k32, "eval_kernel_fp64": k64,
                               "interval_sort_mixed": ms32 - k32,
                               "mixed_unsorted_points_no_sort": u32},
-        "mixed_vs_fp64_error": {"force_max_rel": err_f, "phi_max_rel": err_p, "gate": 1e-6},
+        "mixed_vs_fp64_error": {"force_max_rel": err_f, "phi_max_rel": err_p, "gate": 1e-6,
+                                "forceDeriv_max_rel_1M": err_h, "density_max_rel_1M": err_r},
         "adjoint_over_forward": None if adj is None else adj["ratio"],
         "adjoint": adj,
         "batched": batched,
+        "cylspline": cyl,
         "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
                 "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,
                 "ms_per_step": e2e_ms, "finite": e2e_ok,

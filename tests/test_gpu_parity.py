@@ -303,3 +303,28 @@ def test_eval_host_pipeline_matches_eval(pinned):
     # ill-conditioned outer extrapolation differently, so compare with GRAD on the device
     f_dev = pot.force(xyz.cuda()).cpu()
     assert float((out - f_dev).abs().max()) <= 1e-14 * float(f_dev.abs().max())
+
+
+def test_cylspline_mixed_precision():
+    """CylSpline bar (mmax 6, 32x32 sinh grid), exponential-disk points: the FP32
+    Hermite path against FP64 -- force within the 1e-6 gate, the rest stated."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import disk_points
+    cs = agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))
+    x = torch.from_numpy(disk_points(300_000, 3.0, 0.3, 8)).cuda()
+    cs.set_precision("fp64")
+    p64, f64, d64 = cs.evalDeriv(x)
+    cs.set_precision("mixed")
+    p32, f32, d32 = cs.evalDeriv(x)
+    cs.set_precision(None)
+    # the grid starts at R = 0.1: points inside it go through the FP32 Hermite; the few
+    # below it take the (FP64 in both modes) outer asymptote, whose (r0/r)^(l+1) terms
+    # reach 1e36 there and would swamp a max-normalised error
+    xn = _np(x)
+    inside = np.hypot(xn[:, 0], xn[:, 1]) >= 0.1
+    assert inside.sum() > 0.99 * len(xn) and (~inside).sum() > 0
+    assert rel_max(_np(f32)[inside], _np(f64)[inside]) <= TOL_MIXED_F
+    assert rel_max(_np(p32)[inside], _np(p64)[inside]) <= 1e-7
+    assert rel_max(_np(d32)[inside], _np(d64)[inside]) <= 1e-5
+    assert np.array_equal(_np(f32)[~inside], _np(f64)[~inside])
