@@ -118,6 +118,10 @@ def _load():
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_cylspline_table_vjp.restype = ctypes.c_int
+    lib.agb_cylspline_table_vjp.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     lib.agb_batch_create.restype = ctypes.c_int
     lib.agb_batch_create.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf),
@@ -143,7 +147,7 @@ EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
-    "agb_multipole_adjoint",
+    "agb_multipole_adjoint", "agb_cylspline_table_vjp",
     "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",

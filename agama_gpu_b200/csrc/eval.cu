@@ -19,6 +19,7 @@
 #include "analytic.cuh"
 #include "bin.cuh"
 #include "mp_grad.cuh"
+#include "cs_grad.cuh"
 
 // ---------------------------------------------------------------------------
 // errors and launch accounting
@@ -609,6 +610,28 @@ extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* 
     }
     if (need && own) cudaFreeAsync(ws, st);
     return rc;
+}
+
+extern "C" int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf* leaf,
+                                      const double* xyz, int64_t n, const double* g_phi,
+                                      const double* g_force, double* g_cells, void* stream)
+{
+    if (!comp || !leaf || !g_cells)
+        return set_err(AGB_ERR_ARG, "agb_cylspline_table_vjp: null argument");
+    if (comp->kind != AGB_KIND_CYLSPLINE || comp->layout != 1)
+        return set_err(AGB_ERR_ARG, "agb_cylspline_table_vjp: needs a cell-major CylSpline table");
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_cylspline_table_vjp: negative point count");
+    if (n == 0) return AGB_OK;
+    if (!xyz) return set_err(AGB_ERR_ARG, "agb_cylspline_table_vjp: xyz is null");
+    CSGradArgs g;
+    memset(&g, 0, sizeof(g));
+    int rc = comp_to_dev(*comp, g.c, AGB_PREC_FP64);
+    if (rc) return rc;
+    g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
+    g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
+    g.n = n; g.xyz = xyz; g.gphi = g_phi; g.gforce = g_force; g.grad = g_cells;
+    cs_grad_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(g);
+    return check_launch("cs_grad_kernel");
 }
 
 // ---------------------------------------------------------------------------

@@ -95,3 +95,62 @@ def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int) -> Tuple[torch.T
     out_p[:, cols] = gphi
     out_d[:, cols] = gdphi
     return out_p, out_d
+
+
+def _spline_deriv_matrix(x: np.ndarray, bc_type) -> np.ndarray:
+    """D with D @ y = derivative at the nodes of the cubic spline through (x, y)."""
+    from scipy.interpolate import CubicSpline
+    n = len(x)
+    return CubicSpline(x, np.eye(n), axis=0, bc_type=bc_type)(x, 1)
+
+
+def cylspline_node_vjp(tables, coefs, grad_nodes: torch.Tensor) -> dict:
+    """{m: dL/dPhi_m (nR, nz of the coefficient grid)} from dL/d(node table).
+
+    The node table of the builder (prep_cylspline.build_cylspline_tables) is, per
+    harmonic, f and its spline derivatives f_lR = D_R f, f_lz = f D_z^T,
+    f_lR_lz = D_R f D_z^T -- linear maps (natural spline in lz; zero slope at R = 0
+    and natural at the outer end in lR) -- of f = log(-Phi_0) (m = 0) or
+    Phi_m / Phi_0 under log-scaling, Phi_m otherwise, on the z grid mirrored from
+    z >= 0 when the file stores half of it.  The transpose of each step is applied
+    in turn.  The outer asymptote, Rscale and the asinh grids are held fixed."""
+    G = grad_nodes.detach().to("cpu", torch.float64).numpy()
+    lR, lz = tables.lR_grid, tables.lz_grid
+    nR = len(lR)
+    DR = _spline_deriv_matrix(lR, ((1, np.zeros(nR)), "natural"))
+    Dz = _spline_deriv_matrix(lz, "natural")
+    z0 = np.asarray(coefs.z_grid, dtype=np.float64)
+    half = z0[0] == 0
+    nz0 = len(z0)
+    phi = {}
+    for m, t in coefs.phi.items():
+        t = np.asarray(t, dtype=np.float64)
+        if half:
+            full = np.empty((t.shape[0], 2 * nz0 - 1))
+            full[:, nz0 - 1:] = t
+            full[:, :nz0] = t[:, ::-1]
+            phi[int(m)] = full
+        else:
+            phi[int(m)] = t
+    df = {}
+    for h, m in enumerate(tables.m_arr):
+        Gf, Gx, Gy, Gxy = (G[h, :, :, q] for q in range(4))
+        df[int(m)] = Gf + DR.T @ Gx + Gy @ Dz + DR.T @ Gxy @ Dz
+    if tables.log_scaling:
+        p0 = phi[0]
+        dphi = {0: df[0] / p0}
+        for m, d in df.items():
+            if m == 0:
+                continue
+            dphi[m] = d / p0
+            dphi[0] = dphi[0] - d * phi[m] / (p0 * p0)
+    else:
+        dphi = dict(df)
+    if half:
+        out = {}
+        for m, d in dphi.items():
+            g = d[:, nz0 - 1:].copy()
+            g[:, 1:] += d[:, :nz0 - 1][:, ::-1]
+            out[m] = g
+        return out
+    return dphi

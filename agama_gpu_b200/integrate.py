@@ -207,9 +207,10 @@ class Leapfrog:
                 lam_v: torch.Tensor, table_grads: bool = False, group=None):
         """(dL/dx0, dL/dv0) from (dL/dx_T, dL/dv_T) and the forward's checkpoints.
 
-        With table_grads=True also returns {Multipole component: dL/dpoly}, the
-        gradient with respect to each Multipole's quintic coefficients summed over
-        all force evaluations (component.node_gradients() carries it to the nodes).
+        With table_grads=True also returns {component: gradient}: for each Multipole
+        dL/dpoly (its quintic coefficients), for each CylSpline dL/d(node table),
+        summed over all force evaluations (component.node_gradients() carries either
+        to the coefficient-file nodes).
         Under torch.distributed (each rank integrating its own particles in the same
         potential) the table gradients are summed over the ranks of ``group``.
         """

@@ -252,7 +252,7 @@ class _GPUPotBase:
         if rest:
             self._vjp(arr, t, g_phi, g_force, precision=precision, out=gx, leaves=rest)
             for comp, sigma, gamma, ampl in rest:
-                if comp.kind == _lib.KIND_MULTIPOLE:
+                if comp.kind in (_lib.KIND_MULTIPOLE, _lib.KIND_CYLSPLINE):
                     g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
                     key = ("poly", comp)
                     if key in acc_dev:
@@ -303,11 +303,12 @@ class _GPUPotBase:
 
     def _table_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
                    g_force: Optional[torch.Tensor], acc: Optional[dict] = None) -> dict:
-        """dL/dpoly of every Multipole in the tree: {component: (n_lm, n_int, 6)}, summed
-        over the leaves that use it and added into ``acc`` when given."""
+        """Table gradients of every Multipole and CylSpline in the tree: {component:
+        dL/dpoly (n_lm, n_int, 6) | dL/d(node table) (n_harm, nR, nz, 4)}, summed over
+        the leaves that use it and added into ``acc`` when given."""
         acc = {} if acc is None else acc
         for comp, sigma, gamma, ampl in self._leaves(float(t)):
-            if comp.kind != _lib.KIND_MULTIPOLE:
+            if comp.kind not in (_lib.KIND_MULTIPOLE, _lib.KIND_CYLSPLINE):
                 continue
             g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
             if comp in acc:
@@ -643,11 +644,72 @@ class CylSplinePotentialGPU(_Component):
     kind = _lib.KIND_CYLSPLINE
 
     def __init__(self, coefs) -> None:
-        self.tables = build_cylspline_tables(coefs)
-        t = self.tables
+        self._sync_order = next(_MULTIPOLE_SERIAL)
+        self._coefs = coefs
+        self._set_tables(build_cylspline_tables(coefs))
+
+    def _set_tables(self, t) -> None:
+        self.tables = t
         self._cells = t.cell_major()
         self._cells32 = t.cell_major_f32()
         self._m = t.m_sorted()
+        self.__dict__.pop("_dev_cache", None)
+
+    @classmethod
+    def _from_tables(cls, tables, coefs=None) -> "CylSplinePotentialGPU":
+        """A CylSpline from prepared tables (e.g. a perturbed node table)."""
+        obj = cls.__new__(cls)
+        obj._sync_order = next(_MULTIPOLE_SERIAL)
+        obj._coefs = coefs
+        obj._set_tables(tables)
+        return obj
+
+    def table_vjp(self, xyz: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
+                  g_force: Optional[torch.Tensor], leaf=None) -> torch.Tensor:
+        """dL/d(node table) (n_harm, nR, nz, 4) in the layout of ``tables.node_arr``
+        ({f, f_lR, f_lz, f_lR_lz} at every node, harmonics in m_arr order), for
+        cotangents of the potential and force of the tree this component belongs to;
+        ``leaf`` = (sigma, gamma, ampl) of the component in that tree.  FP64.  Points
+        outside the grid contribute nothing (the outer asymptote is held fixed)."""
+        dev = xyz.device
+        comp = self._device_component(dev)
+        lf = _lib.AgbLeaf()
+        sigma, gamma, ampl = leaf if leaf is not None else (1.0, np.zeros(3), 1.0)
+        lf.comp = 0
+        lf.sigma = float(sigma)
+        lf.gamma[0], lf.gamma[1], lf.gamma[2] = (float(g) for g in gamma)
+        lf.ampl = float(ampl)
+        tb = self.tables
+        nR, nz, H = len(tb.lR_grid), len(tb.lz_grid), tb.n_harm
+        gc = torch.zeros((nR - 1, nz - 1, H, 4, 4), dtype=torch.float64, device=dev)
+        n = xyz.shape[0]
+        if n:
+            arr = xyz.to(dtype=torch.float64).contiguous()
+            gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
+            gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
+            ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+            rc = _lib.lib.agb_cylspline_table_vjp(
+                ctypes.byref(comp), ctypes.byref(lf), arr.data_ptr(), n, ptr(gp), ptr(gf),
+                gc.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+            _lib.check(rc, "agb_cylspline_table_vjp")
+        # fold the cell records onto the nodes: record [quantity][corner], corners
+        # (lo,lo), (lo,hi), (hi,lo), (hi,hi) in (R, z)
+        g_sorted = torch.zeros((H, nR, nz, 4), dtype=torch.float64, device=dev)
+        for corner, (dR, dz) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+            g_sorted[:, dR:dR + nR - 1, dz:dz + nz - 1, :] += gc[:, :, :, :, corner].permute(2, 0, 1, 3)
+        order = torch.from_numpy(tb.harmonic_order()).to(dev)
+        g = torch.zeros_like(g_sorted)
+        g[order] = g_sorted
+        return g
+
+    def node_gradients(self, grad_nodes: torch.Tensor):
+        """{m: dL/dPhi_m} on the input coefficient grid from dL/d(node table), through
+        the node-derivative splines, the log-scaling and the z mirroring of the table
+        builder (the outer asymptote, Rscale and the grids are held fixed)."""
+        from .diff_tables import cylspline_node_vjp
+        if self._coefs is None:
+            raise ValueError("node_gradients() needs the coefficients the object was built from")
+        return cylspline_node_vjp(self.tables, self._coefs, grad_nodes)
 
     @classmethod
     def from_file(cls, path, **kw) -> "CylSplinePotentialGPU":

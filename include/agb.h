@@ -252,6 +252,20 @@ int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
                           void* stream);
 
 /*
+ * Gradient of a loss with respect to one CylSpline leaf's node table: adds into
+ * g_cells, laid out like the component's cell-major FP64 table
+ * [(nR-1)(nz-1)][n_harm][16] (each cell record holds its four corners' f, f_R,
+ * f_z, f_Rz, so a node's gradient is the sum over the up to four records that
+ * hold it), the sum over points of dL/dv for cotangents g_phi [N] and g_force
+ * [N,3] of the composite's outputs; leaf gives the component's transform.
+ * Points outside the grid contribute nothing (the outer asymptote and Rscale
+ * are held fixed).  FP64, no scratch.  No counterpart in the reference.
+ */
+int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf* leaf,
+                            const double* xyz, int64_t n, const double* g_phi,
+                            const double* g_force, double* g_cells, void* stream);
+
+/*
  * agb_eval_static -- agb_eval that allocates nothing.  No counterpart in the
  * reference: it exists for callers that may not allocate device memory (a
  * code that reserved the GPU for its own pools, a loop that must not pay

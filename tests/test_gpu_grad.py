@@ -354,3 +354,101 @@ def test_fused_adjoint_matches_separate_passes(prec, tol_x, tol_g, lmax):
     eg = ((tg - 2 * ref_g).abs().max() / ref_g.abs().max()).item()
     assert ex <= tol_x, ex
     assert eg <= tol_g, eg
+
+
+def _cyl_local_points(n, seed):
+    rng = np.random.default_rng(seed)
+    R = np.exp(rng.uniform(np.log(0.3), np.log(120.0), n))
+    ph = rng.uniform(0, 2 * np.pi, n)
+    z = np.sinh(rng.uniform(-3.0, 3.0, n)) * 3.0
+    return np.stack([R * np.cos(ph), R * np.sin(ph), z], 1)
+
+
+@pytest.mark.parametrize("log_scaled", [True, False])
+def test_cylspline_table_vjp_matches_finite_differences(log_scaled):
+    """dL/d(node table) of a CylSpline seen through Shifted/Scaled, and its chain to
+    the coefficient grid, against central differences of the GPU evaluation."""
+    import copy
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.coefs import CylSplineCoefs
+    coefs = cs_coefs(golden("cs_cfg1"))
+    if not log_scaled:                 # a positive m=0 offset switches log-scaling off
+        coefs = CylSplineCoefs(coefs.R_grid, coefs.z_grid,
+                               {m: (np.asarray(v) + (3e4 if m == 0 else 0.0)) for m, v in coefs.phi.items()})
+    cs = agb.CylSplinePotentialGPU(coefs)
+    assert bool(cs.tables.log_scaling) == log_scaled
+    shift, scale, ampl = np.array([0.4, -0.3, 0.2]), 1.3, 0.8
+
+    def tree(c):
+        return agb.ScaledPotentialGPU(agb.ShiftedPotentialGPU(c, list(shift)), scale, ampl)
+    _, sigma, gamma, A = tree(cs)._leaves(0.0)[0]
+    xl = _cyl_local_points(3000, 41)
+    x = torch.from_numpy((xl + np.asarray(gamma)) / sigma).cuda()
+    rng = np.random.default_rng(42)
+    gphi = torch.from_numpy(rng.normal(size=len(xl))).cuda()
+    gf = torch.from_numpy(rng.normal(size=(len(xl), 3))).cuda()
+
+    def L(c):
+        p, f, _, _ = tree(c)._launch(x, 0.0, 1, True, precision="fp64")
+        return float((p * gphi).sum() + (f * gf).sum())
+
+    g = cs.table_vjp(x, 0.0, gphi, gf, leaf=(sigma, gamma, A)).cpu().numpy()
+    tb = cs.tables
+    nodes = tb.node_arr
+    H = tb.n_harm
+    for (h, i, j, q) in [(tb.m_arr.tolist().index(0), 12, 15, 0), (tb.m_arr.tolist().index(0), 8, 17, 1),
+                         (tb.m_arr.tolist().index(2), 10, 14, 2), (tb.m_arr.tolist().index(-4), 14, 16, 3),
+                         (H - 1, 6, 18, 0)]:
+        # step on the harmonic's value scale: some derivative nodes are ~1e-17 here
+        step = 1e-6 * max(np.abs(nodes[h, :, :, q]).max(), np.abs(nodes[h, :, :, 0]).max())
+        tp, tm = copy.deepcopy(tb), copy.deepcopy(tb)
+        tp.node_arr = nodes.copy(); tp.node_arr[h, i, j, q] += step
+        tm.node_arr = nodes.copy(); tm.node_arr[h, i, j, q] -= step
+        fd = (L(agb.CylSplinePotentialGPU._from_tables(tp)) -
+              L(agb.CylSplinePotentialGPU._from_tables(tm))) / (2 * step)
+        # central differences resolve ~1e-8 of the largest gradient entry here
+        assert abs(g[h, i, j, q] - fd) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(g).max()), (h, i, j, q, g[h, i, j, q], fd)
+    # chained to the coefficient grid (interior nodes: the asymptote fit and Rscale stay put)
+    gc = cs.node_gradients(torch.from_numpy(g))
+    for m, i, j in [(0, 12, 15), (2, 10, 14), (-6, 14, 17)]:
+        step = 1e-6 * np.abs(np.asarray(coefs.phi[m])).max()
+        pp = {k: np.array(v, dtype=float) for k, v in coefs.phi.items()}
+        pm = {k: np.array(v, dtype=float) for k, v in coefs.phi.items()}
+        pp[m][i, j] += step
+        pm[m][i, j] -= step
+        fd = (L(agb.CylSplinePotentialGPU(CylSplineCoefs(coefs.R_grid, coefs.z_grid, pp))) -
+              L(agb.CylSplinePotentialGPU(CylSplineCoefs(coefs.R_grid, coefs.z_grid, pm)))) / (2 * step)
+        assert abs(gc[m][i, j] - fd) <= 1e-5 * max(abs(fd), 1e-4 * max(np.abs(v).max() for v in gc.values())), \
+            (m, i, j, gc[m][i, j], fd)
+
+
+def test_leapfrog_cylspline_table_gradients():
+    import copy
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    cs = agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))
+    nfw = agb.NFWPotentialGPU(mass=5e11, scaleRadius=15.0)
+    x0, v0 = _disk_ics(40, 13)
+    target = x0 * 1.05
+
+    def run(c, want=False):
+        integ = Leapfrog(c + nfw, 0.002, precision="fp64")
+        xT, vT, ck = integ.run(x0, v0, 30, checkpoint_every=8)
+        if not want:
+            return float(((xT - target) ** 2).sum())
+        _, _, tg = integ.adjoint(ck, 30, 2 * (xT - target), torch.zeros_like(vT), table_grads=True)
+        return tg[c]
+
+    g = run(cs, True).cpu().numpy()
+    tb = cs.tables
+    h0 = tb.m_arr.tolist().index(0)
+    for (h, i, j, q) in [(h0, 14, 15, 0), (h0, 16, 16, 1), (tb.m_arr.tolist().index(2), 15, 16, 0)]:
+        step = 1e-6 * max(np.abs(tb.node_arr[h, :, :, q]).max(), np.abs(tb.node_arr[h, :, :, 0]).max())
+        tp, tm = copy.deepcopy(tb), copy.deepcopy(tb)
+        tp.node_arr = tb.node_arr.copy(); tp.node_arr[h, i, j, q] += step
+        tm.node_arr = tb.node_arr.copy(); tm.node_arr[h, i, j, q] -= step
+        fd = (run(agb.CylSplinePotentialGPU._from_tables(tp)) -
+              run(agb.CylSplinePotentialGPU._from_tables(tm))) / (2 * step)
+        assert abs(g[h, i, j, q] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(g).max()), (h, i, j, q, g[h, i, j, q], fd)
