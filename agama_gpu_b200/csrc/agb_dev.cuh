@@ -55,6 +55,8 @@ struct EvalArgs {
     double* grad;
     double* hess;
     double* rho;
+    double* stage;           // binned calls: outputs in sorted order, [pos][rec] (or null)
+    const int* dest;         // binned calls: sorted position of input point i
     const double* gphi;      // VJP mode: dL/dPhi [N] (may be null)
     const double* gforce;    // VJP mode: dL/dF [N,3] (may be null)
     DevComp comps[AGB_MAX_COMPONENTS];

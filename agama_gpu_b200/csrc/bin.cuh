@@ -13,7 +13,8 @@
 //   2. bin_scan:    one block, exclusive scan of the bin counts -> offsets
 //   3. bin_scatter: the same tiles as pass 1; each block reserves its range
 //                   in every bin with one global atomic, then places its
-//                   points: perm[pos] = i and a sorted AoS copy of xyz
+//                   points: perm[pos] = i, keys[i] = pos (overwriting the
+//                   key) and a sorted AoS copy of xyz
 // Within a bin the order is not deterministic; each point's result does not
 // depend on it.
 #pragma once
@@ -26,6 +27,12 @@ struct BinKey {
     double sigma, g0, g1, g2;     // frame of the keyed Multipole leaf
     double logr_min, inv_dlogr;
     int n_int;
+    // Output blocks: the key of point i is (i >> log_block) * (n_int + 2) + its
+    // interval, so the sorted order runs through the points block by block.  A
+    // kernel that walks the sorted order then writes its (permuted) outputs into
+    // one block-sized window at a time, which L2 holds and merges, instead of
+    // scattering partial-sector writes over the whole output array.
+    int log_block;
 };
 
 // in-grid interval k in [0, n_int), n_int for the inner region (and the
@@ -51,7 +58,8 @@ bin_count(const double* __restrict__ xyz, long long n, BinKey b, int n_bins,
     const long long lo = (long long)blockIdx.x * AGB_BIN_TILE;
     const long long hi = min(lo + (long long)AGB_BIN_TILE, n);
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        const int k = bin_of(b, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        const int k = bin_of(b, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]) +
+                      (int)(i >> b.log_block) * (b.n_int + 2);
         keys[i] = k;
         atomicAdd(&hist[k], 1);
     }
@@ -86,7 +94,7 @@ bin_scan(const int* __restrict__ counts, int* __restrict__ cursor, int n_bins)
 
 __global__ void __launch_bounds__(256)
 bin_scatter(const double* __restrict__ xyz, long long n, int n_bins,
-            const int* __restrict__ keys, int* __restrict__ cursor,
+            int* __restrict__ keys, int* __restrict__ cursor,
             int* __restrict__ perm, double* __restrict__ xyz_sorted)
 {
     extern __shared__ int sm[];
@@ -108,6 +116,7 @@ bin_scatter(const double* __restrict__ xyz, long long n, int n_bins,
         const int k = keys[i];
         const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
         perm[pos] = (int)i;
+        keys[i] = (int)pos;          // from here on: where point i went (the inverse of perm)
         xyz_sorted[3 * pos] = xyz[3 * i];
         xyz_sorted[3 * pos + 1] = xyz[3 * i + 1];
         xyz_sorted[3 * pos + 2] = xyz[3 * i + 2];

@@ -73,6 +73,43 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
     }
 }
 
+// Binned calls evaluate the points in interval order.  Writing each point's
+// outputs straight to its input position scatters 8-byte stores over the whole
+// output (uncoalesced: one sector per lane per store); with room in the
+// workspace the kernel instead writes records in sorted order ("stage") and
+// unpermute_kernel gathers them back, reading one record per point and writing
+// every output array contiguously.
+__host__ __device__ constexpr int stage_rec(int mode)
+{
+    return mode == AGB_MODE_HESS ? 10 : mode == AGB_MODE_GRAD ? 4 : mode == AGB_MODE_VJP ? 3 : 1;
+}
+#define AGB_STAGE_MAX_REC 10
+
+template <int MODE>
+__global__ void __launch_bounds__(256)
+unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage, long long n,
+                 double* phi, double* grad, double* hess, double* rho)
+{
+    constexpr int REC = stage_rec(MODE);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double* t = stage + (long long)REC * __ldg(dest + i);
+        if (MODE == AGB_MODE_DENS) { rho[i] = t[0]; continue; }
+        if (MODE == AGB_MODE_VJP) {
+            grad[3 * i] = t[0]; grad[3 * i + 1] = t[1]; grad[3 * i + 2] = t[2];
+            continue;
+        }
+        if (phi) phi[i] = t[0];
+        if (MODE != AGB_MODE_POT && grad) {
+            grad[3 * i] = t[1]; grad[3 * i + 1] = t[2]; grad[3 * i + 2] = t[3];
+        }
+        if (MODE == AGB_MODE_HESS) {
+            #pragma unroll
+            for (int q = 0; q < 6; ++q) hess[6 * i + q] = t[4 + q];
+        }
+    }
+}
+
 // Hessian-carrying modes hold about twice the live state: one block per SM
 // with up to 255 registers beats two blocks with heavy spilling.
 template <int MODE, typename R>
@@ -128,14 +165,29 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             const double gp = a.gphi ? a.gphi[i] : 0.0;
             double f0 = 0.0, f1 = 0.0, f2 = 0.0;
             if (a.gforce) { f0 = a.gforce[3 * i]; f1 = a.gforce[3 * i + 1]; f2 = a.gforce[3 * i + 2]; }
-            a.grad[3 * i]     = gp * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
-            a.grad[3 * i + 1] = gp * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
-            a.grad[3 * i + 2] = gp * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
+            const double v0 = gp * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
+            const double v1 = gp * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
+            const double v2 = gp * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
+            double* o = a.stage ? a.stage + 3 * pos : a.grad + 3 * i;
+            o[0] = v0; o[1] = v1; o[2] = v2;
             continue;
         }
         const double sg = (a.out_flags & AGB_OUT_NEGATE) ? -1.0 : 1.0;
         if (MODE == AGB_MODE_DENS) {
-            a.rho[i] = rho;
+            if (a.stage) a.stage[pos] = rho;
+            else a.rho[i] = rho;
+            continue;
+        }
+        if (a.stage) {
+            // sorted order: consecutive threads write consecutive records
+            constexpr int REC = stage_rec(MODE);
+            double* o = a.stage + REC * pos;
+            o[0] = phi;
+            if (MODE != AGB_MODE_POT) { o[1] = sg * g0; o[2] = sg * g1; o[3] = sg * g2; }
+            if (MODE == AGB_MODE_HESS) {
+                #pragma unroll
+                for (int q = 0; q < 6; ++q) o[4 + q] = sg * h[q];
+            }
             continue;
         }
         if (a.phi) a.phi[i] = phi;
@@ -191,7 +243,30 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
     agb_eval_kernel<MODE, R><<<(int)grid, 256, 0, st>>>(a);
 }
 
+static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t st);
+
+template <int MODE>
+static void launch_unpermute(const EvalArgs& a, cudaStream_t st)
+{
+    unpermute_kernel<MODE><<<grid_for(a.n), 256, 0, st>>>(a.dest, a.stage, a.n, a.phi, a.grad,
+                                                          a.hess, a.rho);
+}
+
 static int launch_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
+{
+    int rc = launch_eval_mode(mode, precision, a, st);
+    if (rc || !a.stage) return rc;
+    switch (mode) {
+    case AGB_MODE_POT:  launch_unpermute<AGB_MODE_POT>(a, st); break;
+    case AGB_MODE_GRAD: launch_unpermute<AGB_MODE_GRAD>(a, st); break;
+    case AGB_MODE_HESS: launch_unpermute<AGB_MODE_HESS>(a, st); break;
+    case AGB_MODE_DENS: launch_unpermute<AGB_MODE_DENS>(a, st); break;
+    default:            launch_unpermute<AGB_MODE_VJP>(a, st); break;
+    }
+    return check_launch("unpermute_kernel");
+}
+
+static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
 {
     const bool mixed = precision == AGB_PREC_MIXED;
     switch (mode) {
@@ -286,7 +361,13 @@ static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, 
     b.key.logr_min = c.p[0];
     b.key.inv_dlogr = c.p[2];
     b.key.n_int = c.n_int;
-    b.n_bins = c.n_int + 2;
+    // output blocks of 2^19 points (40 MB of Hessian output at most), more
+    // points per block when the block count would exceed the bin limit
+    const int nb = c.n_int + 2;
+    int lb = 19;
+    while ((long long)((n + (1LL << lb) - 1) >> lb) * nb > AGB_MAX_BINS) ++lb;
+    b.key.log_block = lb;
+    b.n_bins = (int)((n + (1LL << lb) - 1) >> lb) * nb;
     return b;
 }
 
@@ -296,6 +377,13 @@ static size_t ws_bytes(const BinPlan& b, int64_t n)
 {
     if (!b.on) return 0;
     return al256(4 * (size_t)n) * 2 + al256(24 * (size_t)n) + al256(4 * (size_t)b.n_bins) * 2;
+}
+
+// with room for the sorted-order output records (stage_rec doubles per point)
+static size_t ws_bytes_staged(const BinPlan& b, int64_t n)
+{
+    if (!b.on) return 0;
+    return ws_bytes(b, n) + al256(8 * (size_t)AGB_STAGE_MAX_REC * (size_t)n);
 }
 
 static int validate(const agb_component* comps, int n_comps, const agb_leaf* leaves, int n_leaves,
@@ -406,7 +494,11 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
     if ((rc = pack_args(a, comps, n_comps, leaves, n_leaves, precision))) return rc;
 
     const BinPlan b = plan_binning(comps, leaves, n_leaves, n, out_flags);
-    const size_t need = ws_bytes(b, n);
+    // sorted-order output staging when the workspace has room for it (always for
+    // agb_eval's own allocation and for workspaces sized by agb_eval_workspace_bytes)
+    const size_t staged = ws_bytes_staged(b, n);
+    const bool stage = b.on && (own_ws || (workspace && workspace_bytes >= staged));
+    const size_t need = stage ? staged : ws_bytes(b, n);
     void* ws = workspace;
     if (need) {
         if (own_ws) {
@@ -421,6 +513,10 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
             return set_err(AGB_ERR_ARG, "agb_eval_ws: workspace must be 256-byte aligned");
         }
         rc = run_binning(a, b, xyz, n, (char*)ws, st);
+        if (stage) {
+            a.stage = (double*)((char*)ws + ws_bytes(b, n));
+            a.dest = (const int*)ws;             // bin_scatter leaves pos of point i in keys[i]
+        }
     }
     if (!rc) rc = launch_mode(mode, precision, a, st);
     if (need && own_ws) cudaFreeAsync(ws, st);
@@ -434,7 +530,7 @@ extern "C" size_t agb_eval_workspace_bytes(const agb_component* comps, int n_com
     if (!comps || !leaves || n_leaves < 1 || n_comps < 1) return 0;
     for (int L = 0; L < n_leaves; ++L)
         if (leaves[L].comp < 0 || leaves[L].comp >= n_comps) return 0;
-    return ws_bytes(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
+    return ws_bytes_staged(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
 }
 
 extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf* leaves,
@@ -677,7 +773,15 @@ extern "C" int agb_eval_static(const agb_component* comps, int n_comps, const ag
                            cudaGetErrorString(e));
         g_static_scratch_addr[dev] = p;
     }
-    const size_t need = agb_eval_workspace_bytes(comps, n_comps, leaves, n_leaves, n, out_flags);
+    // the sort scratch this call cannot do without (output staging is used only
+    // when it fits as well)
+    size_t need = 0;
+    if (comps && leaves && n_comps >= 1 && n_leaves >= 1) {
+        bool ok = true;
+        for (int L = 0; L < n_leaves; ++L)
+            ok = ok && leaves[L].comp >= 0 && leaves[L].comp < n_comps;
+        if (ok) need = ws_bytes(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
+    }
     if (need > (size_t)AGB_STATIC_SCRATCH_BYTES)
         return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_static: needs %zu bytes of scratch, more "
                        "than its fixed %d", need, AGB_STATIC_SCRATCH_BYTES);
