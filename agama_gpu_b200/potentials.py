@@ -368,7 +368,7 @@ class _GPUPotBase:
                   t: float = 0.0, chunk_points: Optional[int] = None, out=None, device=None):
         """``eval`` for positions and results in HOST memory, pipelined.
 
-        The points go through the GPU in chunks of ``chunk_points`` (default: N/6,
+        The points go through the GPU in chunks of ``chunk_points`` (default: N/4,
         clamped to [2^17, 2^20] points, so a chunk still fills the GPU): while chunk i
         is evaluated, chunk i+1 is copied in and chunk i-1's results are copied
         out (three CUDA streams, two device buffers per stream stage), so the
@@ -406,17 +406,20 @@ class _GPUPotBase:
                           or h.device.type != "cpu" or not h.is_contiguous()):
                     raise ValueError(f"out buffer must be a contiguous float64 CPU tensor {shape}")
         if chunk_points is None:
-            chunk_points = min(1 << 20, max(1 << 17, -(-n // 6)))
+            chunk_points = min(1 << 20, max(1 << 17, -(-n // 4)))
         chunk = max(1, min(int(chunk_points), max(n, 1)))
+        pipe = _host_pipe(dev)
+        with pipe["lock"]:
+            return self._eval_host_run(src, host, want, n, chunk, t, mode, pot, dev, pipe)
+
+    def _eval_host_run(self, src, host, want, n, chunk, t, mode, pot, dev, pipe):
         cur = torch.cuda.current_stream(dev)
-        s_in, s_cmp, s_out = (torch.cuda.Stream(device=dev) for _ in range(3))
+        s_in, s_cmp, s_out = pipe["streams"]
         for s in (s_in, s_cmp, s_out):
             s.wait_stream(cur)
-        f64 = dict(dtype=torch.float64, device=dev)
-        with torch.cuda.device(dev):
-            xb = [torch.empty((chunk, 3), **f64) for _ in range(2)]
-            ob = [[torch.empty((chunk,) + shape[1:], **f64) if w else None
-                   for w, shape, _ in want] for _ in range(2)]
+        xb = pipe_buffers(pipe, dev, ("x", chunk), (chunk, 3))
+        ob = [[pipe_buffers(pipe, dev, (k, chunk), (chunk,) + shape[1:])[j] if w else None
+               for w, shape, k in want] for j in range(2)]
         ev_in = [torch.cuda.Event() for _ in range(2)]
         ev_cmp = [torch.cuda.Event() for _ in range(2)]
         ev_out = [torch.cuda.Event() for _ in range(2)]
@@ -448,6 +451,32 @@ class _GPUPotBase:
         s_out.synchronize()
         res = [h for h in host if h is not None]
         return res[0] if len(res) == 1 else tuple(res)
+
+
+# Per device: the three streams of eval_host and its double-buffered device chunks,
+# kept between calls so that a call allocates nothing once the sizes were seen
+# (torch's allocator caches blocks per stream).  A lock serialises callers.
+_HOST_PIPES = {}
+
+
+def _host_pipe(dev: torch.device) -> dict:
+    key = dev.index
+    pipe = _HOST_PIPES.get(key)
+    if pipe is None:
+        import threading
+        pipe = {"lock": threading.Lock(), "bufs": {},
+                "streams": tuple(torch.cuda.Stream(device=dev) for _ in range(3))}
+        _HOST_PIPES[key] = pipe
+    return pipe
+
+
+def pipe_buffers(pipe: dict, dev: torch.device, key, shape):
+    bufs = pipe["bufs"].get(key)
+    if bufs is None:
+        with torch.cuda.device(dev):
+            bufs = [torch.empty(shape, dtype=torch.float64, device=dev) for _ in range(2)]
+        pipe["bufs"][key] = bufs
+    return bufs
 
 
 class _Component(_GPUPotBase):
