@@ -75,6 +75,19 @@ def main(out_path: Path) -> None:
             else:
                 beta.append(Decimal(0))
 
+    # Rescaled recurrence Q_l = Ybar_l / C_l with C_l = prod_{j=m+1..l} ALPHA[m][j]:
+    #   Q_l = cos(theta) Q_{l-1} - BETAQ[m][l] Q_{l-2},  BETAQ = BETA[m][l] / (ALPHA[m][l] ALPHA[m][l-1])
+    # (stored negated); the C_l are folded into the coefficient tables of regular
+    # structures, so the walk needs one constant and one multiply less per step.
+    nbetaq = []
+    for m in range(LMAX + 1):
+        for l in range(LMAX + 1):
+            i = m * (LMAX + 1) + l
+            if l >= m + 2:
+                nbetaq.append(-beta[i] / (alpha[i] * alpha[i - 1]))
+            else:
+                nbetaq.append(Decimal(0))
+
     def arr(name, vals, typ="double", per_line=4):
         items = [f"{float(v)!r}" + ("f" if typ == "float" else "") for v in vals]
         lines = [", ".join(items[i:i + per_line]) for i in range(0, len(items), per_line)]
@@ -95,7 +108,9 @@ def main(out_path: Path) -> None:
            arr("AGB_ALPHA", alpha),
            arr("AGB_BETA", beta),
            arr("AGB_ALPHA_F", alpha, "float"),
-           arr("AGB_BETA_F", beta, "float")]
+           arr("AGB_BETA_F", beta, "float"),
+           arr("AGB_NBETAQ", nbetaq),
+           arr("AGB_NBETAQ_F", nbetaq, "float")]
     out_path.write_text("\n".join(src))
 
 

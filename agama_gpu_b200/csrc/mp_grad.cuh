@@ -445,10 +445,13 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
         gc.zero();
         gs.zero();
         const int tb = m * AGB_LEG_N;
+        // the rescaled recurrence of the regular tables (multipole.cuh); the emitted
+        // gradients are then w.r.t. the rescaled coefficients (the host multiplies
+        // each column by its scale)
         auto step = [&](int L) {
-            const R a = MPConst<R>::alpha(tb + L), b = MPConst<R>::beta(tb + L);
-            const R Pn = fma(a * cth, Pc, -b * Pp);
-            const R dPn = fma(a, fma(cth, dPc, -sth * Pc), -b * dPp);
+            const R nb = MPConst<R>::nbetaq(tb + L);
+            const R Pn = fma(cth, Pc, nb * Pp);
+            const R dPn = fma(cth, dPc, fma(-sth, Pc, nb * dPp));
             dPp = dPc; dPc = dPn; Pp = Pc; Pc = Pn;
         };
         auto acc = [&](int L) {

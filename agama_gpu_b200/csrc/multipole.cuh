@@ -60,10 +60,12 @@ template <typename R> struct MPConst;
 template <> struct MPConst<double> {
     static __device__ __forceinline__ double alpha(int i) { return AGB_ALPHA[i]; }
     static __device__ __forceinline__ double beta(int i) { return AGB_BETA[i]; }
+    static __device__ __forceinline__ double nbetaq(int i) { return AGB_NBETAQ[i]; }
 };
 template <> struct MPConst<float> {
     static __device__ __forceinline__ float alpha(int i) { return AGB_ALPHA_F[i]; }
     static __device__ __forceinline__ float beta(int i) { return AGB_BETA_F[i]; }
+    static __device__ __forceinline__ float nbetaq(int i) { return AGB_NBETAQ_F[i]; }
 };
 
 // Quintic coefficients of harmonic c in radial interval k.
@@ -282,8 +284,13 @@ __device__ __forceinline__ void mp_col_acc(MPCol<R>& g, const R a[6], const R sp
     constexpr bool NEED_B = MODE != AGB_MODE_POT;
     constexpr bool NEED_D = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
     constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
-    // C = sum a_j s^j as two short chains
-    const R C = fma(a[2], sp[2], fma(a[1], sp[1], a[0])) + fma(a[5], sp[5], fma(a[4], sp[4], a[3] * sp[3]));
+    // C = sum a_j s^j: Horner in FP32 (one instruction less); two short chains in
+    // FP64, where the longer dependent DFMA chain costs more than it saves
+    R C;
+    if (std::is_same<R, float>::value)
+        C = fma(fma(fma(fma(fma(a[5], sp[1], a[4]), sp[1], a[3]), sp[1], a[2]), sp[1], a[1]), sp[1], a[0]);
+    else
+        C = fma(a[2], sp[2], fma(a[1], sp[1], a[0])) + fma(a[5], sp[5], fma(a[4], sp[4], a[3] * sp[3]));
     g.V = fma(C, Y, g.V);
     if (NEED_B) {
         const R dC = fma(a[2], dw[2], a[1]) + fma(a[5], dw[5], fma(a[4], dw[4], a[3] * dw[3]));
@@ -348,11 +355,13 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
         gc.zero();
         gs.zero();
         const int tb = m * AGB_LEG_N;
+        // rescaled recurrence (Q_l = Ybar_l / C_l, the C_l folded into the regular
+        // tables): Q_l = cos Q_{l-1} - betaq Q_{l-2}, dQ_l = cos dQ_{l-1} - sin Q_{l-1} - betaq dQ_{l-2}
         auto step = [&](int L) {
-            const R a = MPConst<R>::alpha(tb + L), b = MPConst<R>::beta(tb + L);
-            const R Pn = fma(a * cth, Pc, -b * Pp);
+            const R nb = MPConst<R>::nbetaq(tb + L);
+            const R Pn = fma(cth, Pc, nb * Pp);
             if (NEED_ANG) {
-                const R dPn = fma(a, fma(cth, dPc, -sth * Pc), -b * dPp);
+                const R dPn = fma(cth, dPc, fma(-sth, Pc, nb * dPp));
                 dPp = dPc;
                 dPc = dPn;
             }

@@ -297,6 +297,9 @@ class _GPUPotBase:
                 continue
             comp = key
             cols = torch.from_numpy(comp._col_of).to(g.device)
+            # the fused adjoint differentiates the rescaled table: back to the builder's
+            scale = torch.from_numpy(comp._col_scale).to(g.device)
+            g = g * scale[None, :, None]
             gp = g.index_select(1, cols).permute(1, 0, 2).contiguous()
             out[comp] = out[comp] + gp if comp in out else gp
         return out
@@ -544,6 +547,15 @@ class MultipolePotentialGPU(_Component):
                     if am > 0:
                         cols[(l, -am)] = len(cols)
             self._col_of = np.array([cols[(int(l), int(m))] for l, m in zip(t.lm_l, t.lm_m)])
+        # regular structures: column (l, m) carries the scale C_l^m = prod_{j=|m|+1..l}
+        # sqrt((4j^2 - 1) / (j^2 - m^2)) of the kernels' rescaled Legendre recurrence
+        self._col_scale = np.ones(self._n_cols)
+        if reg is not None:
+            for (l, m), c in cols.items():
+                am = abs(m)
+                j = np.arange(am + 1, l + 1, dtype=np.float64)
+                self._col_scale[c] = float(np.prod(np.sqrt((4 * j * j - 1) / (j * j - am * am))))
+            poly = poly * self._col_scale[:, None, None]
         self._poly_im = np.ascontiguousarray(poly.transpose(1, 0, 2))
         p32 = np.zeros((t.n_int, self._n_cols, 8), dtype=np.float32)
         p32[:, :, :6] = self._poly_im.astype(np.float32)

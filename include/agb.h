@@ -112,7 +112,11 @@ extern "C" {
  *              AGB_STRUCT_ALL / AGB_STRUCT_EVEN: the columns are every (l, m)
  *              with l <= lmax (every l, or even l only), ordered by (|m|, l,
  *              cos before sin), pruned harmonics present as zero columns; the
- *              kernel then walks the harmonics without reading lm
+ *              kernel then walks the harmonics without reading lm; in these
+ *              structures column (l, m) holds its coefficients multiplied by
+ *              C_l^|m| = prod_{j=|m|+1..l} sqrt((4j^2 - 1) / (j^2 - m^2)) (both
+ *              tables), the normalisation the kernels' rescaled Legendre
+ *              recurrence leaves out
  *   p[0..9]    logr_min, dlogr, inv_dlogr, invPhi0, inner_s, inner_U, inner_W,
  *              outer_s, outer_U, outer_W
  * CYLSPLINE  (tables from gpu_potential.py:1143-1253, relaid per cell)

@@ -223,6 +223,7 @@ def _mp_variants():
     t = lst.tables
     lst._structure, lst._n_cols = 0, t.n_lm
     lst._poly_im, lst._poly32 = t.interval_major(), t.interval_major_f32()
+    lst._col_scale = np.ones(t.n_lm)
     lst._col_of = np.arange(t.n_lm)
     return [reg, lst]
 

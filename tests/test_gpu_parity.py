@@ -262,6 +262,7 @@ def test_list_and_regular_structures_agree():
         t = lst.tables
         lst._structure, lst._n_cols = 0, t.n_lm
         lst._poly_im, lst._poly32 = t.interval_major(), t.interval_major_f32()
+        lst._col_scale = np.ones(t.n_lm)
         assert reg._structure != 0 and reg._n_cols > t.n_lm
         xyz = _big_points(40_000, 3)
         x = torch.from_numpy(xyz).cuda()
