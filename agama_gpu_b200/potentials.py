@@ -427,9 +427,8 @@ class _GPUPotBase:
         ev_cmp = [torch.cuda.Event() for _ in range(2)]
         ev_out = [torch.cuda.Event() for _ in range(2)]
         started = [False, False]
-        for i, lo in enumerate(range(0, n, chunk)):
+        for i, (lo, hi) in enumerate(_chunk_bounds(n, chunk)):
             b = i & 1
-            hi = min(n, lo + chunk)
             m = hi - lo
             with torch.cuda.stream(s_in):
                 if started[b]:
@@ -454,6 +453,27 @@ class _GPUPotBase:
         s_out.synchronize()
         res = [h for h in host if h is not None]
         return res[0] if len(res) == 1 else tuple(res)
+
+
+def _chunk_bounds(n: int, chunk: int):
+    """Chunk ranges of eval_host: a quarter chunk first and last (the first copy-in
+    and the last copy-out cannot overlap a kernel, so they are kept short), full
+    chunks in between."""
+    q = max(1, chunk // 4)
+    if n <= 2 * chunk:
+        return [(lo, min(n, lo + chunk)) for lo in range(0, n, chunk)]
+    out = [(0, q)]
+    lo = q
+    while n - lo > chunk + q:
+        out.append((lo, lo + chunk))
+        lo += chunk
+    rest = n - lo
+    if rest > q:
+        out.append((lo, n - q))
+        out.append((n - q, n))
+    else:
+        out.append((lo, n))
+    return out
 
 
 # Per device: the three streams of eval_host and its double-buffered device chunks,
