@@ -383,7 +383,7 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
             int l = m;
             while (l < l0) step(++l);
             acc(l, has_sin);
-            #pragma unroll 2
+            #pragma unroll 4
             for (l = l0 + PAR; l <= lmax; l += PAR) {
                 if (PAR == 2) step(l - 1);
                 step(l);

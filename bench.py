@@ -557,7 +557,7 @@ def main():
         "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
                 "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,
                 "ms_per_step": e2e_ms, "finite": e2e_ok,
-                "path": "pot.eval_host(pinned xyz, pot=True, acc=True): N/6-point chunks, "
+                "path": "pot.eval_host(pinned xyz, pot=True, acc=True): N/4-point chunks (quarter-size first and last), "
                         "H2D / kernel / D2H overlapped on three streams"},
         "gpu_launches": int(l32),
         "roofline": {
