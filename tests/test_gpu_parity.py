@@ -329,3 +329,45 @@ def test_cylspline_mixed_precision():
     assert rel_max(_np(p32)[inside], _np(p64)[inside]) <= 1e-7
     assert rel_max(_np(d32)[inside], _np(d64)[inside]) <= 1e-5
     assert np.array_equal(_np(f32)[~inside], _np(f64)[~inside])
+
+
+def test_finite_difference_self_consistency():
+    """F = -grad Phi, forceDeriv = dF/dx and density = Laplacian/(4 pi G) by central
+    differences of the kernel's own outputs (FP64), for a Multipole + analytic composite
+    and for a CylSpline (whose density keeps the reference's sign, -trace H / 4 pi G)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import nfw_multipole
+    rng = np.random.default_rng(17)
+    mp = (agb.MultipolePotentialGPU(nfw_multipole(lmax=8, n_nodes=50, seed=4, amp=0.3))
+          + agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3)
+          + agb.PlummerPotentialGPU(mass=1e10, scaleRadius=1.0))
+    cs = agb.CylSplinePotentialGPU(cs_coefs(golden("cs_cfg1")))
+    for pot, sign in ((mp, 1.0), (cs, -1.0)):
+        r = np.exp(rng.uniform(np.log(0.5), np.log(80.0), 400))
+        u = rng.normal(size=(400, 3))
+        xyz = u / np.linalg.norm(u, axis=1)[:, None] * r[:, None]
+        xyz = xyz[np.hypot(xyz[:, 0], xyz[:, 1]) > 0.3]          # inside the CylSpline grid
+        x = torch.from_numpy(xyz).cuda()
+        phi, F, D = pot.evalDeriv(x)
+        rho = pot.density(x)
+        hs = 1e-5 * np.maximum(np.linalg.norm(xyz, axis=1), 1.0)
+        fd_F = np.zeros_like(xyz)
+        fd_D = np.zeros((len(xyz), 3, 3))
+        for d in range(3):
+            e = np.zeros_like(xyz)
+            e[:, d] = hs
+            pp, Fp, _ = pot.evalDeriv(torch.from_numpy(xyz + e).cuda())
+            pm, Fm, _ = pot.evalDeriv(torch.from_numpy(xyz - e).cuda())
+            fd_F[:, d] = -(_np(pp) - _np(pm)) / (2 * hs)
+            fd_D[:, :, d] = (_np(Fp) - _np(Fm)) / (2 * hs)[:, None]
+        Fn, Dn = _np(F), _np(D)
+        assert np.abs(Fn - fd_F).max() <= 1e-6 * np.abs(Fn).max()
+        # forceDeriv order [xx, yy, zz, xy, yz, zx]
+        Dm = np.stack([fd_D[:, 0, 0], fd_D[:, 1, 1], fd_D[:, 2, 2], fd_D[:, 0, 1], fd_D[:, 1, 2],
+                       fd_D[:, 2, 0]], 1)
+        if pot is mp:      # the CylSpline forceDeriv omits the reference's dPhi/dphi terms
+            assert np.abs(Dn - Dm).max() <= 1e-5 * np.abs(Dn).max()
+        lap = -(Dn[:, 0] + Dn[:, 1] + Dn[:, 2])
+        want = sign * lap * agb.INV_4PIG
+        assert np.abs(_np(rho) - want).max() <= 1e-9 * np.abs(want).max()
