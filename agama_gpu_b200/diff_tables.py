@@ -77,16 +77,23 @@ def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) 
     return quintic_poly_torch(logr, f, df, float(tables.dlogr))
 
 
-def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int) -> Tuple[torch.Tensor, torch.Tensor]:
+def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int,
+             nodes=None) -> Tuple[torch.Tensor, torch.Tensor]:
     """Carry dL/dpoly back to the node tables in the coefficient file's column order.
 
     Returns (dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_cols); columns
     the table builder pruned (all-zero) get zero (build with prune_threshold=0
-    to differentiate every harmonic).
+    to differentiate every harmonic).  ``nodes`` = (phi, dphi_dr) in the builder's
+    order when the tables were replaced on the device (set_node_tables), else the
+    builder's own node values are used.
     """
     dev = grad_poly.device
-    phi = torch.tensor(tables.node_phi, dtype=torch.float64, device=dev, requires_grad=True)
-    dphi = torch.tensor(tables.node_dphi_dr, dtype=torch.float64, device=dev, requires_grad=True)
+    if nodes is None:
+        phi = torch.tensor(tables.node_phi, dtype=torch.float64, device=dev, requires_grad=True)
+        dphi = torch.tensor(tables.node_dphi_dr, dtype=torch.float64, device=dev, requires_grad=True)
+    else:
+        phi = nodes[0].detach().to(dev, torch.float64).requires_grad_(True)
+        dphi = nodes[1].detach().to(dev, torch.float64).requires_grad_(True)
     poly = multipole_poly_from_nodes(tables, phi, dphi)
     gphi, gdphi = torch.autograd.grad(poly, (phi, dphi), grad_outputs=grad_poly.to(torch.float64))
     cols = torch.as_tensor(np.asarray(tables.node_cols), dtype=torch.long, device=dev)

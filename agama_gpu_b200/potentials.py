@@ -577,22 +577,25 @@ class MultipolePotentialGPU(_Component):
                 self._col_scale[c] = float(np.prod(np.sqrt((4 * j * j - 1) / (j * j - am * am))))
             poly = poly * self._col_scale[:, None, None]
         self._poly_im = np.ascontiguousarray(poly.transpose(1, 0, 2))
-        p32 = np.zeros((t.n_int, self._n_cols, 8), dtype=np.float32)
-        p32[:, :, :6] = self._poly_im.astype(np.float32)
+        # FP32 table: 8-float records (a0..a5, 2 pads); with a regular structure each
+        # m>0 (cos, sin) column pair is one 16-float record c0 s0 c1 s1 ... c5 s5 + 4
+        # pads.  _p32_src maps every float of an interval's FP32 slab to its source in
+        # the FP64 slab (n_cols x 6), -1 for a pad.
+        src = np.full(self._n_cols * 8, -1, dtype=np.int64)
+        for c in range(self._n_cols):
+            src[c * 8:c * 8 + 6] = c * 6 + np.arange(6)
         if reg is not None:
-            # FP32 table of a regular structure: each m>0 (cos, sin) column pair as one
-            # 16-float record, c0 s0 c1 s1 ... c5 s5 + 4 pads (the mixed kernel reads
-            # the pair with packed two-lane loads); m=0 columns keep 8-float records
-            flat = p32.reshape(t.n_int, self._n_cols * 8)
             for (l, m), c in cols.items():
                 if m > 0:
-                    rec = np.zeros((t.n_int, 16), dtype=np.float32)
-                    rec[:, 0:12:2] = p32[:, c, :6]
-                    rec[:, 1:12:2] = p32[:, c + 1, :6]
-                    flat[:, c * 8:(c + 2) * 8] = rec
-            p32 = flat.reshape(t.n_int, self._n_cols, 8)
-        self._poly32 = p32
+                    src[c * 8:(c + 2) * 8] = -1
+                    src[c * 8:c * 8 + 12:2] = c * 6 + np.arange(6)
+                    src[c * 8 + 1:c * 8 + 12:2] = (c + 1) * 6 + np.arange(6)
+        self._p32_src = src
+        flat64 = self._poly_im.reshape(t.n_int, self._n_cols * 6)
+        p32 = np.where(src >= 0, flat64[:, np.maximum(src, 0)], 0.0).astype(np.float32)
+        self._poly32 = np.ascontiguousarray(p32.reshape(t.n_int, self._n_cols, 8))
         self._lm = t.lm_packed()
+        self._nodes = None          # device node tables set by set_node_tables()
 
     @classmethod
     def from_file(cls, path: Union[str, Path], **kw) -> "MultipolePotentialGPU":
@@ -665,14 +668,57 @@ class MultipolePotentialGPU(_Component):
         """
         from .diff_tables import node_vjp
         n_file = int(max(self.tables.node_cols)) + 1 if self._n_file_cols is None else self._n_file_cols
-        return node_vjp(self.tables, grad_poly, n_file)
+        return node_vjp(self.tables, grad_poly, n_file, nodes=self._nodes)
 
     _n_file_cols = None
 
+    def _device_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor):
+        """(FP64 interval-major, FP32) device tables of this object's layout from node
+        tables (nR, n_lm) in the builder's harmonic order, computed with torch on
+        their device (differentiable restatement of the builder: diff_tables)."""
+        from .diff_tables import multipole_poly_from_nodes
+        t = self.tables
+        dev = phi.device
+        pb = multipole_poly_from_nodes(t, phi.to(torch.float64), dphi_dr.to(torch.float64))
+        full = torch.zeros((self._n_cols, t.n_int, 6), dtype=torch.float64, device=dev)
+        full[torch.from_numpy(self._col_of).to(dev)] = pb
+        full = full * torch.from_numpy(self._col_scale).to(dev)[:, None, None]
+        im = full.permute(1, 0, 2).contiguous()
+        src = torch.from_numpy(self._p32_src).to(dev)
+        flat = im.reshape(t.n_int, self._n_cols * 6)
+        p32 = torch.where(src >= 0, flat[:, src.clamp(min=0)], torch.zeros((), dtype=torch.float64,
+                                                                           device=dev))
+        return im, p32.to(torch.float32).reshape(t.n_int, self._n_cols, 8).contiguous()
+
+    def set_node_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor) -> None:
+        """Replace the expansion's node values Phi_lm(r_i) and dPhi_lm/dr(r_i) -- (nR,
+        n_lm) tensors in the builder's harmonic order (the layout of tables.node_phi) --
+        rebuilding the quintic tables on the GPU, in place: nothing goes through the
+        host, and CUDA graphs captured over this potential (leapfrog) stay valid and
+        see the new tables.  The radial grid, the harmonic set, invPhi0 and the l=0
+        extrapolation constants are kept from construction (the same constants that
+        node_gradients() holds fixed).  Not differentiable itself: use
+        node_gradients() on the adjoint's table gradient."""
+        if phi.shape != self.tables.node_phi.shape or dphi_dr.shape != phi.shape:
+            raise ValueError(f"node tables must have shape {self.tables.node_phi.shape}")
+        dev = phi.device if phi.device.type == "cuda" else _cuda_device()
+        phi = phi.detach().to(dev, torch.float64)
+        dphi_dr = dphi_dr.detach().to(dev, torch.float64)
+        im, p32 = self._device_tables(phi, dphi_dr)
+        self._nodes = (phi, dphi_dr)
+        self._node_tables = (im, p32)
+        for cdev, (_, keep) in self.__dict__.get("_dev_cache", {}).items():
+            keep[0].copy_(im.to(cdev), non_blocking=True)
+            keep[1].copy_(p32.to(cdev), non_blocking=True)
+
     def _upload(self, dev):
         t = self.tables
-        poly = torch.from_numpy(self._poly_im).to(dev)
-        poly32 = torch.from_numpy(self._poly32).to(dev)
+        over = self.__dict__.get("_node_tables")
+        if over is not None:
+            poly, poly32 = over[0].to(dev).clone(), over[1].to(dev).clone()
+        else:
+            poly = torch.from_numpy(self._poly_im).to(dev)
+            poly32 = torch.from_numpy(self._poly32).to(dev)
         lm = torch.from_numpy(self._lm).to(dev)
         c = _lib.AgbComponent()
         c.kind = self.kind

@@ -453,3 +453,51 @@ def test_leapfrog_cylspline_table_gradients():
         fd = (run(agb.CylSplinePotentialGPU._from_tables(tp)) -
               run(agb.CylSplinePotentialGPU._from_tables(tm))) / (2 * step)
         assert abs(g[h, i, j, q] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(g).max()), (h, i, j, q, g[h, i, j, q], fd)
+
+
+def test_set_node_tables_on_device():
+    """Rebuilding a Multipole's tables on the GPU from new node values: equal to a
+    fresh host-built object (l>0 changes leave invPhi0 and the extrapolation alone),
+    in place (a captured leapfrog graph sees them), and node_gradients() follows."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.coefs import MultipoleCoefs
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    coefs = nfw_multipole(lmax=6, n_nodes=40, seed=21, amp=0.3)
+    mp = agb.MultipolePotentialGPU(coefs)
+    t = mp.tables
+    xyz = torch.from_numpy(_pts(5000, 22, 0.05, 500.0)).cuda()
+    x0, v0 = _disk_ics(200, 23)
+    integ = Leapfrog(mp, 0.002, graph_steps=5)
+    assert integ.use_graph
+    xa, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)          # captures the graph
+    f0 = mp.force(xyz)
+    # the same nodes rebuilt on the device: the same tables
+    mp.set_node_tables(torch.from_numpy(t.node_phi).cuda(), torch.from_numpy(t.node_dphi_dr).cuda())
+    f1 = mp.force(xyz)
+    assert float((f1 - f0).abs().max()) <= 1e-12 * float(f0.abs().max())
+    # new l>0 values: compare with a potential built on the host from the same coefficients
+    lab = coefs.lm_labels
+    phi2, dphi2 = coefs.phi.copy(), coefs.dphi_dr.copy()
+    c22 = lab.index((2, 2))
+    phi2[:, c22] *= 1.7
+    dphi2[:, c22] *= 1.7
+    ref = agb.MultipolePotentialGPU(MultipoleCoefs(coefs.R_grid, phi2, dphi2, lab))
+    nodes_p = torch.from_numpy(ref.tables.node_phi).cuda()
+    nodes_d = torch.from_numpy(ref.tables.node_dphi_dr).cuda()
+    mp.set_node_tables(nodes_p, nodes_d)
+    for prec in ("fp64", "mixed"):
+        fm = mp._launch(xyz, 0.0, 1, True, precision=prec)[1]
+        fr = ref._launch(xyz, 0.0, 1, True, precision=prec)[1]
+        assert float((fm - fr).abs().max()) <= 1e-12 * float(fr.abs().max()), prec
+    # the graph captured before the change integrates in the new potential
+    xb, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)
+    xc, _, _ = Leapfrog(ref, 0.002, use_graph=False).run(x0, v0, 10, checkpoint_every=64)
+    assert not torch.equal(xa, xb)
+    assert float((xb - xc).abs().max()) <= 1e-11 * float(xc.abs().max())
+    # node gradients are taken at the new nodes
+    g = mp.table_vjp(xyz, 0.0, None, torch.ones_like(xyz))
+    gp, gd = mp.node_gradients(g)
+    gp_ref, gd_ref = ref.node_gradients(ref.table_vjp(xyz, 0.0, None, torch.ones_like(xyz)))
+    assert float((gp - gp_ref).abs().max()) <= 1e-9 * float(gp_ref.abs().max())
