@@ -18,6 +18,11 @@ evaluations), a re-computation (n evaluations; none when every step is a
 checkpoint, which is what ``checkpoint_every=None`` picks whenever the
 positions of every step fit in 60% of the free device memory) and n+1 VJPs.
 
+Higher order: ``scheme="yoshida4"`` composes each step of three such
+kick-drift-kick substeps of sizes w1 dt, w0 dt, w1 dt (Yoshida 1990, 4th
+order, three force evaluations per step); the checkpoints and the adjoint then
+run over substeps with their own dt_j and h_j = dt_j / 2.
+
 For potentials that do not depend on time, steps are captured into CUDA
 graphs (``graph_steps`` per graph) and replayed.
 """
@@ -60,6 +65,8 @@ def auto_checkpoint_every(like: torch.Tensor, n_steps: int, fraction: float = 0.
     re-computation in the adjoint) when they fit, else the smallest k whose (x, v)
     checkpoints fit."""
     row = like.numel() * 8
+    if like.device.type != "cuda":
+        return 64
     try:
         free, _ = torch.cuda.mem_get_info(like.device)
     except (RuntimeError, AssertionError):
@@ -84,15 +91,54 @@ def allreduce_table_grads(tg: dict, group=None) -> dict:
     return tg
 
 
+_CBRT2 = 2.0 ** (1.0 / 3.0)
+SCHEMES = {
+    # kick-drift-kick substeps of fractions c_j of the step (sum 1), applied in turn
+    "leapfrog": (1.0,),
+    # Yoshida (1990) 4th-order composition: w1, w0, w1 with w1 = 1/(2 - 2^(1/3)),
+    # w0 = -2^(1/3)/(2 - 2^(1/3)); three force evaluations per step
+    "yoshida4": (1.0 / (2.0 - _CBRT2), -_CBRT2 / (2.0 - _CBRT2), 1.0 / (2.0 - _CBRT2)),
+}
+
+
+def scheme_coefficients(scheme) -> Tuple[float, ...]:
+    """Substep fractions of a scheme name in ``SCHEMES`` or an explicit sequence
+    (a symmetric composition of leapfrog substeps, fractions summing to 1)."""
+    if isinstance(scheme, str):
+        if scheme not in SCHEMES:
+            raise ValueError(f"unknown integration scheme {scheme!r}; known: {sorted(SCHEMES)}")
+        return SCHEMES[scheme]
+    c = tuple(float(x) for x in scheme)
+    if not c or abs(sum(c) - 1.0) > 1e-12:
+        raise ValueError("substep fractions must be non-empty and sum to 1")
+    return c
+
+
 class Leapfrog:
-    """Integrate N particles; keeps x, v, F as device buffers updated in place."""
+    """Integrate N particles; keeps x, v, F as device buffers updated in place.
+
+    ``scheme`` composes each step of S kick-drift-kick substeps of sizes c_j dt
+    ("leapfrog": S = 1; "yoshida4": the 4th-order triple, S = 3).  Substeps are the
+    unit of the forward and of the adjoint: substep g (step g // S, fraction
+    c[g % S]) ends at time t0 + (g // S) dt + (c_0 + ... + c_{g % S}) dt.
+    """
 
     def __init__(self, pot, dt: float, t0: float = 0.0, precision: Optional[str] = None,
-                 use_graph: Optional[bool] = None, graph_steps: int = 16):
+                 use_graph: Optional[bool] = None, graph_steps: int = 16, scheme="leapfrog"):
         self.pot = pot
         self.dt = float(dt)
         self.h = 0.5 * self.dt
         self.t0 = float(t0)
+        self.coefs = scheme_coefficients(scheme)
+        self.S = len(self.coefs)
+        if self.S == 1:
+            self._sub = [(self.dt, self.h, self.dt)]
+        else:
+            cum, sub = 0.0, []
+            for c in self.coefs:
+                cum += c
+                sub.append((c * self.dt, 0.5 * c * self.dt, cum * self.dt))
+            self._sub = sub                 # (dt_j, h_j, end offset within the step)
         self.precision = precision
         self.static = is_static(pot)
         self.use_graph = self.static if use_graph is None else (use_graph and self.static)
@@ -105,11 +151,31 @@ class Leapfrog:
         self.pot._launch(x, t, _lib.MODE_GRAD, False, precision=self.precision,
                          out=(None, F, None, None))
 
+    def _t(self, g: int) -> float:
+        """Time at the end of substep g - 1 (= at the start of substep g)."""
+        n, j = divmod(int(g), self.S)
+        return self.t0 + n * self.dt + (self._sub[j - 1][2] if j else 0.0)
+
+    def _substep(self, x, v, F, g: int) -> None:
+        dtj, hj, off = self._sub[g % self.S]
+        v.add_(F, alpha=hj)
+        x.add_(v, alpha=dtj)
+        self._force_into(x, self.t0 + (g // self.S) * self.dt + off, F)
+        v.add_(F, alpha=hj)
+
     def _step(self, x, v, F, t) -> None:
-        v.add_(F, alpha=self.h)
-        x.add_(v, alpha=self.dt)
-        self._force_into(x, t + self.dt, F)
-        v.add_(F, alpha=self.h)
+        """One step from time t (all S substeps)."""
+        if self.S == 1:
+            v.add_(F, alpha=self.h)
+            x.add_(v, alpha=self.dt)
+            self._force_into(x, t + self.dt, F)
+            v.add_(F, alpha=self.h)
+            return
+        for dtj, hj, off in self._sub:
+            v.add_(F, alpha=hj)
+            x.add_(v, alpha=dtj)
+            self._force_into(x, t + off, F)
+            v.add_(F, alpha=hj)
 
     def _advance(self, x, v, F, n0: int, n_steps: int) -> None:
         """n_steps steps from step index n0 (time t0 + n0 dt)."""
@@ -150,28 +216,38 @@ class Leapfrog:
     # -- forward with checkpoints ------------------------------------------------------
     def run(self, x0: torch.Tensor, v0: torch.Tensor, n_steps: int,
             checkpoint_every: Optional[int] = 64) -> Tuple[torch.Tensor, torch.Tensor, List]:
-        """Returns (x_T, v_T, checkpoints); checkpoints = [(step, x, v)] every k steps and
-        at the end.  k = 1 keeps every step's positions (v is None except at the end) and
-        the adjoint then re-computes nothing; checkpoint_every=None picks k with
-        ``auto_checkpoint_every`` (1 whenever the trajectory fits in 60% of the free
-        device memory)."""
+        """Returns (x_T, v_T, checkpoints); checkpoints = [(substep, x, v)] every k steps
+        (substep = step * S) and at the end.  k = 1 keeps the positions at every substep
+        (v is None except at the end) and the adjoint then re-computes nothing;
+        checkpoint_every=None picks k with ``auto_checkpoint_every`` (1 whenever the
+        trajectory fits in 60% of the free device memory)."""
         x, v, F = self._buffers(x0)
         x.copy_(x0.detach())
         v.copy_(v0.detach())
         self._force_into(x, self.t0, F)
-        k = auto_checkpoint_every(x, n_steps) if checkpoint_every is None else int(checkpoint_every)
+        S = self.S
+        G = int(n_steps) * S
+        if checkpoint_every is None:
+            k = auto_checkpoint_every(x, G)
+            k = 1 if k == 1 else max(2, -(-k // S))
+        else:
+            k = int(checkpoint_every)
         k = max(1, k)
         if k == 1:
-            # every step's positions in one allocation [step][particle][3]; the adjoint
-            # re-computes nothing and needs no velocities
-            store = torch.empty((int(n_steps) + 1,) + tuple(x.shape), dtype=torch.float64,
-                                device=x.device)
-            for n in range(n_steps):
-                store[n].copy_(x)
-                self._step(x, v, F, self.t0 + n * self.dt)
-            store[n_steps].copy_(x)
-            ckpts = [(n, store[n], None) for n in range(n_steps)]
-            ckpts.append((n_steps, store[n_steps], v.clone()))
+            # every substep's positions in one allocation [substep][particle][3]; the
+            # adjoint re-computes nothing and needs no velocities
+            store = torch.empty((G + 1,) + tuple(x.shape), dtype=torch.float64, device=x.device)
+            if S == 1:
+                for n in range(n_steps):
+                    store[n].copy_(x)
+                    self._step(x, v, F, self.t0 + n * self.dt)
+            else:
+                for g in range(G):
+                    store[g].copy_(x)
+                    self._substep(x, v, F, g)
+            store[G].copy_(x)
+            ckpts = [(g, store[g], None) for g in range(G)]
+            ckpts.append((G, store[G], v.clone()))
             return x.clone(), v.clone(), ckpts
         # one allocation for all checkpoints: [checkpoint][x|v][particle][3]
         store = torch.empty((-(-int(n_steps) // k) + 1, 2) + tuple(x.shape), dtype=torch.float64,
@@ -182,14 +258,14 @@ class Leapfrog:
             j = len(ckpts)
             store[j, 0].copy_(x)
             store[j, 1].copy_(v)
-            ckpts.append((n, store[j, 0], store[j, 1]))
+            ckpts.append((n * S, store[j, 0], store[j, 1]))
             m = min(k, n_steps - n)
             self._advance(x, v, F, n, m)
             n += m
         j = len(ckpts)
         store[j, 0].copy_(x)
         store[j, 1].copy_(v)
-        ckpts.append((n_steps, store[j, 0], store[j, 1]))
+        ckpts.append((G, store[j, 0], store[j, 1]))
         return x.clone(), v.clone(), ckpts
 
     def _buffers(self, like: torch.Tensor):
@@ -213,15 +289,30 @@ class Leapfrog:
         to the coefficient-file nodes).
         Under torch.distributed (each rank integrating its own particles in the same
         potential) the table gradients are summed over the ranks of ``group``.
+
+        Per substep g (backwards; dt_g, h_g its drift and half-kick):
+            gF = h_g lv + pending;  lx += (dF/dx)^T gF at x_{g+1};
+            lv += dt_g lx;          pending = h_g lv
+        where pending is the cotangent of F(x_{g+1}) from the first half-kick of
+        substep g + 1, and at the end dL/dx0 += (dF/dx)^T pending at x_0.
         """
         tg = {} if table_grads else None
+        S = self.S
+        G = int(n_steps) * S
         lx = lam_x.detach().to(torch.float64).contiguous().clone()
         lv = lam_v.detach().to(torch.float64).contiguous().clone()
-        pending = None                      # cotangent on F(x_n) from the later half-kick
+        pending = None                      # cotangent on F(x_g) from the later half-kick
         gx = torch.empty_like(lx)
         at = {c[0]: c for c in ckpts}
-        starts = sorted(c[0] for c in ckpts if c[0] < n_steps)
-        bounds = starts + [n_steps]
+        starts = sorted(c[0] for c in ckpts if c[0] < G)
+        bounds = starts + [G]
+
+        def vjp(xg, t, g_force):
+            if tg is None:
+                self.pot._vjp(xg, t, None, g_force, precision=self.precision, out=gx)
+            else:
+                self.pot._adjoint_vjp(xg, t, None, g_force, tg, precision=self.precision, out=gx)
+
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
             _, xs, vs = at[s]
@@ -234,31 +325,23 @@ class Leapfrog:
                 X = torch.empty((last - s,) + tuple(xs.shape), dtype=torch.float64, device=xs.device)
                 x, v = xs.clone(), vs.clone()
                 F = torch.empty_like(x)
-                self._force_into(x, self.t0 + s * self.dt, F)
-                for n in range(s, last):
-                    self._step(x, v, F, self.t0 + n * self.dt)
-                    X[n - s].copy_(x)
-                    pos[n + 1] = X[n - s]
-            for n in range(e - 1, s - 1, -1):
-                gF = lv * self.h
+                self._force_into(x, self._t(s), F)
+                for g in range(s, last):
+                    self._substep(x, v, F, g)
+                    X[g - s].copy_(x)
+                    pos[g + 1] = X[g - s]
+            for g in range(e - 1, s - 1, -1):
+                dtg, hg, _ = self._sub[g % S]
+                gF = lv * hg
                 if pending is not None:
                     gF.add_(pending)
-                if tg is None:
-                    self.pot._vjp(pos[n + 1], self.t0 + (n + 1) * self.dt, None, gF,
-                                  precision=self.precision, out=gx)
-                else:
-                    self.pot._adjoint_vjp(pos[n + 1], self.t0 + (n + 1) * self.dt, None, gF,
-                                          tg, precision=self.precision, out=gx)
+                vjp(pos[g + 1], self._t(g + 1), gF)
                 lx.add_(gx)
-                lv.add_(lx, alpha=self.dt)
-                pending = lv * self.h
+                lv.add_(lx, alpha=dtg)
+                pending = lv * hg
         if pending is not None:
             _, x0, _ = at[0]
-            if tg is None:
-                self.pot._vjp(x0, self.t0, None, pending, precision=self.precision, out=gx)
-            else:
-                self.pot._adjoint_vjp(x0, self.t0, None, pending, tg, precision=self.precision,
-                                      out=gx)
+            vjp(x0, self.t0, pending)
             lx.add_(gx)
         if tg is not None:
             return lx, lv, allreduce_table_grads(self.pot._table_grads_from_device(tg), group)
@@ -277,16 +360,17 @@ class _LeapfrogFn(torch.autograd.Function):
         if gx is None:
             gx = torch.zeros_like(ctx.ckpts[0][1])
         if gv is None:
-            gv = torch.zeros_like(ctx.ckpts[0][2])
+            gv = torch.zeros_like(ctx.ckpts[0][1])
         lx, lv = ctx.integrator.adjoint(ctx.ckpts, ctx.n_steps, gx, gv)
         return lx, lv, None, None, None
 
 
 def leapfrog(pot, x0: torch.Tensor, v0: torch.Tensor, dt: float, n_steps: int, t0: float = 0.0,
              checkpoint_every: Optional[int] = 64, precision: Optional[str] = None,
-             use_graph: Optional[bool] = None):
-    """(x_T, v_T) after n_steps leapfrog steps; differentiable w.r.t. (x0, v0) through the
+             use_graph: Optional[bool] = None, scheme="leapfrog"):
+    """(x_T, v_T) after n_steps steps of ``scheme`` (leapfrog, or a composition of
+    leapfrog substeps such as "yoshida4"); differentiable w.r.t. (x0, v0) through the
     checkpointed adjoint."""
-    integ = Leapfrog(pot, dt, t0=t0, precision=precision, use_graph=use_graph)
+    integ = Leapfrog(pot, dt, t0=t0, precision=precision, use_graph=use_graph, scheme=scheme)
     k = None if checkpoint_every is None else int(checkpoint_every)
     return _LeapfrogFn.apply(x0, v0, integ, int(n_steps), k)

@@ -127,14 +127,15 @@ def _disk_ics(n, seed):
     return torch.from_numpy(x).cuda(), torch.from_numpy(v).cuda()
 
 
+@pytest.mark.parametrize("scheme", ["leapfrog", "yoshida4"])
 @pytest.mark.parametrize("static", [True, False])
-def test_leapfrog_adjoint_matches_finite_differences(static):
+def test_leapfrog_adjoint_matches_finite_differences(static, scheme):
     import torch
     from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
     pot = _composite(static=static)
     x0, v0 = _disk_ics(16, 7)
     target = x0 + 1.0
-    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64")
+    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64", scheme=scheme)
     n_steps = 90
 
     def loss(xx, vv):
@@ -157,15 +158,16 @@ def test_leapfrog_adjoint_matches_finite_differences(static):
             assert abs(an - fd) <= 1e-5 * max(abs(fd), 1e-3 * float(lam.abs().max())), (which, an, fd)
 
 
+@pytest.mark.parametrize("scheme", ["leapfrog", "yoshida4"])
 @pytest.mark.parametrize("static", [True, False])
-def test_leapfrog_adjoint_independent_of_checkpoint_interval(static):
+def test_leapfrog_adjoint_independent_of_checkpoint_interval(static, scheme):
     """Every interval (1: the stored trajectory, no re-computation; None: chosen
     from free memory) gives the gradients of the default interval."""
     import torch
     from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
     pot = _composite(static=static)
     x0, v0 = _disk_ics(300, 17)
-    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64")
+    integ = Leapfrog(pot, gyr_to_time(2e-3), t0=0.1, precision="fp64", scheme=scheme)
     n_steps = 45
     ref = None
     for k in (16, 1, 7, 45, 200, None):
@@ -179,13 +181,14 @@ def test_leapfrog_adjoint_independent_of_checkpoint_interval(static):
         assert torch.allclose(lv, ref[2], rtol=1e-13, atol=0), k
 
 
-def test_leapfrog_graph_replay_equals_eager():
+@pytest.mark.parametrize("scheme", ["leapfrog", "yoshida4"])
+def test_leapfrog_graph_replay_equals_eager(scheme):
     import torch
     from agama_gpu_b200.integrate import Leapfrog
     pot = _composite(static=True)
     x0, v0 = _disk_ics(5000, 9)
-    a = Leapfrog(pot, 0.001, use_graph=True, graph_steps=8)
-    b = Leapfrog(pot, 0.001, use_graph=False)
+    a = Leapfrog(pot, 0.001, use_graph=True, graph_steps=8, scheme=scheme)
+    b = Leapfrog(pot, 0.001, use_graph=False, scheme=scheme)
     assert a.use_graph and not b.use_graph
     xa, va, _ = a.run(x0, v0, 40, checkpoint_every=64)
     xb, vb, _ = b.run(x0, v0, 40, checkpoint_every=64)
@@ -289,7 +292,8 @@ def test_node_gradients_match_finite_differences():
             assert abs(G[i, c] - fd) <= 1e-5 * max(abs(fd), 1e-4 * np.abs(G).max()), (which, i, c, G[i, c], fd)
 
 
-def test_leapfrog_table_gradients():
+@pytest.mark.parametrize("scheme", ["leapfrog", "yoshida4"])
+def test_leapfrog_table_gradients(scheme):
     import torch
     import agama_gpu_b200 as agb
     from agama_gpu_b200.integrate import Leapfrog
@@ -301,7 +305,7 @@ def test_leapfrog_table_gradients():
 
     def run(c, want=False):
         mp = agb.MultipolePotentialGPU(c)
-        integ = Leapfrog(mp + mn, 0.002, precision="fp64")
+        integ = Leapfrog(mp + mn, 0.002, precision="fp64", scheme=scheme)
         xT, vT, ck = integ.run(x0, v0, 60, checkpoint_every=16)
         Lv = float(((xT - target) ** 2).sum())
         if not want:
@@ -501,3 +505,29 @@ def test_set_node_tables_on_device():
     gp, gd = mp.node_gradients(g)
     gp_ref, gd_ref = ref.node_gradients(ref.table_vjp(xyz, 0.0, None, torch.ones_like(xyz)))
     assert float((gp - gp_ref).abs().max()) <= 1e-9 * float(gp_ref.abs().max())
+
+
+def test_yoshida4_order_in_composite():
+    """Global position error in a Multipole + Miyamoto-Nagai composite falls as
+    dt^4 for the 4th-order composition (and as dt^2 for leapfrog).  (A CylSpline
+    is left out: its bicubic force has jumps in dF/dx at cell edges, which cap the
+    observed order of any scheme near 3.)"""
+    import math
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    pot = agb.CompositePotentialGPU([
+        agb.MultipolePotentialGPU(nfw_multipole(lmax=6, n_nodes=40, seed=2)),
+        agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3)])
+    x0, v0 = _disk_ics(200, 21)
+    T = 0.05                                  # ~1/4 of an orbit at 8 kpc
+    ref, _, _ = Leapfrog(pot, T / 800, precision="fp64", scheme="yoshida4").run(
+        x0, v0, 800, checkpoint_every=1000)
+    for scheme, order in (("leapfrog", 2), ("yoshida4", 4)):
+        e = []
+        for n in (25, 50):
+            xT, _, _ = Leapfrog(pot, T / n, precision="fp64", scheme=scheme).run(
+                x0, v0, n, checkpoint_every=1000)
+            e.append(float((xT - ref).abs().max()))
+        rate = math.log2(e[0] / e[1])
+        assert abs(rate - order) < 0.4, (scheme, e, rate)
