@@ -15,6 +15,8 @@ from .factory import PotentialGPU
 from .potentials import (G_AGAMA, INV_4PIG, CompositePotentialGPU, CylSplinePotentialGPU,
                          EvolvingPotentialGPU, MultipolePotentialGPU, ScaledPotentialGPU,
                          ShiftedPotentialGPU, prep_xyz, set_default_precision)
+from .integrate import Leapfrog, leapfrog
+from .stream import Stream, integrate_releases, particle_spray
 
 __all__ = [
     "PotentialGPU", "BatchedPotentialGPU", "MultipolePotentialGPU", "CylSplinePotentialGPU", "CompositePotentialGPU",
@@ -23,4 +25,5 @@ __all__ = [
     "IsochronePotentialGPU", "MiyamotoNagaiPotentialGPU", "LogHaloPotentialGPU",
     "DiskAnsatzPotentialGPU", "UniformAccelerationGPU", "MultipoleCoefs", "CylSplineCoefs",
     "read_coefs", "write_coefs", "set_default_precision", "prep_xyz", "G_AGAMA", "INV_4PIG",
+    "Leapfrog", "leapfrog", "Stream", "particle_spray", "integrate_releases",
 ]
