@@ -7,8 +7,11 @@ skipped), component dicts, several positional sources -> composite, and the
 ``center=``/``scale=``/``ampl=`` modifiers (Scaled applied first, then Shifted).
 
 Types that the reference builds through Agama's CPU library (Spheroid, King,
-triaxial or gamma=2 Dehnen, Disk) need ``agama`` importable, exactly as in the
-reference; without it they raise ImportError.
+triaxial or gamma=2 Dehnen, Disk) go through Agama when ``agama`` is importable,
+exactly as in the reference; without it they are built by this package's own
+Poisson solver (density_bfe: the density projected on the device, radial
+integrals per harmonic), with the optional keywords lmax, mmax, gridSizeR,
+rmin, rmax.
 """
 from __future__ import annotations
 
@@ -31,21 +34,65 @@ def _kl(kw: dict) -> dict:
 
 
 def _agama():
+    """The agama module, or None when it is not installed."""
     try:
-        import agama  # noqa: F401
-    except ImportError as e:
-        raise ImportError("this potential type is built by Agama's CPU library "
-                          "(as in the reference); `agama` is not installed") from e
+        import agama
+    except ImportError:
+        return None
     return agama
+
+
+_SOLVER_KEYS = {"lmax": int, "mmax": int, "gridsizer": int, "rmin": float, "rmax": float}
+_SOLVER_NAMES = {"lmax": "lmax", "mmax": "mmax", "gridsizer": "gridSizeR", "rmin": "rmin",
+                 "rmax": "rmax"}
+
+
+def _split_solver(kw: dict, allowed: dict):
+    """(density parameters by canonical name, solver options) from case-insensitive kwargs."""
+    dens, solver = {}, {}
+    for k, v in kw.items():
+        key = k.lower().replace("_", "")
+        if key in _SOLVER_KEYS:
+            solver[_SOLVER_NAMES[key]] = _SOLVER_KEYS[key](v)
+        elif key in allowed:
+            dens[allowed[key]] = float(v)
+        elif key != "type":
+            raise TypeError(f"unknown parameter {k!r}")
+    return dens, solver
+
+
+_SPHEROID_KEYS = {k.lower(): k for k in (
+    "densityNorm", "mass", "scaleRadius", "gamma", "beta", "alpha", "axisRatioY", "axisRatioZ",
+    "outerCutoffRadius", "cutoffStrength")}
+_DISK_KEYS = {k.lower(): k for k in (
+    "surfaceDensity", "mass", "scaleRadius", "scaleHeight", "innerCutoffRadius", "sersicIndex")}
+_KING_KEYS = {k.lower(): k for k in ("mass", "scaleRadius", "W0", "trunc")}
+
+
+def _spheroid_own(**kw):
+    from .density_bfe import multipole_from_density, spheroid_density
+    dens, solver = _split_solver(kw, _SPHEROID_KEYS)
+    rho = spheroid_density(**dens)
+    return MultipolePotentialGPU(multipole_from_density(
+        rho, symmetry=rho.symmetry, length_hint=rho.length, **solver))
 
 
 def _build_spheroid_gpu(**kw):
     agama = _agama()
+    if agama is None:
+        return _spheroid_own(**kw)
     return MultipolePotentialGPU.from_agama(agama.Potential(type="Spheroid", **kw))
 
 
 def _build_king_gpu(**kw):
     agama = _agama()
+    if agama is None:
+        from .density_bfe import king_multipole
+        dens, solver = _split_solver(kw, _KING_KEYS)
+        extra = set(solver) - {"gridSizeR"}
+        if extra:
+            raise TypeError(f"King accepts only gridSizeR of the solver options, got {sorted(extra)}")
+        return MultipolePotentialGPU(king_multipole(**dens, **solver))
     return MultipolePotentialGPU.from_agama(agama.Potential(type="King", **kw))
 
 
@@ -63,12 +110,43 @@ def _build_dehnen_gpu(**kw):
                                            scaleRadius=float(kl.get("scaleradius", 1.0)),
                                            gamma=gamma)
     agama = _agama()
+    if agama is None:
+        return _spheroid_own(alpha=1, beta=4, **kw)
     return MultipolePotentialGPU.from_agama(agama.Potential(type="Spheroid", alpha=1, beta=4, **kw))
+
+
+def _disk_own(**kw):
+    """DiskAnsatz + a Multipole of the residual density (true disk minus ansatz),
+    axisymmetric, lmax 32 unless given."""
+    from .density_bfe import (_auto_range, disk_density, disk_residual_density,
+                              multipole_from_density)
+    dens, solver = _split_solver(kw, _DISK_KEYS)
+    rho = disk_density(**dens)
+    hz = dens.get("scaleHeight", 0.1)
+    Rd = dens.get("scaleRadius", 1.0)
+    Rin = dens.get("innerCutoffRadius", 0.0)
+    ansatz = DiskAnsatzPotentialGPU(surfaceDensity=rho.sigma0, scaleRadius=Rd, scaleHeight=hz,
+                                    innerCutoffRadius=Rin)
+    res = disk_residual_density(rho, rho.sigma0, Rd, hz, Rin)
+    solver.setdefault("lmax", 32)
+    solver.setdefault("n_theta", 2048)
+    if "rmin" not in solver or "rmax" not in solver:
+        import torch
+        dev = torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu")
+        a, b = _auto_range(rho, dev, Rd)
+        # beyond the exponential cut-off the monopole is Keplerian to ~1e-8 only well past
+        # the 1 - 1e-4 mass radius; the outer extrapolation is fitted there
+        solver.setdefault("rmin", min(a, 0.1 * abs(hz)))
+        solver.setdefault("rmax", 3.0 * b)
+    mp = MultipolePotentialGPU(multipole_from_density(res, symmetry="axisymmetric", **solver))
+    return CompositePotentialGPU([ansatz, mp])
 
 
 def _build_disk_gpu(**kw):
     """DiskAnsatz (from the input parameters) + the Multipole section of Agama's Disk export."""
     agama = _agama()
+    if agama is None:
+        return _disk_own(**kw)
     kl = _kl(kw)
     disk = DiskAnsatzPotentialGPU(
         surfaceDensity=float(kl.get("surfacedensity", kl.get("densitynorm", 1.0))),

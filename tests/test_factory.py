@@ -112,8 +112,11 @@ def test_factory_keyword_and_dict_dispatch():
         agb.PotentialGPU(type="Multipole")
     with pytest.raises(TypeError):
         agb.PotentialGPU()
-    with pytest.raises(ImportError):
-        agb.PotentialGPU(type="King", mass=1.0)     # Agama-routed; agama is not installed
+    # Agama-routed types without agama: built by the package's own Poisson solver
+    k = agb.PotentialGPU(type="King", mass=1e5, scaleRadius=0.01, W0=6)
+    assert isinstance(k, agb.MultipolePotentialGPU)
+    with pytest.raises(TypeError, match="unknown parameter"):
+        agb.PotentialGPU(type="Spheroid", mass=1e10, bogus=1)
     with pytest.raises(ValueError, match="gamma"):
         agb.DehnenSphericalPotentialGPU(gamma=2.5)
 
