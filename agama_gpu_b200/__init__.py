@@ -17,6 +17,7 @@ from .potentials import (G_AGAMA, INV_4PIG, CompositePotentialGPU, CylSplinePote
                          ShiftedPotentialGPU, prep_xyz, set_default_precision)
 from .integrate import Leapfrog, leapfrog
 from .stream import Stream, integrate_releases, particle_spray
+from .export import export_potential
 
 __all__ = [
     "PotentialGPU", "BatchedPotentialGPU", "MultipolePotentialGPU", "CylSplinePotentialGPU", "CompositePotentialGPU",
@@ -25,5 +26,5 @@ __all__ = [
     "IsochronePotentialGPU", "MiyamotoNagaiPotentialGPU", "LogHaloPotentialGPU",
     "DiskAnsatzPotentialGPU", "UniformAccelerationGPU", "MultipoleCoefs", "CylSplineCoefs",
     "read_coefs", "write_coefs", "set_default_precision", "prep_xyz", "G_AGAMA", "INV_4PIG",
-    "Leapfrog", "leapfrog", "Stream", "particle_spray", "integrate_releases",
+    "Leapfrog", "leapfrog", "Stream", "particle_spray", "integrate_releases", "export_potential",
 ]

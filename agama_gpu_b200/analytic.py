@@ -6,6 +6,8 @@ bodies.  All of them evaluate inside the same fused kernel as the expansions.
 """
 from __future__ import annotations
 
+import functools
+import inspect
 import math
 
 from . import _lib
@@ -18,12 +20,30 @@ __all__ = ["NFWPotentialGPU", "PlummerPotentialGPU", "HernquistPotentialGPU",
            "LogHaloPotentialGPU", "DiskAnsatzPotentialGPU", "UniformAccelerationGPU"]
 
 
+def _records_args(cls):
+    """Keep the constructor's arguments (``_init_args``) so the potential can be written
+    back as an INI section with the same parameters."""
+    init = cls.__init__
+    sig = inspect.signature(init)
+
+    @functools.wraps(init)
+    def wrapped(self, *args, **kwargs):
+        b = sig.bind(self, *args, **kwargs)
+        b.apply_defaults()
+        self._init_args = {k: v for k, v in b.arguments.items() if k != "self"}
+        init(self, *args, **kwargs)
+
+    cls.__init__ = wrapped
+    return cls
+
+
 def _no_agama(name: str, ctor: str):
     raise TypeError(
         f"{name}.from_agama() is not supported: Agama does not export analytic potential "
         f"parameters.\nConstruct directly:  {name}({ctor})")
 
 
+@_records_args
 class NFWPotentialGPU(_Component):
     """Phi = -G M ln(1 + r/rs) / r  (_analytic_potentials.py:176-283)."""
     kind = _lib.KIND_NFW
@@ -41,6 +61,7 @@ class NFWPotentialGPU(_Component):
         return [self._GM, self._rs, self._M]
 
 
+@_records_args
 class PlummerPotentialGPU(_Component):
     """Phi = -G M / sqrt(r^2 + b^2)  (_analytic_potentials.py:288-378)."""
     kind = _lib.KIND_PLUMMER
@@ -58,6 +79,7 @@ class PlummerPotentialGPU(_Component):
         return [self._GM, self._b2, self._M]
 
 
+@_records_args
 class HernquistPotentialGPU(_Component):
     """Phi = -G M / (r + a)  (_analytic_potentials.py:383-480)."""
     kind = _lib.KIND_HERNQUIST
@@ -75,6 +97,7 @@ class HernquistPotentialGPU(_Component):
         return [self._GM, self._a, self._M]
 
 
+@_records_args
 class DehnenSphericalPotentialGPU(_Component):
     """Phi = -(G M/a) (1 - (r/(r+a))^(2-gamma)) / (2-gamma), 0 <= gamma < 2
     (_analytic_potentials.py:486-590)."""
@@ -100,6 +123,7 @@ class DehnenSphericalPotentialGPU(_Component):
         return [self._GM, self._a, self._gamma, self._exp, self._M]
 
 
+@_records_args
 class IsochronePotentialGPU(_Component):
     """Phi = -G M / (b + sqrt(r^2 + b^2))  (_analytic_potentials.py:603-715)."""
     kind = _lib.KIND_ISOCHRONE
@@ -117,6 +141,7 @@ class IsochronePotentialGPU(_Component):
         return [self._GM, self._b]
 
 
+@_records_args
 class MiyamotoNagaiPotentialGPU(_Component):
     """Phi = -G M / sqrt(R^2 + (a + sqrt(z^2 + b^2))^2)  (_analytic_potentials.py:720-836)."""
     kind = _lib.KIND_MIYAMOTONAGAI
@@ -136,6 +161,7 @@ class MiyamotoNagaiPotentialGPU(_Component):
         return [self._GM, self._a, self._b]
 
 
+@_records_args
 class LogHaloPotentialGPU(_Component):
     """Phi = (v0^2/2) ln(rc^2 + x^2 + y^2/p^2 + z^2/q^2)  (_analytic_potentials.py:842-931).
 
@@ -158,6 +184,7 @@ class LogHaloPotentialGPU(_Component):
         return [self._v02, self._rc2, self._p2, self._q2]
 
 
+@_records_args
 class DiskAnsatzPotentialGPU(_Component):
     """Phi = f(r) H(z), f = 4 pi Sigma exp(-r/hr - hin/r)  (_analytic_potentials.py:950-1101).
 
@@ -188,6 +215,7 @@ class DiskAnsatzPotentialGPU(_Component):
         return [self._Sigma, self._hr, self._hz, self._hin]
 
 
+@_records_args
 class UniformAccelerationGPU(_Component):
     """Phi = -(ax x + ay y + az z)  (_analytic_potentials.py:1112-1165)."""
     kind = _lib.KIND_UNIFORMACC

@@ -258,6 +258,11 @@ def _fmt(v: float) -> str:
 
 def write_coefs(path: Union[str, Path], coefs: Union[MultipoleCoefs, CylSplineCoefs]) -> None:
     """Write coefficients in the same text format (round-trips through read_coefs)."""
+    Path(path).write_text(coefs_text(coefs))
+
+
+def coefs_text(coefs: Union[MultipoleCoefs, CylSplineCoefs]) -> str:
+    """The coefficient file's text: a [Potential] section with inline Coefficients."""
     out: List[str] = ["[Potential]"]
     if isinstance(coefs, MultipoleCoefs):
         lmax = coefs.lmax
@@ -281,4 +286,4 @@ def write_coefs(path: Union[str, Path], coefs: Union[MultipoleCoefs, CylSplineCo
             tab = coefs.phi[m]
             for i, R in enumerate(coefs.R_grid):
                 out.append("\t".join([_fmt(R)] + [_fmt(v) for v in tab[i]]))
-    Path(path).write_text("\n".join(out) + "\n")
+    return "\n".join(out) + "\n"

@@ -21,6 +21,8 @@ import tempfile
 import uuid
 from pathlib import Path
 
+import numpy as np
+
 from .analytic import (DehnenSphericalPotentialGPU, DiskAnsatzPotentialGPU, HernquistPotentialGPU,
                        IsochronePotentialGPU, LogHaloPotentialGPU, MiyamotoNagaiPotentialGPU,
                        NFWPotentialGPU, PlummerPotentialGPU, UniformAccelerationGPU)
@@ -239,6 +241,38 @@ def _resolve(base: Path, f: str) -> Path:
     return p if p.is_absolute() else base / p
 
 
+def _ini_modifiers(params: dict, base: Path) -> dict:
+    """center / scale / ampl of an INI section as values _apply_modifiers takes:
+    'x,y,z' (or 'x y z') -> (3,) array; a file name -> its rows ((T,4)/(T,7) track,
+    (T,2)/(T,3) scale table); 'v' or 'ampl scale' scale strings are kept."""
+    out = {}
+    for key in ("center", "scale", "ampl"):
+        for k in list(params):
+            if k.lower() == key:
+                out[key] = params.pop(k)
+    c = out.get("center")
+    if isinstance(c, str):
+        parts = [t for t in re.split(r"[,\s]+", c.strip()) if t]
+        try:
+            out["center"] = np.array([float(t) for t in parts], dtype=np.float64)
+        except ValueError:
+            out["center"] = np.loadtxt(_resolve(base, c.strip()), dtype=np.float64, ndmin=2)
+    sc = out.get("scale")
+    if isinstance(sc, str):
+        try:
+            [float(t) for t in sc.split()]
+        except ValueError:
+            out["scale"] = np.loadtxt(_resolve(base, sc.strip()), dtype=np.float64, ndmin=2)
+    return out
+
+
+def _with_modifiers(pot, mods: dict):
+    if not mods:
+        return pot
+    return _apply_modifiers(pot, mods.get("center"), mods.get("scale"),
+                            float(mods.get("ampl", 1.0)))
+
+
 def _load_potential_ini(p: Path):
     """Parse an Agama INI potential (one or more [Potential ...] sections)."""
     base = p.parent
@@ -265,19 +299,20 @@ def _load_potential_ini(p: Path):
                 k, _, v = s.partition("=")
                 params[k.strip()] = _coerce(v.split("#")[0].strip())
         typ = str(params.get("type") or params.get("Type", "")).lower().replace(" ", "").replace("_", "")
-        if typ == "diskansatz":
+        mods = _ini_modifiers(params, base)
+        if typ == "diskansatz" and len(params) <= 1:
             continue                        # exported without parameters: skipped, as the reference
         if typ in ("multipole", "cylspline"):
             cls = MultipolePotentialGPU if typ == "multipole" else CylSplinePotentialGPU
             if data_kind == "coef":
-                built.append(cls(read_coefs("\n".join(sec))))
+                built.append(_with_modifiers(cls(read_coefs("\n".join(sec))), mods))
             else:
                 f = str(params.get("file") or params.get("File", ""))
                 if not f:
                     name = "Multipole" if typ == "multipole" else "CylSpline"
                     raise ValueError(f"{name} section in {p} has neither inline Coefficients "
                                      "nor a 'file' key.")
-                built.append(cls.from_file(_resolve(base, f)))
+                built.append(_with_modifiers(cls.from_file(_resolve(base, f)), mods))
             continue
         if typ == "evolving":
             if data_kind != "ts":
@@ -299,9 +334,9 @@ def _load_potential_ini(p: Path):
             if not pots:
                 raise ValueError(f"Evolving section in {p} has no valid Timestamps entries.")
             lin = bool(params.get("linearInterp", params.get("interpLinear", False)))
-            built.append(EvolvingPotentialGPU(pots, times, interpolate=lin))
+            built.append(_with_modifiers(EvolvingPotentialGPU(pots, times, interpolate=lin), mods))
             continue
-        built.append(_build_single(params, {}))
+        built.append(_with_modifiers(_build_single(params, {}), mods))
     if not built:
         raise ValueError(f"No buildable components found in {p}. "
                          "(All sections may have been DiskAnsatz stubs with no stored params.)")

@@ -547,6 +547,7 @@ class MultipolePotentialGPU(_Component):
         # construction order: ranks that build the same potentials in the same order
         # agree on it, which fixes the order of the gradient all-reduces
         self._sync_order = next(_MULTIPOLE_SERIAL)
+        self._coefs = coefs
         self.tables = build_multipole_tables(coefs, prune_threshold=prune_threshold)
         self._n_file_cols = len(coefs.lm_labels)
         t = self.tables
@@ -940,6 +941,7 @@ class ShiftedPotentialGPU(_GPUPotBase):
     def __init__(self, inner, center) -> None:
         self._inner = inner
         center = np.asarray(center, dtype=np.float64)
+        self._center_arr = center.copy()
         if center.ndim == 1 and center.shape == (3,):
             self._is_static = True
             self._center_static = center
@@ -988,7 +990,9 @@ class ScaledPotentialGPU(_GPUPotBase):
         else:
             arr = np.asarray(scale, dtype=np.float64)
             if arr.ndim == 0:
+                scale = float(arr)
                 arr = None
+        self._scale_arr = None if arr is None else arr.copy()
         if arr is None:
             self._is_static = True
             self._scale_val = float(scale)
