@@ -18,6 +18,7 @@ from .potentials import (G_AGAMA, INV_4PIG, CompositePotentialGPU, CylSplinePote
 from .integrate import Leapfrog, leapfrog
 from .stream import Stream, integrate_releases, particle_spray
 from .export import export_potential
+from .adaptive import DormandPrince, integrate_adaptive
 
 __all__ = [
     "PotentialGPU", "BatchedPotentialGPU", "MultipolePotentialGPU", "CylSplinePotentialGPU", "CompositePotentialGPU",
@@ -27,4 +28,5 @@ __all__ = [
     "DiskAnsatzPotentialGPU", "UniformAccelerationGPU", "MultipoleCoefs", "CylSplineCoefs",
     "read_coefs", "write_coefs", "set_default_precision", "prep_xyz", "G_AGAMA", "INV_4PIG",
     "Leapfrog", "leapfrog", "Stream", "particle_spray", "integrate_releases", "export_potential",
+    "DormandPrince", "integrate_adaptive",
 ]
