@@ -88,6 +88,29 @@ def main(out_path: Path) -> None:
             else:
                 nbetaq.append(Decimal(0))
 
+    # Two-step form for even-l (symmetric) walks: from Q_l = c Q_{l-1} + NB_l Q_{l-2}
+    # applied at l and l-1 and c Q_{l-3} = Q_{l-2} - NB_{l-2} Q_{l-4},
+    #   Q_l = (c^2 + SKIPA[m][l]) Q_{l-2} + SKIPB[m][l] Q_{l-4}
+    #   SKIPA = NB_l + NB_{l-1},  SKIPB = -NB_{l-1} NB_{l-2}
+    # (NB = NBETAQ, zero below l = m + 2, which makes the first step of every
+    # walk exact).  Stored for even l only, index m * 17 + l / 2, as (A, B) pairs.
+    def nb(m, l):
+        return nbetaq[m * (LMAX + 1) + l] if 0 <= l <= LMAX else Decimal(0)
+    skip = []
+    for m in range(LMAX + 1):
+        for j in range(LMAX // 2 + 1):
+            l = 2 * j
+            if l >= m + 2:
+                skip.append((nb(m, l) + nb(m, l - 1), -nb(m, l - 1) * nb(m, l - 2)))
+            else:
+                skip.append((Decimal(0), Decimal(0)))
+
+    def arr2(name, pairs, typ="double2", suffix=""):
+        items = [f"{{{float(a)!r}{suffix}, {float(b)!r}{suffix}}}" for a, b in pairs]
+        lines = [", ".join(items[i:i + 2]) for i in range(0, len(items), 2)]
+        return (f"__constant__ {typ} {name}[{len(pairs)}] = {{\n    " +
+                ",\n    ".join(lines) + "\n};\n")
+
     def arr(name, vals, typ="double", per_line=4):
         items = [f"{float(v)!r}" + ("f" if typ == "float" else "") for v in vals]
         lines = [", ".join(items[i:i + per_line]) for i in range(0, len(items), per_line)]
@@ -110,7 +133,10 @@ def main(out_path: Path) -> None:
            arr("AGB_ALPHA_F", alpha, "float"),
            arr("AGB_BETA_F", beta, "float"),
            arr("AGB_NBETAQ", nbetaq),
-           arr("AGB_NBETAQ_F", nbetaq, "float")]
+           arr("AGB_NBETAQ_F", nbetaq, "float"),
+           f"#define AGB_SKIP_N {LMAX // 2 + 1}",
+           arr2("AGB_SKIP", skip),
+           arr2("AGB_SKIP_F", skip, "float2", "f")]
     out_path.write_text("\n".join(src))
 
 

@@ -61,11 +61,13 @@ template <> struct MPConst<double> {
     static __device__ __forceinline__ double alpha(int i) { return AGB_ALPHA[i]; }
     static __device__ __forceinline__ double beta(int i) { return AGB_BETA[i]; }
     static __device__ __forceinline__ double nbetaq(int i) { return AGB_NBETAQ[i]; }
+    static __device__ __forceinline__ double2 skip(int i) { return AGB_SKIP[i]; }
 };
 template <> struct MPConst<float> {
     static __device__ __forceinline__ float alpha(int i) { return AGB_ALPHA_F[i]; }
     static __device__ __forceinline__ float beta(int i) { return AGB_BETA_F[i]; }
     static __device__ __forceinline__ float nbetaq(int i) { return AGB_NBETAQ_F[i]; }
+    static __device__ __forceinline__ float2 skip(int i) { return AGB_SKIP_F[i]; }
 };
 
 // Quintic coefficients of harmonic c in radial interval k.
@@ -327,6 +329,7 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
     dw[0] = R(0); dw[1] = R(1); dw[2] = R(2) * s; dw[3] = R(3) * sp[2]; dw[4] = R(4) * sp[3]; dw[5] = R(5) * sp[4];
     ew[0] = R(0); ew[1] = R(0); ew[2] = R(2); ew[3] = R(6) * s; ew[4] = R(12) * sp[2]; ew[5] = R(20) * sp[3];
     const R cth = (R)cth_d, sth = (R)sth_d;
+    const R c2 = (R)(cth_d * cth_d), w2 = (R)(-2.0 * cth_d * sth_d);   // two-step walk
     const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
     const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
     const R np1 = near_pole ? R(0) : R(1);
@@ -379,15 +382,40 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
             mp_col_acc<MODE, R>(gc, ac, sp, dw, ew, Pc, dPc, ll1);
             if (has_sin) mp_col_acc<MODE, R>(gs, as, sp, dw, ew, Pc, dPc, ll1);
         };
+        // even l only: Q_l = (cos^2 + A_l) Q_{l-2} + B_l Q_{l-4} (one step per stored l)
+        const int ts = m * AGB_SKIP_N;
+        auto skip2 = [&](int L) {
+            const auto ab = MPConst<R>::skip(ts + (L >> 1));
+            const R t = c2 + (R)ab.x;
+            const R Pn = fma(t, Pc, (R)ab.y * Pp);
+            if (NEED_ANG) {
+                const R dPn = fma(w2, Pc, fma(t, dPc, (R)ab.y * dPp));
+                dPp = dPc;
+                dPc = dPn;
+            }
+            Pp = Pc;
+            Pc = Pn;
+        };
+        const R seed = Pc;
         auto walk = [&](auto has_sin) {
             int l = m;
             while (l < l0) step(++l);
             acc(l, has_sin);
-            #pragma unroll 4
-            for (l = l0 + PAR; l <= lmax; l += PAR) {
-                if (PAR == 2) step(l - 1);
-                step(l);
-                acc(l, has_sin);
+            if (PAR == 2) {
+                // the two-step state (Q_l0, Q_l0-2): Q_0 for m = 0, zero otherwise
+                Pp = (m == 0) ? seed : R(0);
+                dPp = R(0);
+                #pragma unroll 4
+                for (l = l0 + 2; l <= lmax; l += 2) {
+                    skip2(l);
+                    acc(l, has_sin);
+                }
+            } else {
+                #pragma unroll 4
+                for (l = l0 + 1; l <= lmax; ++l) {
+                    step(l);
+                    acc(l, has_sin);
+                }
             }
         };
         if (m == 0) walk(std::false_type());
