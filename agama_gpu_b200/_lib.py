@@ -93,6 +93,11 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_eval_vjp_force.restype = ctypes.c_int
+    lib.agb_eval_vjp_force.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_table_vjp_workspace_bytes.restype = ctypes.c_size_t
     lib.agb_multipole_table_vjp_workspace_bytes.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_int64]
@@ -106,6 +111,11 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_multipole_adjoint_force.restype = ctypes.c_int
+    lib.agb_multipole_adjoint_force.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_eval_static.restype = ctypes.c_int
     lib.agb_eval_static.argtypes = lib.agb_eval.argtypes
     lib.agb_eval_workspace_bytes.restype = ctypes.c_size_t
@@ -146,6 +156,7 @@ lib = _load()
 EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
+    "agb_eval_vjp_force", "agb_multipole_adjoint_force",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
     "agb_multipole_adjoint", "agb_cylspline_table_vjp",
     "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",

@@ -79,9 +79,14 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 // workspace the kernel instead writes records in sorted order ("stage") and
 // unpermute_kernel gathers them back, reading one record per point and writing
 // every output array contiguously.
+// internal mode of agb_eval_vjp_force: the VJP plus the force of the same leaves
+// (written to the `hess` pointer as [N,3]) from the same per-point sums
+#define AGB_MODE_VJPF 5
+
 __host__ __device__ constexpr int stage_rec(int mode)
 {
-    return mode == AGB_MODE_HESS ? 10 : mode == AGB_MODE_GRAD ? 4 : mode == AGB_MODE_VJP ? 3 : 1;
+    return mode == AGB_MODE_HESS ? 10 : mode == AGB_MODE_GRAD ? 4 : mode == AGB_MODE_VJP ? 3
+         : mode == AGB_MODE_VJPF ? 6 : 1;
 }
 #define AGB_STAGE_MAX_REC 10
 
@@ -95,8 +100,11 @@ unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage,
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double* t = stage + (long long)REC * __ldg(dest + i);
         if (MODE == AGB_MODE_DENS) { rho[i] = t[0]; continue; }
-        if (MODE == AGB_MODE_VJP) {
+        if (MODE == AGB_MODE_VJP || MODE == AGB_MODE_VJPF) {
             grad[3 * i] = t[0]; grad[3 * i + 1] = t[1]; grad[3 * i + 2] = t[2];
+            if (MODE == AGB_MODE_VJPF) {
+                hess[3 * i] = t[3]; hess[3 * i + 1] = t[4]; hess[3 * i + 2] = t[5];
+            }
             continue;
         }
         if (phi) phi[i] = t[0];
@@ -113,11 +121,13 @@ unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage,
 // Hessian-carrying modes hold about twice the live state: one block per SM
 // with up to 255 registers beats two blocks with heavy spilling.
 template <int MODE, typename R>
-__global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP) ? 1 : 2)
+__global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP ||
+                                      MODE == AGB_MODE_VJPF) ? 1 : 2)
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
-    // the VJP mode evaluates every component with its Hessian and contracts at the end
-    constexpr int CM = (MODE == AGB_MODE_VJP) ? AGB_MODE_HESS : MODE;
+    // the VJP modes evaluate every component with its Hessian and contract at the end
+    constexpr bool VJP = MODE == AGB_MODE_VJP || MODE == AGB_MODE_VJPF;
+    constexpr int CM = VJP ? AGB_MODE_HESS : MODE;
     // a contiguous range of (interval-sorted) points per block: consecutive
     // iterations of a block reuse the same interval's table records from L1
     const long long lo = (long long)blockIdx.x * a.chunk;
@@ -143,7 +153,7 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             o.g[0] = o.g[1] = o.g[2] = 0.0;
             #pragma unroll
             for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
-            eval_component<CM, R, MODE == AGB_MODE_VJP>(c, lx, ly, lz, o);
+            eval_component<CM, R, VJP>(c, lx, ly, lz, o);
             const double A = lf.ampl;
             if (CM == AGB_MODE_DENS) {
                 rho += (A * lf.sigma * lf.sigma) * o.rho;
@@ -160,7 +170,7 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
                 }
             }
         }
-        if (MODE == AGB_MODE_VJP) {
+        if (VJP) {
             // L(Phi, F): dL/dx = gPhi grad(Phi) + (dF/dx)^T gF = gPhi grad(Phi) - H gF
             const double gp = a.gphi ? a.gphi[i] : 0.0;
             double f0 = 0.0, f1 = 0.0, f2 = 0.0;
@@ -168,6 +178,16 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             const double v0 = gp * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
             const double v1 = gp * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
             const double v2 = gp * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
+            if (MODE == AGB_MODE_VJPF) {
+                if (a.stage) {
+                    double* o = a.stage + 6 * pos;
+                    o[0] = v0; o[1] = v1; o[2] = v2; o[3] = -g0; o[4] = -g1; o[5] = -g2;
+                } else {
+                    a.grad[3 * i] = v0; a.grad[3 * i + 1] = v1; a.grad[3 * i + 2] = v2;
+                    a.hess[3 * i] = -g0; a.hess[3 * i + 1] = -g1; a.hess[3 * i + 2] = -g2;
+                }
+                continue;
+            }
             double* o = a.stage ? a.stage + 3 * pos : a.grad + 3 * i;
             o[0] = v0; o[1] = v1; o[2] = v2;
             continue;
@@ -261,6 +281,7 @@ static int launch_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
     case AGB_MODE_GRAD: launch_unpermute<AGB_MODE_GRAD>(a, st); break;
     case AGB_MODE_HESS: launch_unpermute<AGB_MODE_HESS>(a, st); break;
     case AGB_MODE_DENS: launch_unpermute<AGB_MODE_DENS>(a, st); break;
+    case AGB_MODE_VJPF: launch_unpermute<AGB_MODE_VJPF>(a, st); break;
     default:            launch_unpermute<AGB_MODE_VJP>(a, st); break;
     }
     return check_launch("unpermute_kernel");
@@ -275,6 +296,7 @@ static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t s
     case AGB_MODE_HESS: mixed ? launch_eval<AGB_MODE_HESS, float>(a, st) : launch_eval<AGB_MODE_HESS, double>(a, st); break;
     case AGB_MODE_DENS: mixed ? launch_eval<AGB_MODE_DENS, float>(a, st) : launch_eval<AGB_MODE_DENS, double>(a, st); break;
     case AGB_MODE_VJP:  mixed ? launch_eval<AGB_MODE_VJP, float>(a, st)  : launch_eval<AGB_MODE_VJP, double>(a, st); break;
+    case AGB_MODE_VJPF: mixed ? launch_eval<AGB_MODE_VJPF, float>(a, st) : launch_eval<AGB_MODE_VJPF, double>(a, st); break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
     return check_launch("agb_eval_kernel");
@@ -408,6 +430,9 @@ static int validate(const agb_component* comps, int n_comps, const agb_leaf* lea
     case AGB_MODE_HESS: if (!hess) return set_err(AGB_ERR_ARG, "agb_eval: hess is null"); break;
     case AGB_MODE_DENS: if (!rho) return set_err(AGB_ERR_ARG, "agb_eval: rho is null"); break;
     case AGB_MODE_VJP:  if (!grad) return set_err(AGB_ERR_ARG, "agb_eval_vjp: g_xyz is null"); break;
+    case AGB_MODE_VJPF:
+        if (!grad || !hess) return set_err(AGB_ERR_ARG, "agb_eval_vjp_force: g_xyz or force is null");
+        break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
     return AGB_OK;
@@ -557,6 +582,22 @@ extern "C" int agb_eval_vjp(const agb_component* comps, int n_comps, const agb_l
     return rc;
 }
 
+extern "C" int agb_eval_vjp_force(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                                  int n_leaves, const double* xyz, int64_t n, int precision,
+                                  const double* g_phi, const double* g_force, double* g_xyz,
+                                  double* force, void* workspace, size_t workspace_bytes,
+                                  void* stream)
+{
+    g_vjp_phi = g_phi;
+    g_vjp_force = g_force;
+    const int rc = eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, AGB_MODE_VJPF, precision,
+                             nullptr, g_xyz, force, nullptr, 0, workspace, workspace_bytes,
+                             workspace == nullptr, stream);
+    g_vjp_phi = nullptr;
+    g_vjp_force = nullptr;
+    return rc;
+}
+
 extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                            int n_leaves, const double* xyz, int64_t n, int mode, int precision,
                            double* phi, double* grad, double* hess, double* rho, int out_flags,
@@ -629,11 +670,11 @@ extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf
 // ---------------------------------------------------------------------------
 // fused adjoint of one Multipole leaf (position VJP + coefficient gradient)
 // ---------------------------------------------------------------------------
-extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
-                                     const double* xyz, int64_t n, int precision,
-                                     const double* g_phi, const double* g_force, double* g_xyz,
-                                     double* g_table, void* workspace, size_t workspace_bytes,
-                                     void* stream)
+static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* leaf,
+                                  const double* xyz, int64_t n, int precision,
+                                  const double* g_phi, const double* g_force, double* g_xyz,
+                                  double* force, double* g_table, void* workspace,
+                                  size_t workspace_bytes, void* stream)
 {
     if (!comp || !leaf || !g_table || !g_xyz)
         return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: null argument");
@@ -653,7 +694,7 @@ extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* 
     g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
     g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
     g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force;
-    g.gx = g_xyz; g.grad = g_table;
+    g.gx = g_xyz; g.grad = g_table; g.force = force;
     cudaStream_t st = (cudaStream_t)stream;
     agb_leaf l = *leaf;
     l.comp = 0;
@@ -706,6 +747,27 @@ extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* 
     }
     if (need && own) cudaFreeAsync(ws, st);
     return rc;
+}
+
+extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
+                                     const double* xyz, int64_t n, int precision,
+                                     const double* g_phi, const double* g_force, double* g_xyz,
+                                     double* g_table, void* workspace, size_t workspace_bytes,
+                                     void* stream)
+{
+    return multipole_adjoint_impl(comp, leaf, xyz, n, precision, g_phi, g_force, g_xyz, nullptr,
+                                  g_table, workspace, workspace_bytes, stream);
+}
+
+extern "C" int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
+                                           const double* xyz, int64_t n, int precision,
+                                           const double* g_phi, const double* g_force,
+                                           double* g_xyz, double* force, double* g_table,
+                                           void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (!force) return set_err(AGB_ERR_ARG, "agb_multipole_adjoint_force: force is null");
+    return multipole_adjoint_impl(comp, leaf, xyz, n, precision, g_phi, g_force, g_xyz, force,
+                                  g_table, workspace, workspace_bytes, stream);
 }
 
 extern "C" int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf* leaf,

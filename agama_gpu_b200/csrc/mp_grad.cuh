@@ -322,6 +322,7 @@ struct MPAdjArgs {
     long long chunk;          // points per warp (multiple of 32)
     int warp_smem;            // bytes of dynamic shared memory per warp
     int staged;               // 1: interval sums staged in shared memory
+    double* force;            // [N,3] or null: this leaf's force added (+=)
     DevComp c;
     DevLeaf leaf;
 };
@@ -334,8 +335,29 @@ struct MPAdjArgs {
 // contracts it with the points' powers of s (broadcast reads), 10 FMAs per
 // point, then adds its 6 sums to the interval's accumulator.
 template <typename R> struct AdjVec;
-template <> struct AdjVec<float> { typedef float2 T2; };
-template <> struct AdjVec<double> { typedef double2 T2; };
+template <> struct AdjVec<float> {
+    typedef float2 T2;
+    // a point's 9 weights (s..s^5, 2s, 3s^2, 4s^3, 5s^4) from its 16-byte aligned row
+    static __device__ __forceinline__ void weights(const float* w, float o[9])
+    {
+        const float4 a = *reinterpret_cast<const float4*>(w);
+        const float4 b = *reinterpret_cast<const float4*>(w + 4);
+        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+        o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w; o[8] = w[8];
+    }
+};
+template <> struct AdjVec<double> {
+    typedef double2 T2;
+    static __device__ __forceinline__ void weights(const double* w, double o[9])
+    {
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double2 v = *reinterpret_cast<const double2*>(w + 2 * j);
+            o[2 * j] = v.x; o[2 * j + 1] = v.y;
+        }
+        o[8] = w[8];
+    }
+};
 
 #define AGB_ADJ_TILE_STRIDE 33          // tile row length (columns + 1: no bank conflicts)
 #define AGB_ADJ_SPW 12                  // per-point powers: s..s^5, 2s, 3s^2, 4s^3, 5s^4, pad
@@ -365,7 +387,8 @@ __device__ __forceinline__ void adj_contract(AdjTile<R>& T, int lane)
         #pragma unroll 4
         for (int p = 0; p < 32; ++p) {
             const typename AdjVec<R>::T2 uv = T.uv[p * AGB_ADJ_TILE_STRIDE + lane];
-            const R* w = T.spw + p * AGB_ADJ_SPW;
+            R w[9];
+            AdjVec<R>::weights(T.spw + p * AGB_ADJ_SPW, w);
             g0 += uv.x;
             g1 = fma(w[0], uv.x, g1 + uv.y);
             g2 = fma(w[1], uv.x, fma(w[5], uv.y, g2));
@@ -418,6 +441,7 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
     dw[0] = R(0); dw[1] = R(1); dw[2] = R(2) * s; dw[3] = R(3) * sp[2]; dw[4] = R(4) * sp[3]; dw[5] = R(5) * sp[4];
     ew[0] = R(0); ew[1] = R(0); ew[2] = R(2); ew[3] = R(6) * s; ew[4] = R(12) * sp[2]; ew[5] = R(20) * sp[3];
     const R cth = (R)cth_d, sth = (R)sth_d;
+    const R c2 = (R)(cth_d * cth_d), w2 = (R)(-2.0 * cth_d * sth_d);   // two-step walk
     const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
     const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
     const R np1 = near_pole ? R(0) : R(1);
@@ -475,13 +499,29 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
             }
             rec += (m > 0 ? 2 : 1) * MPPtr<R>::REC;
         };
+        const R seed = Pc;
         int l = m;
         while (l < l0) step(++l);
         acc(l);
-        for (l = l0 + PAR; l <= c.lmax; l += PAR) {
-            if (PAR == 2) step(l - 1);
-            step(l);
-            acc(l);
+        if (PAR == 2) {
+            // even l: Q_l = (cos^2 + A_l) Q_{l-2} + B_l Q_{l-4} (multipole.cuh)
+            const int ts = m * AGB_SKIP_N;
+            Pp = (m == 0) ? seed : R(0);
+            dPp = R(0);
+            #pragma unroll 2
+            for (l = l0 + 2; l <= c.lmax; l += 2) {
+                const auto ab = MPConst<R>::skip(ts + (l >> 1));
+                const R t = c2 + (R)ab.x;
+                const R Pn = fma(t, Pc, (R)ab.y * Pp);
+                const R dPn = fma(w2, Pc, fma(t, dPc, (R)ab.y * dPp));
+                dPp = dPc; dPc = dPn; Pp = Pc; Pc = Pn;
+                acc(l);
+            }
+        } else {
+            for (l = l0 + 1; l <= c.lmax; ++l) {
+                step(l);
+                acc(l);
+            }
         }
         mp_col_finish<MODE, R>(gc, inv_sth, q1, np1, cot, m2);
         mp_col_finish<MODE, R>(gs, inv_sth, q1, np1, cot, m2);
@@ -672,6 +712,11 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
         a.gx[3 * i]     += As * (gp * o.g[0] - s2 * (h[0] * gf0 + h[3] * gf1 + h[5] * gf2));
         a.gx[3 * i + 1] += As * (gp * o.g[1] - s2 * (h[3] * gf0 + h[1] * gf1 + h[4] * gf2));
         a.gx[3 * i + 2] += As * (gp * o.g[2] - s2 * (h[5] * gf0 + h[4] * gf1 + h[2] * gf2));
+        if (a.force) {
+            a.force[3 * i] -= As * o.g[0];
+            a.force[3 * i + 1] -= As * o.g[1];
+            a.force[3 * i + 2] -= As * o.g[2];
+        }
     }
     if (swarp) flush();
 }

@@ -280,7 +280,8 @@ class Leapfrog:
 
     # -- adjoint -----------------------------------------------------------------------
     def adjoint(self, ckpts: List, n_steps: int, lam_x: torch.Tensor,
-                lam_v: torch.Tensor, table_grads: bool = False, group=None):
+                lam_v: torch.Tensor, table_grads: bool = False, group=None,
+                reconstruct: str = "recompute"):
         """(dL/dx0, dL/dv0) from (dL/dx_T, dL/dv_T) and the forward's checkpoints.
 
         With table_grads=True also returns {component: gradient}: for each Multipole
@@ -295,7 +296,19 @@ class Leapfrog:
             lv += dt_g lx;          pending = h_g lv
         where pending is the cotangent of F(x_{g+1}) from the first half-kick of
         substep g + 1, and at the end dL/dx0 += (dF/dx)^T pending at x_0.
+
+        Positions between checkpoints (k >= 2): reconstruct="recompute" integrates
+        each segment forwards again from its first checkpoint (one extra force per
+        substep, bit-identical positions); reconstruct="reverse" steps backwards
+        from the segment's last checkpoint (x, v) with the time-reversed substep,
+        taking F(x_{g+1}) from the VJP launch at x_{g+1} itself (the adjoint
+        kernels output the force they form anyway), so no force is evaluated
+        twice.  Leapfrog is time-reversible: the reversed positions differ from
+        the forward's by rounding only (amplified over at most k steps, and reset
+        at every checkpoint).
         """
+        if reconstruct not in ("recompute", "reverse"):
+            raise ValueError("reconstruct must be 'recompute' or 'reverse'")
         tg = {} if table_grads else None
         S = self.S
         G = int(n_steps) * S
@@ -307,15 +320,43 @@ class Leapfrog:
         starts = sorted(c[0] for c in ckpts if c[0] < G)
         bounds = starts + [G]
 
-        def vjp(xg, t, g_force):
+        def vjp(xg, t, g_force, force=None):
+            kw = {} if force is None else {"force_out": force}
             if tg is None:
-                self.pot._vjp(xg, t, None, g_force, precision=self.precision, out=gx)
+                self.pot._vjp(xg, t, None, g_force, precision=self.precision, out=gx, **kw)
             else:
-                self.pot._adjoint_vjp(xg, t, None, g_force, tg, precision=self.precision, out=gx)
+                self.pot._adjoint_vjp(xg, t, None, g_force, tg, precision=self.precision, out=gx,
+                                      **kw)
 
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
             _, xs, vs = at[s]
+            if reconstruct == "reverse" and e in at and at[e][2] is not None and e - 1 > s:
+                # backwards from (x_e, v_e): v_h(g) = v_{g+1} - h_g F(x_{g+1}),
+                # x_g = x_{g+1} - dt_g v_h(g), and v_{g+1} = v_h(g+1) - h_{g+1} F(x_{g+1})
+                xc = at[e][1].clone()
+                vh = None
+                Fg = torch.empty_like(xc)
+                h_next = 0.0
+                for g in range(e - 1, s - 1, -1):
+                    dtg, hg, _ = self._sub[g % S]
+                    gF = lv * hg
+                    if pending is not None:
+                        gF.add_(pending)
+                    need = g > s
+                    vjp(xc, self._t(g + 1), gF, Fg if need else None)
+                    lx.add_(gx)
+                    lv.add_(lx, alpha=dtg)
+                    pending = lv * hg
+                    if need:
+                        if vh is None:
+                            vh = at[e][2].clone()
+                            vh.sub_(Fg, alpha=hg)
+                        else:
+                            vh.sub_(Fg, alpha=h_next + hg)
+                        xc.sub_(vh, alpha=dtg)
+                        h_next = hg
+                continue
             # the segment's positions: x_s and x_e from checkpoints, the others re-computed
             pos = {s: xs}
             if e in at:

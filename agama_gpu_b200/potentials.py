@@ -215,8 +215,10 @@ class _GPUPotBase:
 
     def _vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
              g_force: Optional[torch.Tensor], precision: Optional[str] = None,
-             out: Optional[torch.Tensor] = None, leaves=None) -> torch.Tensor:
-        """dL/dx = g_phi * grad(Phi) - H g_force for cotangents of (Phi, force)."""
+             out: Optional[torch.Tensor] = None, leaves=None,
+             force_out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """dL/dx = g_phi * grad(Phi) - H g_force for cotangents of (Phi, force).
+        force_out [N,3]: also receives the force of the same leaves (assigned)."""
         n = arr.shape[0]
         dev = arr.device
         prec = _PRECISIONS[precision or self.precision or _default_precision]
@@ -228,19 +230,27 @@ class _GPUPotBase:
         gf = None if g_force is None else g_force.to(device=dev, dtype=torch.float64).contiguous()
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         ws, nws = self._workspace(cargs, n, dev, 0)       # agb_eval_vjp sorts by default
-        rc = _lib.lib.agb_eval_vjp(*cargs, arr.data_ptr(), n, prec, ptr(gp), ptr(gf), gx.data_ptr(),
-                                   ptr(ws), nws,
-                                   ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
-        _lib.check(rc, "agb_eval_vjp")
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        if force_out is None:
+            rc = _lib.lib.agb_eval_vjp(*cargs, arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
+                                       gx.data_ptr(), ptr(ws), nws, stream)
+            _lib.check(rc, "agb_eval_vjp")
+        else:
+            rc = _lib.lib.agb_eval_vjp_force(*cargs, arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
+                                             gx.data_ptr(), force_out.data_ptr(), ptr(ws), nws,
+                                             stream)
+            _lib.check(rc, "agb_eval_vjp_force")
         return gx
 
     def _adjoint_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
                      g_force: Optional[torch.Tensor], acc_dev: dict,
-                     precision: Optional[str] = None, out: Optional[torch.Tensor] = None):
+                     precision: Optional[str] = None, out: Optional[torch.Tensor] = None,
+                     force_out: Optional[torch.Tensor] = None):
         """Position VJP of the tree and, fused into the same walk, the coefficient
         gradients of its (regular-layout) Multipoles, accumulated into ``acc_dev``
         as device-layout buffers {component: (n_int, n_cols, 6)}; convert them with
-        ``_table_grads_from_device``.  Other Multipoles use the separate passes."""
+        ``_table_grads_from_device``.  Other Multipoles use the separate passes.
+        force_out [N,3]: also receives the tree's force at arr (assigned)."""
         n = arr.shape[0]
         dev = arr.device
         prec = _PRECISIONS[precision or self.precision or _default_precision]
@@ -250,7 +260,8 @@ class _GPUPotBase:
         rest = [lf for lf in leaves if not any(lf is f for f in fused)]
         gx = out if out is not None else torch.empty((n, 3), dtype=torch.float64, device=dev)
         if rest:
-            self._vjp(arr, t, g_phi, g_force, precision=precision, out=gx, leaves=rest)
+            self._vjp(arr, t, g_phi, g_force, precision=precision, out=gx, leaves=rest,
+                      force_out=force_out)
             for comp, sigma, gamma, ampl in rest:
                 if comp.kind in (_lib.KIND_MULTIPOLE, _lib.KIND_CYLSPLINE):
                     g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
@@ -261,6 +272,8 @@ class _GPUPotBase:
                         acc_dev[key] = g
         else:
             gx.zero_()
+            if force_out is not None:
+                force_out.zero_()
         if n == 0:
             return gx
         gp = None if g_phi is None else g_phi.to(device=dev, dtype=torch.float64).contiguous()
@@ -280,10 +293,18 @@ class _GPUPotBase:
             nws = int(_lib.lib.agb_multipole_table_vjp_workspace_bytes(ctypes.byref(c),
                                                                        ctypes.byref(lf), n))
             ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
-            rc = _lib.lib.agb_multipole_adjoint(ctypes.byref(c), ctypes.byref(lf), arr.data_ptr(),
-                                                n, prec, ptr(gp), ptr(gf), gx.data_ptr(),
-                                                buf.data_ptr(), ptr(ws), nws, stream)
-            _lib.check(rc, "agb_multipole_adjoint")
+            if force_out is None:
+                rc = _lib.lib.agb_multipole_adjoint(ctypes.byref(c), ctypes.byref(lf),
+                                                    arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
+                                                    gx.data_ptr(), buf.data_ptr(), ptr(ws), nws,
+                                                    stream)
+                _lib.check(rc, "agb_multipole_adjoint")
+            else:
+                rc = _lib.lib.agb_multipole_adjoint_force(ctypes.byref(c), ctypes.byref(lf),
+                                                          arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
+                                                          gx.data_ptr(), force_out.data_ptr(),
+                                                          buf.data_ptr(), ptr(ws), nws, stream)
+                _lib.check(rc, "agb_multipole_adjoint_force")
         return gx
 
     @staticmethod

@@ -164,7 +164,7 @@ def run_reference(args):
 
 
 def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision: str,
-                  checkpoint_every=None):
+                  checkpoint_every=None, reconstruct="recompute"):
     """Adjoint / forward time of the stream workload (1024 clouds x 2048 particles, 2000
     steps by default): Gaussian clouds (0.1 kpc, 1 km/s)
     on circular orbits at 10-60 kpc in an lmax=16 x 64-node Multipole + Miyamoto-Nagai,
@@ -195,8 +195,9 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
     # warm-up: graph capture, every kernel of the adjoint, and the allocator's blocks
     nw = 2 * integ.graph_steps
     xw, vw, ck = integ.run(x0t, v0t, nw, checkpoint_every)
-    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw), table_grads=True)
-    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw))
+    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw), table_grads=True,
+                  reconstruct=reconstruct)
+    integ.adjoint(ck, nw, 2 * (xw - target), torch.zeros_like(vw), reconstruct=reconstruct)
     mp.node_gradients(mp.table_vjp(x0t[:1024], 0.0, None, torch.ones_like(x0t[:1024])))
     del ck
     xw, vw, ck = integ.run(x0t, v0t, n_steps, checkpoint_every)
@@ -207,10 +208,11 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
     xT, vT, ck = integ.run(x0t, v0t, n_steps, checkpoint_every)
     e1.record()
     lx, lv, tg = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT),
-                               table_grads=True)
+                               table_grads=True, reconstruct=reconstruct)
     gnodes = mp.node_gradients(tg[mp])
     e2.record()
-    lx2, _ = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT))
+    lx2, _ = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT),
+                           reconstruct=reconstruct)
     e3.record()
     torch.cuda.synchronize()
     del ck
@@ -221,7 +223,7 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
             "adjoint_phase_space_only_ms": adj_x, "ratio_phase_space_only": adj_x / fwd,
             "steps": n_steps,
             "particles": n_streams * per_stream, "checkpoint_every": checkpoint_every,
-            "precision": precision, "finite": ok,
+            "precision": precision, "finite": ok, "reconstruct": reconstruct,
             "backward_returns": "dL/dx0, dL/dv0, dL/dPhi_nodes, dL/d(dPhi/dr)_nodes (17^2 x 64)"}
 
 
@@ -515,6 +517,14 @@ def main():
         adj["recompute_k64"] = {q: r64[q] for q in ("forward_ms", "adjoint_ms", "ratio",
                                                     "adjoint_phase_space_only_ms",
                                                     "ratio_phase_space_only")}
+        torch.cuda.empty_cache()
+        # the configured interval (k = 64) with the segments stepped backwards from
+        # their later checkpoint: no force is evaluated twice
+        rr = adjoint_ratio(dev, args.adj_clouds, 2048, args.adj_steps, "mixed",
+                           checkpoint_every=64, reconstruct="reverse")
+        adj["reverse_k64"] = {q: max_over_ranks(rr[q]) if q == "ratio" else rr[q]
+                              for q in ("forward_ms", "adjoint_ms", "ratio",
+                                        "adjoint_phase_space_only_ms", "ratio_phase_space_only")}
 
     cyl = cylspline_leg(dev, 1_000_000, max(3, args.steps), 3)
     batched = None

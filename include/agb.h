@@ -222,6 +222,20 @@ int agb_eval_vjp(const agb_component* comps, int n_comps,
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * agb_eval_vjp that also writes the force of the same leaves, F = -grad Phi,
+ * into force [N,3] (assigned), from the per-point sums the VJP forms anyway.
+ * A reverse-time adjoint uses it to step the trajectory backwards from a
+ * checkpoint without a separate force evaluation.  No counterpart in the
+ * reference.
+ */
+int agb_eval_vjp_force(const agb_component* comps, int n_comps,
+                       const agb_leaf* leaves, int n_leaves,
+                       const double* xyz, int64_t n, int precision,
+                       const double* g_phi, const double* g_force, double* g_xyz,
+                       double* force, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/*
  * Gradient of a loss with respect to one Multipole leaf's quintic coefficients
  * (the table half of the backward): accumulates into g_table, laid out like the
  * component's interval-major FP64 table [n_int][n_lm][6], the sum over points
@@ -254,6 +268,17 @@ int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
                           const double* g_phi, const double* g_force, double* g_xyz,
                           double* g_table, void* workspace, size_t workspace_bytes,
                           void* stream);
+
+/*
+ * agb_multipole_adjoint that also ADDS this leaf's force, -A sigma grad Phi,
+ * into force [N,3] (for the reverse-time adjoint, as agb_eval_vjp_force).
+ * No counterpart in the reference.
+ */
+int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
+                                const double* xyz, int64_t n, int precision,
+                                const double* g_phi, const double* g_force,
+                                double* g_xyz, double* force, double* g_table,
+                                void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Gradient of a loss with respect to one CylSpline leaf's node table: adds into

@@ -531,3 +531,45 @@ def test_yoshida4_order_in_composite():
             e.append(float((xT - ref).abs().max()))
         rate = math.log2(e[0] / e[1])
         assert abs(rate - order) < 0.4, (scheme, e, rate)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 2e-6)])
+def test_vjp_force_output(prec, tol):
+    """The VJP launches' force output (agb_eval_vjp_force, agb_multipole_adjoint_force)
+    equals the force of the same tree."""
+    import torch
+    pot = _composite(static=False)
+    x = torch.from_numpy(_pts(3000, 31)).cuda()
+    gf = torch.from_numpy(np.random.default_rng(3).normal(size=(3000, 3))).cuda()
+    F = pot._launch(x, 0.4, 1, False, precision="fp64")[1]
+    scale = float(F.abs().max())
+    f1 = torch.full_like(x, np.nan)
+    g1 = pot._vjp(x, 0.4, None, gf, precision=prec, force_out=f1)
+    assert float((f1 - F).abs().max()) <= tol * scale
+    assert torch.equal(g1, pot._vjp(x, 0.4, None, gf, precision=prec))
+    f2 = torch.full_like(x, np.nan)
+    tg = {}
+    g2 = pot._adjoint_vjp(x, 0.4, None, gf, tg, precision=prec, force_out=f2)
+    assert float((f2 - F).abs().max()) <= tol * scale
+    g3 = pot._adjoint_vjp(x, 0.4, None, gf, {}, precision=prec)
+    assert torch.equal(g2, g3)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+@pytest.mark.parametrize("static", [True, False])
+def test_reverse_reconstruction_matches_recompute(static, prec, tol):
+    """Segments stepped backwards from their later checkpoint give the gradients of the
+    forward re-computation (rounding of the reversed positions only)."""
+    import torch
+    from agama_gpu_b200.integrate import Leapfrog, gyr_to_time
+    pot = _composite(static=static)
+    x0, v0 = _disk_ics(2000, 41)
+    target = x0 + 0.5
+    integ = Leapfrog(pot, gyr_to_time(1e-3), t0=0.1, precision=prec)
+    xT, vT, ck = integ.run(x0, v0, 96, checkpoint_every=32)
+    a = integ.adjoint(ck, 96, 2 * (xT - target), 0.1 * vT, table_grads=True)
+    b = integ.adjoint(ck, 96, 2 * (xT - target), 0.1 * vT, table_grads=True, reconstruct="reverse")
+    for u, w in zip(a[:2], b[:2]):
+        assert float((u - w).abs().max()) <= tol * float(u.abs().max())
+    for comp in a[2]:
+        assert float((a[2][comp] - b[2][comp]).abs().max()) <= tol * float(a[2][comp].abs().max())
