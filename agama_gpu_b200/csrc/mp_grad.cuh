@@ -410,12 +410,29 @@ __device__ __forceinline__ void adj_contract(AdjTile<R>& T, int lane)
     T.nb = 0;
 }
 
-// one column's (U, V) of this lane's point
-template <typename R>
+// one column's (U, V) of this lane's point.  EMIT: 0 decides per column (tile
+// when the warp shares one interval, else atomics), 1 writes the tile without a
+// flush check (the caller flushes per |m| group), 2 always uses atomics.
+template <typename R, int EMIT = 0>
 __device__ __forceinline__ void adj_put(AdjTile<R>& T, double* __restrict__ gk, int col,
                                         const R sp[6], const R dw[6], R U, R V, int lane,
                                         bool active)
 {
+    if (EMIT == 1) {
+        typename AdjVec<R>::T2 uv;
+        uv.x = U;
+        uv.y = V;
+        T.uv[lane * AGB_ADJ_TILE_STRIDE + T.nb] = uv;
+        ++T.nb;
+        return;
+    }
+    if (EMIT == 2) {
+        if (active && gk) {
+            #pragma unroll
+            for (int j = 0; j < 6; ++j) atomicAdd(gk + (long long)col * 6 + j, (double)fma(sp[j], U, dw[j] * V));
+        }
+        return;
+    }
     if (T.on) {
         typename AdjVec<R>::T2 uv;
         uv.x = U;
@@ -428,7 +445,7 @@ __device__ __forceinline__ void adj_put(AdjTile<R>& T, double* __restrict__ gk, 
     }
 }
 
-template <typename R, int PAR>
+template <typename R, int PAR, int EMIT>
 __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, double cth_d,
                                             double sth_d, double cph, double sph, R P1, R P2,
                                             R P3, R P4, double* gbase, AdjTile<R>& T, int lane,
@@ -459,6 +476,12 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
         int l0 = (PAR == 2) ? (m + (m & 1)) : m;
         if (m == 0) l0 = PAR;
         if (l0 > c.lmax) continue;
+        if (EMIT == 1) {
+            // even l, lmax <= 32: a group holds at most 32 columns; flush before it
+            // when it would not fit, so the loop below never branches to flush
+            const int ncols = (m == 0 ? 1 : 2) * ((c.lmax - l0) / PAR + 1);
+            if (T.nb + ncols > 32) adj_contract(T, lane);
+        }
         const R q1 = (near_pole && m == 1) ? R(1) : R(0);
         const R m2 = R(m * m) * inv_sth * inv_sth;
         const R Tc = (R)cm, Ts = (R)sm, dTc = -R(m) * Ts, dTs = R(m) * Tc;
@@ -490,11 +513,12 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
             if (F32 && m > 0) MPPtr<R>::load_cs(rec, a, b);
             else MPPtr<R>::load(rec, a);
             mp_col_acc<MODE, R>(gc, a, sp, dw, ew, Pc, dPc, ll1);
-            adj_put<R>(T, gbase, col++, sp, dw, fma(Tc, base, dTc * Pq), P2 * Pc * Tc, lane, active);
+            adj_put<R, EMIT>(T, gbase, col++, sp, dw, fma(Tc, base, dTc * Pq), P2 * Pc * Tc, lane,
+                             active);
             if (m > 0) {
                 if (!F32) MPPtr<R>::load(rec + MPPtr<R>::REC, b);
                 mp_col_acc<MODE, R>(gs, b, sp, dw, ew, Pc, dPc, ll1);
-                adj_put<R>(T, gbase, col++, sp, dw, fma(Ts, base, dTs * Pq), P2 * Pc * Ts, lane,
+                adj_put<R, EMIT>(T, gbase, col++, sp, dw, fma(Ts, base, dTs * Pq), P2 * Pc * Ts, lane,
                            active);
             }
             rec += (m > 0 ? 2 : 1) * MPPtr<R>::REC;
@@ -672,10 +696,18 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
             w[5] = R(2) * sr; w[6] = R(3) * s2; w[7] = R(4) * s3; w[8] = R(5) * s4;
         }
         MPSums t = {};
-        if (c.structure == AGB_STRUCT_EVEN)
-            mp_adj_walk<R, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
-        else
-            mp_adj_walk<R, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+        // warp-uniform choice: tile emission (all 32 points in one interval) or atomics
+        if (c.structure == AGB_STRUCT_EVEN) {
+            if (T.on)
+                mp_adj_walk<R, 2, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+            else
+                mp_adj_walk<R, 2, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+        } else {
+            if (T.on)
+                mp_adj_walk<R, 1, 0>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+            else
+                mp_adj_walk<R, 1, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+        }
         // monopole column of the coefficient gradient
         {
             const double Bp = t.B * inv_dlogr;
