@@ -53,13 +53,15 @@ static int check_launch(const char* what)
 // ---------------------------------------------------------------------------
 // the fused kernel
 // ---------------------------------------------------------------------------
-template <int MODE, typename R, bool EXACT>
+// AN: the tree holds analytic leaves only (no expansion code compiled in: a
+// small register footprint and more resident blocks for the Hessian modes)
+template <int MODE, typename R, bool EXACT, bool AN = false>
 __device__ __forceinline__ void eval_component(const DevComp& c, double x, double y, double z,
                                                PointOut& o)
 {
     switch (c.kind) {
-    case AGB_KIND_MULTIPOLE:     multipole_point<MODE, R>(c, x, y, z, o); break;
-    case AGB_KIND_CYLSPLINE:     cylspline_point<MODE, EXACT, R>(c, x, y, z, o); break;
+    case AGB_KIND_MULTIPOLE:     if (!AN) multipole_point<MODE, R>(c, x, y, z, o); break;
+    case AGB_KIND_CYLSPLINE:     if (!AN) cylspline_point<MODE, EXACT, R>(c, x, y, z, o); break;
     case AGB_KIND_NFW:           nfw_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_PLUMMER:       plummer_point<MODE>(c.p, x, y, z, o); break;
     case AGB_KIND_HERNQUIST:     hernquist_point<MODE>(c.p, x, y, z, o); break;
@@ -120,9 +122,9 @@ unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage,
 
 // Hessian-carrying modes hold about twice the live state: one block per SM
 // with up to 255 registers beats two blocks with heavy spilling.
-template <int MODE, typename R>
-__global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP ||
-                                      MODE == AGB_MODE_VJPF) ? 1 : 2)
+template <int MODE, typename R, bool AN = false>
+__global__ void __launch_bounds__(256, ((MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP ||
+                                       MODE == AGB_MODE_VJPF) && !AN) ? 1 : 2)
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
     // the VJP modes evaluate every component with its Hessian and contract at the end
@@ -153,7 +155,7 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             o.g[0] = o.g[1] = o.g[2] = 0.0;
             #pragma unroll
             for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
-            eval_component<CM, R, VJP>(c, lx, ly, lz, o);
+            eval_component<CM, R, VJP, AN>(c, lx, ly, lz, o);
             const double A = lf.ampl;
             if (CM == AGB_MODE_DENS) {
                 rho += (A * lf.sigma * lf.sigma) * o.rho;
@@ -243,13 +245,13 @@ static int grid_for(long long n)
 #define AGB_EVAL_WAVES 4      // blocks per resident slot: balances the cost spread along r
 #endif
 
-template <int MODE, typename R>
+template <int MODE, typename R, bool AN = false>
 static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
     static int per_sm = 0;    // resident blocks per SM of this instantiation
     if (per_sm == 0) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_eval_kernel<MODE, R>, 256, 0)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_eval_kernel<MODE, R, AN>, 256, 0)
             != cudaSuccess || b < 1)
             b = 1;
         per_sm = b;
@@ -260,7 +262,16 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
     const long long slots = (long long)g_num_sms * per_sm * (w ? w : AGB_EVAL_WAVES);
     const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
     a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
-    agb_eval_kernel<MODE, R><<<(int)grid, 256, 0, st>>>(a);
+    agb_eval_kernel<MODE, R, AN><<<(int)grid, 256, 0, st>>>(a);
+}
+
+static bool analytic_only(const EvalArgs& a)
+{
+    for (int L = 0; L < a.n_leaves; ++L) {
+        const int k = a.comps[a.leaves[L].comp].kind;
+        if (k == AGB_KIND_MULTIPOLE || k == AGB_KIND_CYLSPLINE) return false;
+    }
+    return true;
 }
 
 static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t st);
@@ -295,8 +306,15 @@ static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t s
     case AGB_MODE_GRAD: mixed ? launch_eval<AGB_MODE_GRAD, float>(a, st) : launch_eval<AGB_MODE_GRAD, double>(a, st); break;
     case AGB_MODE_HESS: mixed ? launch_eval<AGB_MODE_HESS, float>(a, st) : launch_eval<AGB_MODE_HESS, double>(a, st); break;
     case AGB_MODE_DENS: mixed ? launch_eval<AGB_MODE_DENS, float>(a, st) : launch_eval<AGB_MODE_DENS, double>(a, st); break;
-    case AGB_MODE_VJP:  mixed ? launch_eval<AGB_MODE_VJP, float>(a, st)  : launch_eval<AGB_MODE_VJP, double>(a, st); break;
-    case AGB_MODE_VJPF: mixed ? launch_eval<AGB_MODE_VJPF, float>(a, st) : launch_eval<AGB_MODE_VJPF, double>(a, st); break;
+    // analytic leaves compute in FP64 in both precisions: one lean instantiation
+    case AGB_MODE_VJP:
+        if (analytic_only(a)) launch_eval<AGB_MODE_VJP, double, true>(a, st);
+        else mixed ? launch_eval<AGB_MODE_VJP, float>(a, st) : launch_eval<AGB_MODE_VJP, double>(a, st);
+        break;
+    case AGB_MODE_VJPF:
+        if (analytic_only(a)) launch_eval<AGB_MODE_VJPF, double, true>(a, st);
+        else mixed ? launch_eval<AGB_MODE_VJPF, float>(a, st) : launch_eval<AGB_MODE_VJPF, double>(a, st);
+        break;
     default: return set_err(AGB_ERR_ARG, "agb_eval: unknown mode %d", mode);
     }
     return check_launch("agb_eval_kernel");

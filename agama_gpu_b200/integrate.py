@@ -292,10 +292,9 @@ class Leapfrog:
         potential) the table gradients are summed over the ranks of ``group``.
 
         Per substep g (backwards; dt_g, h_g its drift and half-kick):
-            gF = h_g lv + pending;  lx += (dF/dx)^T gF at x_{g+1};
-            lv += dt_g lx;          pending = h_g lv
-        where pending is the cotangent of F(x_{g+1}) from the first half-kick of
-        substep g + 1, and at the end dL/dx0 += (dF/dx)^T pending at x_0.
+            lx += (dF/dx)^T gF at x_{g+1};  lv += dt_g lx;  gF = (h_g + h_{g-1}) lv
+        where gF is the cotangent of F(x_g): the second half-kick of substep g - 1
+        and the first of substep g both use it (h_0 lv for x_0, taken at the end).
 
         Positions between checkpoints (k >= 2): reconstruct="recompute" integrates
         each segment forwards again from its first checkpoint (one extra force per
@@ -314,11 +313,13 @@ class Leapfrog:
         G = int(n_steps) * S
         lx = lam_x.detach().to(torch.float64).contiguous().clone()
         lv = lam_v.detach().to(torch.float64).contiguous().clone()
-        pending = None                      # cotangent on F(x_g) from the later half-kick
         gx = torch.empty_like(lx)
         at = {c[0]: c for c in ckpts}
         starts = sorted(c[0] for c in ckpts if c[0] < G)
         bounds = starts + [G]
+        # gF: cotangent of F(x_{g+1}) -- h_g lv from substep g's second half-kick plus
+        # h_{g+1} lv from substep g+1's first one, both with the same lv
+        gF = lv * self._sub[(G - 1) % S][1] if G > 0 else None
 
         def vjp(xg, t, g_force, force=None):
             kw = {} if force is None else {"force_out": force}
@@ -327,6 +328,14 @@ class Leapfrog:
             else:
                 self.pot._adjoint_vjp(xg, t, None, g_force, tg, precision=self.precision, out=gx,
                                       **kw)
+
+        def kick(g):
+            """lx += gx; lv += dt_g lx; gF = (h_g + h_{g-1}) lv (h_0 lv after substep 0)."""
+            dtg, hg, _ = self._sub[g % S]
+            lx.add_(gx)
+            lv.add_(lx, alpha=dtg)
+            c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
+            torch.mul(lv, c, out=gF)
 
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
@@ -340,14 +349,9 @@ class Leapfrog:
                 h_next = 0.0
                 for g in range(e - 1, s - 1, -1):
                     dtg, hg, _ = self._sub[g % S]
-                    gF = lv * hg
-                    if pending is not None:
-                        gF.add_(pending)
                     need = g > s
                     vjp(xc, self._t(g + 1), gF, Fg if need else None)
-                    lx.add_(gx)
-                    lv.add_(lx, alpha=dtg)
-                    pending = lv * hg
+                    kick(g)
                     if need:
                         if vh is None:
                             vh = at[e][2].clone()
@@ -372,17 +376,11 @@ class Leapfrog:
                     X[g - s].copy_(x)
                     pos[g + 1] = X[g - s]
             for g in range(e - 1, s - 1, -1):
-                dtg, hg, _ = self._sub[g % S]
-                gF = lv * hg
-                if pending is not None:
-                    gF.add_(pending)
                 vjp(pos[g + 1], self._t(g + 1), gF)
-                lx.add_(gx)
-                lv.add_(lx, alpha=dtg)
-                pending = lv * hg
-        if pending is not None:
+                kick(g)
+        if G > 0:
             _, x0, _ = at[0]
-            vjp(x0, self.t0, pending)
+            vjp(x0, self.t0, gF)
             lx.add_(gx)
         if tg is not None:
             return lx, lv, allreduce_table_grads(self.pot._table_grads_from_device(tg), group)
