@@ -241,9 +241,11 @@ static int grid_for(long long n)
     return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
-#ifndef AGB_EVAL_WAVES
-#define AGB_EVAL_WAVES 4      // blocks per resident slot: balances the cost spread along r
-#endif
+// blocks per resident slot.  Measured on the 4M-point composite (mixed): 1 wave (the
+// largest contiguous chunk per block, most L1 reuse of an interval's records) is best
+// for one large launch, 4.86 ms against 4.99 ms with 4; for the 0.25-1M-point launches
+// of the host pipeline 2 waves give the shortest end-to-end step (6.44 against 6.72 ms).
+static int default_waves(long long n) { return n > (1LL << 21) ? 1 : 2; }
 
 template <int MODE, typename R, bool AN = false>
 static void launch_eval(EvalArgs& a, cudaStream_t st)
@@ -259,7 +261,7 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
     (void)grid_for(a.n);      // reads the SM count once
     const long long want = (a.n + 255) / 256;
     const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
-    const long long slots = (long long)g_num_sms * per_sm * (w ? w : AGB_EVAL_WAVES);
+    const long long slots = (long long)g_num_sms * per_sm * (w ? w : default_waves(a.n));
     const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
     a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
     agb_eval_kernel<MODE, R, AN><<<(int)grid, 256, 0, st>>>(a);

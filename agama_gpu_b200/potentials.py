@@ -144,9 +144,30 @@ class _GPUPotBase:
         return self
 
     # -- evaluation core ----------------------------------------------------
+    def _all_components(self):
+        """Every leaf component the tree can use at any time (all Evolving snapshots)."""
+        if isinstance(self, _Component):
+            return [self]
+        out = []
+        for sub in (getattr(self, "_components", None) or getattr(self, "_pots", None)
+                    or [getattr(self, "_inner")]):
+            out.extend(sub._all_components())
+        return out
+
+    def _preload(self, dev: torch.device) -> None:
+        """Upload every component's tables to dev once, so that a later time step that
+        brings a new Evolving snapshot into use does not upload inside the step."""
+        done = self.__dict__.setdefault("_preloaded", set())
+        if dev in done:
+            return
+        for c in self._all_components():
+            c._device_component(dev)
+        done.add(dev)
+
     def _c_args(self, t: float, dev: torch.device, leaves=None):
         """(component array, n_comps, leaf array, n_leaves) of the tree at time t
         (or of the given leaves)."""
+        self._preload(dev)
         if leaves is None:
             leaves = self._leaves(float(t))
         if not leaves:
@@ -437,8 +458,25 @@ class _GPUPotBase:
             return self._eval_host_run(src, host, want, n, chunk, t, mode, pot, dev, pipe)
 
     def _eval_host_run(self, src, host, want, n, chunk, t, mode, pot, dev, pipe):
+        # everything the launches need is prepared before the first copy is queued (the
+        # tree's arguments at t once, one workspace for the largest chunk), so each chunk
+        # costs the host one C call and the first kernel follows its copy directly
+        bounds = _chunk_bounds(n, chunk)
+        prec = _PRECISIONS[self.precision or _default_precision]
+        cargs = self._c_args(t, dev)
+        sizes = sorted({hi - lo for lo, hi in bounds})
+        flags = {m: self._flags(mode, prec, m) for m in sizes}
+        nws = max((int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3],
+                                                         m, flags[m])) for m in sizes), default=0)
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         cur = torch.cuda.current_stream(dev)
         s_in, s_cmp, s_out = pipe["streams"]
+        ws = pipe["bufs"].get("ws")
+        if nws and (ws is None or ws.numel() < nws):
+            # allocated on the compute stream, the only one that uses it
+            with torch.cuda.device(dev), torch.cuda.stream(s_cmp):
+                ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+            pipe["bufs"]["ws"] = ws
         for s in (s_in, s_cmp, s_out):
             s.wait_stream(cur)
         xb = pipe_buffers(pipe, dev, ("x", chunk), (chunk, 3))
@@ -448,7 +486,7 @@ class _GPUPotBase:
         ev_cmp = [torch.cuda.Event() for _ in range(2)]
         ev_out = [torch.cuda.Event() for _ in range(2)]
         started = [False, False]
-        for i, (lo, hi) in enumerate(_chunk_bounds(n, chunk)):
+        for i, (lo, hi) in enumerate(bounds):
             b = i & 1
             m = hi - lo
             with torch.cuda.stream(s_in):
@@ -461,7 +499,10 @@ class _GPUPotBase:
                 if started[b]:
                     s_cmp.wait_event(ev_out[b])      # the results of chunk i-2 are out
                 p_, f_, d_ = (ob[b][k][:m] if ob[b][k] is not None else None for k in range(3))
-                self._launch(xb[b][:m], t, mode, pot, out=(p_, f_, d_, None))
+                rc = _lib.lib.agb_eval_ws(*cargs, xb[b].data_ptr(), m, mode, prec, ptr(p_),
+                                          ptr(f_), ptr(d_), None, flags[m], ptr(ws), nws,
+                                          ctypes.c_void_p(s_cmp.cuda_stream))
+                _lib.check(rc, "agb_eval_ws")
                 ev_cmp[b].record(s_cmp)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_cmp[b])
@@ -477,23 +518,30 @@ class _GPUPotBase:
 
 
 def _chunk_bounds(n: int, chunk: int):
-    """Chunk ranges of eval_host: a quarter chunk first and last (the first copy-in
-    and the last copy-out cannot overlap a kernel, so they are kept short), full
-    chunks in between."""
-    q = max(1, chunk // 4)
+    """Chunk ranges of eval_host.  The first copy-in and the last copy-out cannot overlap
+    a kernel, so the chunks ramp up (chunk/4, chunk/2: each copy-in then hides behind
+    the previous, half-as-long kernel) and down (chunk/2, chunk/4, chunk/8: each
+    copy-out hides behind the next kernel) around full-size chunks in between."""
     if n <= 2 * chunk:
         return [(lo, min(n, lo + chunk)) for lo in range(0, n, chunk)]
-    out = [(0, q)]
-    lo = q
-    while n - lo > chunk + q:
-        out.append((lo, lo + chunk))
-        lo += chunk
-    rest = n - lo
-    if rest > q:
-        out.append((lo, n - q))
-        out.append((n - q, n))
+    head = [max(1, chunk // 4), max(1, chunk // 2)]
+    tail = [max(1, chunk // 2), max(1, chunk // 4), max(1, chunk // 8)]
+    mid = n - sum(head) - sum(tail)
+    if mid <= 0:
+        q = max(1, chunk // 4)
+        sizes = [q] + [chunk] * ((n - 2 * q) // chunk)
+        sizes.append(n - sum(sizes) - q) if n - sum(sizes) - q > 0 else None
+        sizes.append(q)
     else:
-        out.append((lo, n))
+        k = -(-mid // chunk)                       # full-size chunks, evened out
+        body = [mid // k + (1 if i < mid % k else 0) for i in range(k)]
+        sizes = head + body + tail
+    out, lo = [], 0
+    for m in sizes:
+        if m > 0:
+            out.append((lo, lo + m))
+            lo += m
+    assert lo == n
     return out
 
 
