@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from conftest import golden
-from helpers import close_global, close_pointwise, near_pole, rel_pointwise, tree_allowance
+from helpers import close_global, close_pointwise, near_pole, tree_allowance
 from oracle import cpu
 import agama_gpu_b200 as agb
 from agama_gpu_b200.coefs import MultipoleCoefs, write_coefs

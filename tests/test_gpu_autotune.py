@@ -1,7 +1,6 @@
 """Autotuner: every launch shape gives the same results; the choice is kept and cached."""
 import json
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
