@@ -149,3 +149,36 @@ def test_miyamoto_nagai_density_axisymmetric():
             ex = -G * Mm / math.sqrt(R * R + (a + math.sqrt(z * z + b * b)) ** 2)
             worst = max(worst, abs(val / ex - 1))
     assert worst < 5e-4, worst
+
+
+def test_solver_argument_checks():
+    rho = spheroid_density(mass=M, scaleRadius=A)
+    with pytest.raises(ValueError, match="symmetry"):
+        multipole_from_density(rho, symmetry="bogus", device="cpu")
+    with pytest.raises(ValueError, match="rmin"):
+        multipole_from_density(rho, symmetry="spherical", rmin=10.0, rmax=1.0, device="cpu")
+    with pytest.raises(ValueError, match="not both"):
+        spheroid_density(mass=M, densityNorm=1.0)
+    with pytest.raises(ValueError, match="thin"):
+        disk_density(surfaceDensity=1e9, scaleHeight=0.0)
+    with pytest.raises(ValueError, match="not both"):
+        disk_density(surfaceDensity=1e9, mass=1e10)
+
+
+def test_disk_mass_normalisation_and_sech2():
+    """mass fixes Sigma0 = M / (2 pi Rd^2) for n = 1; the isothermal layer integrates to 1."""
+    rho = disk_density(mass=5e10, scaleRadius=3.0, scaleHeight=-0.3)
+    assert abs(rho.sigma0 / (5e10 / (2 * math.pi * 9.0)) - 1) < 1e-3
+    zs = torch.linspace(-8, 8, 8001, dtype=torch.float64)
+    col = torch.trapezoid(rho(torch.full_like(zs, 3.0), 0 * zs, zs), zs)
+    assert abs(float(col) / (rho.sigma0 * math.exp(-1.0)) - 1) < 1e-4
+
+
+def test_factory_builds_density_types_without_agama():
+    import agama_gpu_b200 as agb
+    s = agb.PotentialGPU(type="Spheroid", mass=1e11, scaleRadius=2.0, gamma=1, beta=4, alpha=1,
+                         axisRatioZ=0.7, lmax=8, gridSizeR=30)
+    assert isinstance(s, agb.MultipolePotentialGPU)
+    assert all(l % 2 == 0 and m == 0 for l, m in s._coefs.lm_labels)      # axisymmetric
+    d = agb.PotentialGPU(type="Dehnen", mass=1e10, scaleRadius=1.0, gamma=2.0)
+    assert isinstance(d, agb.MultipolePotentialGPU) and d._coefs.lm_labels == [(0, 0)]
