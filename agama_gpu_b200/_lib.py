@@ -116,6 +116,14 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_adjoint_kick.restype = ctypes.c_int
+    lib.agb_adjoint_kick.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_void_p]
+    lib.agb_reverse_drift.restype = ctypes.c_int
+    lib.agb_reverse_drift.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_void_p]
     lib.agb_eval_static.restype = ctypes.c_int
     lib.agb_eval_static.argtypes = lib.agb_eval.argtypes
     lib.agb_eval_workspace_bytes.restype = ctypes.c_size_t
@@ -158,7 +166,7 @@ EXPORTED = [
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
     "agb_eval_vjp_force", "agb_multipole_adjoint_force",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
-    "agb_multipole_adjoint", "agb_cylspline_table_vjp",
+    "agb_multipole_adjoint", "agb_cylspline_table_vjp", "agb_adjoint_kick", "agb_reverse_drift",
     "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",

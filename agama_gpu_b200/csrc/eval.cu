@@ -20,6 +20,7 @@
 #include "bin.cuh"
 #include "mp_grad.cuh"
 #include "cs_grad.cuh"
+#include "adjoint_steps.cuh"
 
 // ---------------------------------------------------------------------------
 // errors and launch accounting
@@ -788,6 +789,31 @@ extern "C" int agb_multipole_adjoint_force(const agb_component* comp, const agb_
     if (!force) return set_err(AGB_ERR_ARG, "agb_multipole_adjoint_force: force is null");
     return multipole_adjoint_impl(comp, leaf, xyz, n, precision, g_phi, g_force, g_xyz, force,
                                   g_table, workspace, workspace_bytes, stream);
+}
+
+// ---------------------------------------------------------------------------
+// leapfrog adjoint: per-step vector updates
+// ---------------------------------------------------------------------------
+extern "C" int agb_adjoint_kick(double* lx, double* lv, const double* gx, double* gF, int64_t n,
+                                double dt, double c, void* stream)
+{
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_adjoint_kick: negative count");
+    if (n == 0) return AGB_OK;
+    if (!lx || !lv || !gx || !gF) return set_err(AGB_ERR_ARG, "agb_adjoint_kick: null argument");
+    const long long m = 3LL * n;
+    adjoint_kick_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(lx, lv, gx, gF, m, dt, c);
+    return check_launch("adjoint_kick_kernel");
+}
+
+extern "C" int agb_reverse_drift(double* x, double* vh, const double* F, int64_t n, double k,
+                                 double dt, void* stream)
+{
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_reverse_drift: negative count");
+    if (n == 0) return AGB_OK;
+    if (!x || !vh || !F) return set_err(AGB_ERR_ARG, "agb_reverse_drift: null argument");
+    const long long m = 3LL * n;
+    reverse_drift_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(x, vh, F, m, k, dt);
+    return check_launch("reverse_drift_kernel");
 }
 
 extern "C" int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf* leaf,

@@ -329,13 +329,32 @@ class Leapfrog:
                 self.pot._adjoint_vjp(xg, t, None, g_force, tg, precision=self.precision, out=gx,
                                       **kw)
 
+        on_gpu = lx.is_cuda
+
         def kick(g):
             """lx += gx; lv += dt_g lx; gF = (h_g + h_{g-1}) lv (h_0 lv after substep 0)."""
             dtg, hg, _ = self._sub[g % S]
+            c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
+            if on_gpu:          # one launch (agb_adjoint_kick)
+                rc = _lib.lib.agb_adjoint_kick(lx.data_ptr(), lv.data_ptr(), gx.data_ptr(),
+                                               gF.data_ptr(), lx.shape[0], dtg, c,
+                                               torch.cuda.current_stream(lx.device).cuda_stream)
+                _lib.check(rc, "agb_adjoint_kick")
+                return
             lx.add_(gx)
             lv.add_(lx, alpha=dtg)
-            c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
             torch.mul(lv, c, out=gF)
+
+        def drift_back(xc, vh, Fg, k, dtg):
+            """vh -= k F; x -= dt_g vh (the time-reversed drift)."""
+            if on_gpu:
+                rc = _lib.lib.agb_reverse_drift(xc.data_ptr(), vh.data_ptr(), Fg.data_ptr(),
+                                                xc.shape[0], k, dtg,
+                                                torch.cuda.current_stream(xc.device).cuda_stream)
+                _lib.check(rc, "agb_reverse_drift")
+                return
+            vh.sub_(Fg, alpha=k)
+            xc.sub_(vh, alpha=dtg)
 
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
@@ -355,10 +374,9 @@ class Leapfrog:
                     if need:
                         if vh is None:
                             vh = at[e][2].clone()
-                            vh.sub_(Fg, alpha=hg)
+                            drift_back(xc, vh, Fg, hg, dtg)
                         else:
-                            vh.sub_(Fg, alpha=h_next + hg)
-                        xc.sub_(vh, alpha=dtg)
+                            drift_back(xc, vh, Fg, h_next + hg, dtg)
                         h_next = hg
                 continue
             # the segment's positions: x_s and x_e from checkpoints, the others re-computed

@@ -281,6 +281,17 @@ int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
                                 void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Leapfrog adjoint, per-step vector updates on [N,3] device arrays (one launch each):
+ *   agb_adjoint_kick:  lx += gx;  lv += dt lx;  gF = c lv
+ *   agb_reverse_drift: vh -= k F; x -= dt vh     (the time-reversed drift)
+ * No counterpart in the reference (it has no integrator).
+ */
+int agb_adjoint_kick(double* lx, double* lv, const double* gx, double* gF, int64_t n,
+                     double dt, double c, void* stream);
+int agb_reverse_drift(double* x, double* vh, const double* F, int64_t n, double k,
+                      double dt, void* stream);
+
+/*
  * Gradient of a loss with respect to one CylSpline leaf's node table: adds into
  * g_cells, laid out like the component's cell-major FP64 table
  * [(nR-1)(nz-1)][n_harm][16] (each cell record holds its four corners' f, f_R,

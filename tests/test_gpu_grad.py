@@ -573,3 +573,27 @@ def test_reverse_reconstruction_matches_recompute(static, prec, tol):
         assert float((u - w).abs().max()) <= tol * float(u.abs().max())
     for comp in a[2]:
         assert float((a[2][comp] - b[2][comp]).abs().max()) <= tol * float(a[2][comp].abs().max())
+
+
+def test_adjoint_step_kernels_match_torch():
+    """agb_adjoint_kick and agb_reverse_drift against the same updates in torch."""
+    import torch
+    from agama_gpu_b200 import _lib
+    g = torch.Generator(device="cuda").manual_seed(5)
+    lx, lv, gx, F, x, vh = (torch.randn((1001, 3), generator=g, dtype=torch.float64, device="cuda")
+                            for _ in range(6))
+    gF = torch.empty_like(lx)
+    st = torch.cuda.current_stream().cuda_stream
+    ex, ev = lx + gx, None
+    ev = lv + 0.37 * ex
+    egF = 0.61 * ev
+    assert _lib.lib.agb_adjoint_kick(lx.data_ptr(), lv.data_ptr(), gx.data_ptr(), gF.data_ptr(),
+                                     1001, 0.37, 0.61, st) == 0
+    for a, b in ((lx, ex), (lv, ev), (gF, egF)):
+        assert float((a - b).abs().max()) <= 1e-15 * float(b.abs().max())
+    evh = vh - 0.2 * F
+    exx = x - 0.9 * evh
+    assert _lib.lib.agb_reverse_drift(x.data_ptr(), vh.data_ptr(), F.data_ptr(), 1001, 0.2, 0.9, st) == 0
+    for a, b in ((vh, evh), (x, exx)):
+        assert float((a - b).abs().max()) <= 1e-15 * float(b.abs().max())
+    assert _lib.lib.agb_adjoint_kick(None, None, None, None, 3, 0.1, 0.1, st) != 0
