@@ -151,6 +151,26 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
             const double lx = lf.sigma * x - lf.g0;
             const double ly = lf.sigma * y - lf.g1;
             const double lz = lf.sigma * z - lf.g2;
+            if ((MODE == AGB_MODE_POT || MODE == AGB_MODE_GRAD) && !AN &&
+                std::is_same<R, float>::value && lf.pad == 1) {
+                // this leaf and the next share grid, columns and transform (pack_args);
+                // FP32 walks only (the FP64 walk holds twice the state and would spill)
+                const DevLeaf& lf2 = a.leaves[L + 1];
+                PointOut o1, o2;
+                o1.phi = o2.phi = 0.0;
+                o1.g[0] = o1.g[1] = o1.g[2] = 0.0;
+                o2.g[0] = o2.g[1] = o2.g[2] = 0.0;
+                multipole_pair_point<CM, R>(c, a.comps[lf2.comp], lx, ly, lz, o1, o2);
+                phi += lf.ampl * o1.phi;
+                phi += lf2.ampl * o2.phi;
+                if (CM != AGB_MODE_POT) {
+                    const double As1 = lf.ampl * lf.sigma, As2 = lf2.ampl * lf2.sigma;
+                    g0 += As1 * o1.g[0]; g1 += As1 * o1.g[1]; g2 += As1 * o1.g[2];
+                    g0 += As2 * o2.g[0]; g1 += As2 * o2.g[1]; g2 += As2 * o2.g[2];
+                }
+                ++L;
+                continue;
+            }
             PointOut o;
             o.phi = 0.0; o.rho = 0.0;
             o.g[0] = o.g[1] = o.g[2] = 0.0;
@@ -479,8 +499,27 @@ static int pack_args(EvalArgs& a, const agb_component* comps, int n_comps, const
         d.sigma = leaves[L].sigma;
         d.g0 = leaves[L].gamma[0]; d.g1 = leaves[L].gamma[1]; d.g2 = leaves[L].gamma[2];
         d.ampl = leaves[L].ampl;
+        d.pad = 0;
     }
     a.n_leaves = n_leaves;
+    // pairs of consecutive Multipole leaves that one walk can serve (pad = 1 on the
+    // first): the same transform, radial grid, column structure and harmonic count
+    for (int L = 0; L + 1 < n_leaves; ++L) {
+        const DevLeaf& p = a.leaves[L];
+        const DevLeaf& q = a.leaves[L + 1];
+        const DevComp& c1 = a.comps[p.comp];
+        const DevComp& c2 = a.comps[q.comp];
+        if (c1.kind != AGB_KIND_MULTIPOLE || c2.kind != AGB_KIND_MULTIPOLE) continue;
+        if (!(c1.structure == AGB_STRUCT_EVEN || c1.structure == AGB_STRUCT_ALL)) continue;
+        if (c2.structure != c1.structure || c2.lmax != c1.lmax || c2.n_lm != c1.n_lm ||
+            c2.n_int != c1.n_int || c2.p[0] != c1.p[0] || c2.p[1] != c1.p[1] ||
+            c2.p[2] != c1.p[2] || c2.layout != c1.layout)
+            continue;
+        if (p.sigma != q.sigma || p.g0 != q.g0 || p.g1 != q.g1 || p.g2 != q.g2) continue;
+        if (precision != AGB_PREC_MIXED || !c1.table32 || !c2.table32) continue;
+        a.leaves[L].pad = 1;
+        ++L;                      // a leaf belongs to at most one pair
+    }
     (void)n_comps;
     return AGB_OK;
 }

@@ -445,6 +445,148 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
     }
 }
 
+// The same walk for two tables with one column structure, lmax and radial grid (the
+// two bracketing snapshots of an Evolving potential): the geometry, the Legendre and
+// m-phi recurrences are shared, each table keeps its own sums.  Per table the
+// arithmetic is that of mp_harmonics_reg.
+template <int MODE, typename R, int PAR>
+__device__ __forceinline__ void mp_harmonics_reg2(const DevComp& c1, const DevComp& c2, int k,
+                                                  double s_d, double cth_d, double sth_d,
+                                                  double cph, double sph, MPSums& tot1,
+                                                  MPSums& tot2)
+{
+    constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
+    constexpr bool NEED_ANG2 = MODE == AGB_MODE_HESS;
+    const bool near_pole = sth_d < 1.0e-10;
+    const R s = (R)s_d;
+    R sp[6], dw[6], ew[6];
+    sp[0] = R(1); sp[1] = s; sp[2] = s * s; sp[3] = sp[2] * s; sp[4] = sp[2] * sp[2]; sp[5] = sp[4] * s;
+    dw[0] = R(0); dw[1] = R(1); dw[2] = R(2) * s; dw[3] = R(3) * sp[2]; dw[4] = R(4) * sp[3]; dw[5] = R(5) * sp[4];
+    ew[0] = R(0); ew[1] = R(0); ew[2] = R(2); ew[3] = R(6) * s; ew[4] = R(12) * sp[2]; ew[5] = R(20) * sp[3];
+    const R cth = (R)cth_d, sth = (R)sth_d;
+    const R cc2 = (R)(cth_d * cth_d), w2 = (R)(-2.0 * cth_d * sth_d);
+    const R inv_sth = near_pole ? R(0) : (R)(1.0 / sth_d);
+    const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
+    const R np1 = near_pole ? R(0) : R(1);
+    const int lmax = c1.lmax;
+    const R* rec1 = MPPtr<R>::base(c1, k) + MPPtr<R>::REC;
+    const R* rec2 = MPPtr<R>::base(c2, k) + MPPtr<R>::REC;
+
+    double cm = 1.0, sm = 0.0, sinpow = 1.0, sinpow_m1 = 0.0;
+    for (int m = 0; m <= lmax; ++m) {
+        if (m > 0) {
+            const double t = cm * cph - sm * sph;
+            sm = sm * cph + cm * sph;
+            cm = t;
+            sinpow_m1 = sinpow;
+            sinpow *= sth_d;
+        }
+        int l0 = (PAR == 2) ? (m + (m & 1)) : m;
+        if (m == 0) l0 = PAR;
+        if (l0 > lmax) continue;
+        const R q1 = (near_pole && m == 1) ? R(1) : R(0);
+        const R m2 = R(m * m) * inv_sth * inv_sth;
+        R Pc = (R)(AGB_SEED[m] * sinpow), Pp = R(0), dPc = R(0), dPp = R(0);
+        if (NEED_ANG && m > 0)
+            dPc = (m == 1) ? (R)(AGB_SEED[1] * cth_d)
+                           : (near_pole ? R(0) : (R)((double)m * AGB_SEED[m] * sinpow_m1 * cth_d));
+        MPCol<R> gc1, gs1, gc2, gs2;
+        gc1.zero(); gs1.zero(); gc2.zero(); gs2.zero();
+        const int tb = m * AGB_LEG_N;
+        auto step = [&](int L) {
+            const R nb = MPConst<R>::nbetaq(tb + L);
+            const R Pn = fma(cth, Pc, nb * Pp);
+            if (NEED_ANG) {
+                const R dPn = fma(cth, dPc, fma(-sth, Pc, nb * dPp));
+                dPp = dPc;
+                dPc = dPn;
+            }
+            Pp = Pc;
+            Pc = Pn;
+        };
+        auto acc = [&](int L, auto has_sin) {
+            R ac1[6], as1[6], ac2[6], as2[6];
+            if (has_sin) {
+                MPPtr<R>::load_cs(rec1, ac1, as1);
+                MPPtr<R>::load_cs(rec2, ac2, as2);
+            } else {
+                MPPtr<R>::load(rec1, ac1);
+                MPPtr<R>::load(rec2, ac2);
+            }
+            rec1 += has_sin ? 2 * MPPtr<R>::REC : MPPtr<R>::REC;
+            rec2 += has_sin ? 2 * MPPtr<R>::REC : MPPtr<R>::REC;
+            const R ll1 = R(L * (L + 1));
+            mp_col_acc<MODE, R>(gc1, ac1, sp, dw, ew, Pc, dPc, ll1);
+            mp_col_acc<MODE, R>(gc2, ac2, sp, dw, ew, Pc, dPc, ll1);
+            if (has_sin) {
+                mp_col_acc<MODE, R>(gs1, as1, sp, dw, ew, Pc, dPc, ll1);
+                mp_col_acc<MODE, R>(gs2, as2, sp, dw, ew, Pc, dPc, ll1);
+            }
+        };
+        const int ts = m * AGB_SKIP_N;
+        auto skip2 = [&](int L) {
+            const auto ab = MPConst<R>::skip(ts + (L >> 1));
+            const R t = cc2 + (R)ab.x;
+            const R Pn = fma(t, Pc, (R)ab.y * Pp);
+            if (NEED_ANG) {
+                const R dPn = fma(w2, Pc, fma(t, dPc, (R)ab.y * dPp));
+                dPp = dPc;
+                dPc = dPn;
+            }
+            Pp = Pc;
+            Pc = Pn;
+        };
+        const R seed = Pc;
+        auto walk = [&](auto has_sin) {
+            int l = m;
+            while (l < l0) step(++l);
+            acc(l, has_sin);
+            if (PAR == 2) {
+                Pp = (m == 0) ? seed : R(0);
+                dPp = R(0);
+                #pragma unroll 2
+                for (l = l0 + 2; l <= lmax; l += 2) {
+                    skip2(l);
+                    acc(l, has_sin);
+                }
+            } else {
+                #pragma unroll 2
+                for (l = l0 + 1; l <= lmax; ++l) {
+                    step(l);
+                    acc(l, has_sin);
+                }
+            }
+        };
+        if (m == 0) walk(std::false_type());
+        else walk(std::true_type());
+        const double md = (double)m;
+        const double dTc = -md * sm, dTs = md * cm;
+        auto combine = [&](MPSums& tot, MPCol<R>& gc, MPCol<R>& gs) {
+            mp_col_finish<MODE, R>(gc, inv_sth, q1, np1, cot, m2);
+            mp_col_finish<MODE, R>(gs, inv_sth, q1, np1, cot, m2);
+            tot.A += (double)gc.V * cm + (double)gs.V * sm;
+            if (MODE != AGB_MODE_POT) tot.B += (double)gc.VR * cm + (double)gs.VR * sm;
+            if (MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS)
+                tot.D += (double)gc.VRR * cm + (double)gs.VRR * sm;
+            if (MODE == AGB_MODE_DENS) tot.L += (double)gc.L * cm + (double)gs.L * sm;
+            if (NEED_ANG) {
+                tot.Th += (double)gc.VT * cm + (double)gs.VT * sm;
+                tot.Pos += (double)gc.VP * dTc + (double)gs.VP * dTs;
+            }
+            if (NEED_ANG2) {
+                tot.Thth += (double)gc.VTT * cm + (double)gs.VTT * sm;
+                tot.BTh += (double)gc.VRT * cm + (double)gs.VRT * sm;
+                tot.Ph += (double)gc.V * dTc + (double)gs.V * dTs;
+                tot.Phph += -md * md * ((double)gc.V * cm + (double)gs.V * sm);
+                tot.BPh += (double)gc.VR * dTc + (double)gs.VR * dTs;
+                tot.ThPh += (double)gc.VT * dTc + (double)gs.VT * dTs;
+            }
+        };
+        combine(tot1, gc1, gs1);
+        combine(tot2, gc2, gs2);
+    }
+}
+
 __device__ __forceinline__ void mp_quintic0(const DevComp& c, int k, double s,
                                             double& v, double& d1, double& d2)
 {
@@ -643,4 +785,63 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
 
     mp_finish<MODE>(t, inv_dlogr, F, dF, d2F, mono, dmono, d2mono, px, py, pz, inv_r, Rc,
                     cth, sth, cph, sph, o);
+}
+
+// Two Multipoles on one radial grid and column structure at the same point (the two
+// bracketing snapshots of an Evolving potential, same transform): one geometry and one
+// shared walk (mp_harmonics_reg2); each keeps its monopole, log-scaling and
+// extrapolation.  Off the grid each is evaluated alone.
+template <int MODE, typename R>
+__device__ __forceinline__ void multipole_pair_point(const DevComp& c1, const DevComp& c2,
+                                                     double px, double py, double pz,
+                                                     PointOut& o1, PointOut& o2)
+{
+    const double logr_min = c1.p[0], dlogr = c1.p[1], inv_dlogr = c1.p[2];
+    const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
+    const double r2 = px * px + py * py + pz * pz;
+    const double r = sqrt(r2);
+    const double logr = r < 1.0e-300 ? 0.0 : log(r);
+    const int kk = r < 1.0e-300 || logr < logr_min ? -1 : (int)((logr - logr_min) * inv_dlogr);
+    if (kk < 0 || kk >= c1.n_int) {
+        multipole_point<MODE, R>(c1, px, py, pz, o1);
+        multipole_point<MODE, R>(c2, px, py, pz, o2);
+        return;
+    }
+    const int k = kk;
+    const double Rc = sqrt(px * px + py * py);
+    double s = (logr - (logr_min + k * dlogr)) * inv_dlogr;
+    s = fmin(fmax(s, 0.0), 1.0);
+    const double inv_r = 1.0 / r;
+    const double cth = pz * inv_r;
+    const double sth = Rc * inv_r;
+    const double cph = (Rc > 1.0e-300) ? px / Rc : 1.0;
+    const double sph = (Rc > 1.0e-300) ? py / Rc : 0.0;
+    MPSums t1 = {}, t2 = {};
+    if (c1.structure == AGB_STRUCT_EVEN)
+        mp_harmonics_reg2<MODE, R, 2>(c1, c2, k, s, cth, sth, cph, sph, t1, t2);
+    else
+        mp_harmonics_reg2<MODE, R, 1>(c1, c2, k, s, cth, sth, cph, sph, t1, t2);
+    auto finish = [&](const DevComp& c, const MPSums& t, PointOut& o) {
+        const double invPhi0 = c.p[3];
+        double c0, c0s, c0ss;
+        mp_quintic0(c, k, s, c0, c0s, c0ss);
+        const double dc0 = c0s * inv_dlogr;
+        const double d2c0 = c0ss * inv_dlogr * inv_dlogr;
+        double F = 1.0, dF = 0.0, d2F = 0.0, mono, dmono, d2mono;
+        if (c.log_scaling) {
+            const double ex = exp(c0);
+            const double P0 = 1.0 / (invPhi0 - ex);
+            const double dPdX = P0 * P0 * ex;
+            F = P0;
+            dF = dPdX * dc0;
+            d2F = dPdX * (d2c0 + dc0 * dc0 * P0 * (invPhi0 + ex));
+            mono = MP0 * F; dmono = MP0 * dF; d2mono = MP0 * d2F;
+        } else {
+            mono = MP0 * c0; dmono = MP0 * dc0; d2mono = MP0 * d2c0;
+        }
+        mp_finish<MODE>(t, inv_dlogr, F, dF, d2F, mono, dmono, d2mono, px, py, pz, inv_r, Rc,
+                        cth, sth, cph, sph, o);
+    };
+    finish(c1, t1, o1);
+    finish(c2, t2, o2);
 }

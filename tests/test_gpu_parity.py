@@ -371,3 +371,28 @@ def test_finite_difference_self_consistency():
         lap = -(Dn[:, 0] + Dn[:, 1] + Dn[:, 2])
         want = sign * lap * agb.INV_4PIG
         assert np.abs(_np(rho) - want).max() <= 1e-9 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_evolving_pair_walk_equals_separate_snapshots(prec):
+    """The two bracketing snapshots of an Evolving potential share one harmonic walk in
+    the mixed kernel; the result equals the weighted sum of the snapshots evaluated alone
+    (and the oracle)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    snaps = [agb.MultipolePotentialGPU(nfw_multipole(lmax=12, n_nodes=60, seed=4, drift=0.3 * i,
+                                                     amp=0.2)) for i in range(3)]
+    ev = agb.EvolvingPotentialGPU(snaps, [0.0, 1.0, 2.0], interpolate=True)
+    x = torch.from_numpy(hernquist_points(200_000, 10.0, 9)).cuda()
+    t, alpha = 1.3, 0.3
+    p, f = ev._launch(x, t, 1, True, precision=prec)[:2]
+    p1, f1 = snaps[1]._launch(x, t, 1, True, precision=prec)[:2]
+    p2, f2 = snaps[2]._launch(x, t, 1, True, precision=prec)[:2]
+    pr, fr = (1 - alpha) * p1 + alpha * p2, (1 - alpha) * f1 + alpha * f2
+    assert float((p - pr).abs().max()) <= 1e-13 * float(pr.abs().max())
+    assert float((f - fr).abs().max()) <= 1e-13 * float(fr.abs().max())
+    po, go, _, _ = cpu.eval_potential(ev, 1, x[:20000].cpu().numpy(), t)
+    # FP64 against the oracle: rounding of the outer extrapolation's large terms, ~1e-8
+    tol = 2e-6 if prec == "mixed" else 1e-7
+    assert np.abs(f[:20000].cpu().numpy() + go).max() <= tol * np.abs(go).max()
