@@ -573,7 +573,10 @@ def main():
         "roofline": {
             "bound": "fp32+fp64 pipes (mixed); fp64 pipe (plain)", "unit": "TFLOP/s",
             "note": "FP32/FP64 ALU-bound: the peaks are measured live (FMA chains) because the "
-                    "pool's measured peaks cover only HBM copy and bf16 GEMM",
+                    "pool's measured peaks cover only HBM copy and bf16 GEMM; flops count "
+                    "48 per harmonic per Multipole, the two Evolving snapshots each as if "
+                    "walked alone (the mixed kernel shares their recurrences, ~2 % fewer "
+                    "flops executed)",
             "achieved": achieved32, "peak": eff_peak32, "frac": achieved32 / eff_peak32,
             "traffic": TRAFFIC_BYTES_PER_POINT * N,
             "traffic_source": "ncu DRAM read+write of the mixed launch at 1M points, scaled to N",
