@@ -34,9 +34,10 @@ WORKLOAD = ("time-dependent composite: Multipole lmax=32 x 100 nodes + MiyamotoN
             "isotropic Hernquist a=10 kpc points")
 G = 4.30091727067736e-06
 # DRAM bytes (read + write) per point of one mixed-precision launch on this workload:
-# ncu dram__bytes_read.sum + dram__bytes_write.sum = 30.80 MB + 0.66 MB at 1M points
-# (profiles/eval_kernel_composite_1M_full.txt), scaled linearly with the point count
-TRAFFIC_BYTES_PER_POINT = 31.47
+# ncu dram__bytes_read.sum + dram__bytes_write.sum = 30.86 MB + 1.72 MB (mean of three
+# launches) at 1M points (profiles/eval_kernel_composite_1M_full.txt), scaled linearly
+# with the point count
+TRAFFIC_BYTES_PER_POINT = 32.58
 
 
 def measured_hbm_peak():
