@@ -28,14 +28,14 @@ from .potentials import _GPUPotBase, _PRECISIONS, _cuda_device
 
 
 class BatchedPotentialGPU(_GPUPotBase):
-    """``BatchedPotentialGPU(potentials, counts, tile_points=2048)``.
+    """``BatchedPotentialGPU(potentials, counts, tile_points=4096)``.
 
     potentials: one potential (any static tree: Multipole, CylSpline, analytic,
     Composite, Shifted/Scaled with fixed parameters) per unit; counts: the
     number of particles of each unit, stacked in this order.
     """
 
-    def __init__(self, potentials: Sequence, counts: Sequence[int], tile_points: int = 2048,
+    def __init__(self, potentials: Sequence, counts: Sequence[int], tile_points: int = 4096,
                  precision: Optional[str] = None) -> None:
         from .integrate import is_static
         pots = list(potentials)

@@ -173,7 +173,7 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
         return set_err(AGB_ERR_ARG, "agb_batch_create: empty component, leaf or unit list");
     if (precision != AGB_PREC_FP64 && precision != AGB_PREC_MIXED)
         return set_err(AGB_ERR_ARG, "agb_batch_create: unknown precision %d", precision);
-    if (tile_points == 0) tile_points = 2048;
+    if (tile_points == 0) tile_points = 4096;      // the largest sorted tile: fastest measured
     if (tile_points < 32 || tile_points > (1 << 20))
         return set_err(AGB_ERR_ARG, "agb_batch_create: tile_points %d outside [32, 2^20]", tile_points);
     if (unit_leaf_offsets[0] != 0 || point_offsets[0] != 0)

@@ -332,7 +332,7 @@ int agb_eval_static(const agb_component* comps, int n_comps,
  * [point_offsets[u], point_offsets[u+1]) of one shared xyz array.  The plan
  * uploads the descriptors once (it owns that device memory until
  * agb_batch_destroy) and cuts the units into tiles of at most tile_points
- * points (0: 2048), ordered by estimated cost, largest first.  agb_batch_eval
+ * points (0: 4096), ordered by estimated cost, largest first.  agb_batch_eval
  * then launches one persistent kernel whose blocks take tiles from a device
  * work queue (an atomic counter reset by a memset node before the launch), so
  * a call makes no host-side copies or allocations.  One plan serves one stream
