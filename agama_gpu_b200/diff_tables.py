@@ -111,7 +111,7 @@ def _spline_deriv_matrix(x: np.ndarray, bc_type) -> np.ndarray:
     return CubicSpline(x, np.eye(n), axis=0, bc_type=bc_type)(x, 1)
 
 
-def cylspline_node_vjp(tables, coefs, grad_nodes: torch.Tensor) -> dict:
+def cylspline_node_vjp(tables, coefs, grad_nodes: torch.Tensor, phi=None) -> dict:
     """{m: dL/dPhi_m (nR, nz of the coefficient grid)} from dL/d(node table).
 
     The node table of the builder (prep_cylspline.build_cylspline_tables) is, per
@@ -120,7 +120,9 @@ def cylspline_node_vjp(tables, coefs, grad_nodes: torch.Tensor) -> dict:
     and natural at the outer end in lR) -- of f = log(-Phi_0) (m = 0) or
     Phi_m / Phi_0 under log-scaling, Phi_m otherwise, on the z grid mirrored from
     z >= 0 when the file stores half of it.  The transpose of each step is applied
-    in turn.  The outer asymptote, Rscale and the asinh grids are held fixed."""
+    in turn.  The outer asymptote, Rscale and the asinh grids are held fixed.  ``phi``
+    ({m: grid on the coefficient file's grid}) replaces coefs.phi as the point of
+    differentiation (node values set on the device)."""
     G = grad_nodes.detach().to("cpu", torch.float64).numpy()
     lR, lz = tables.lR_grid, tables.lz_grid
     nR = len(lR)
@@ -129,8 +131,9 @@ def cylspline_node_vjp(tables, coefs, grad_nodes: torch.Tensor) -> dict:
     z0 = np.asarray(coefs.z_grid, dtype=np.float64)
     half = z0[0] == 0
     nz0 = len(z0)
+    src = coefs.phi if phi is None else phi
     phi = {}
-    for m, t in coefs.phi.items():
+    for m, t in src.items():
         t = np.asarray(t, dtype=np.float64)
         if half:
             full = np.empty((t.shape[0], 2 * nz0 - 1))

@@ -7,8 +7,8 @@ back.  Sections:
 * analytic leaves: ``type=<Name>`` and the constructor's own parameters;
 * Multipole / CylSpline: the coefficient tables inline (``Coefficients`` block, the
   text format ``read_coefs`` parses; values written with 17 significant digits so
-  they read back bit for bit).  A Multipole whose node tables were replaced on the
-  device (``set_node_tables``) is written with the current nodes;
+  they read back bit for bit).  A Multipole or CylSpline whose node tables were
+  replaced on the device (``set_node_tables``) is written with the current ones;
 * Evolving: ``type=Evolving``, ``interpLinear``, and a ``Timestamps`` block naming
   one coefficient file per snapshot, written beside the INI file;
 * Shifted / Scaled wrappers: ``center=x,y,z`` or ``center=<track file>`` ((T, 4) or
@@ -57,6 +57,20 @@ def current_multipole_coefs(mp) -> MultipoleCoefs:
     dphi[:, cols] = nodes[1].detach().to("cpu").numpy()
     return MultipoleCoefs(np.asarray(c.R_grid, dtype=np.float64).copy(), phi, dphi,
                           list(c.lm_labels), dict(c.params))
+
+
+def current_cylspline_coefs(cs):
+    """The coefficient grids of a CylSplinePotentialGPU as it evaluates now (the grids
+    set on the device by set_node_tables, when there were any)."""
+    from .coefs import CylSplineCoefs
+    grids = cs.__dict__.get("_phi_nodes")
+    if grids is None:
+        return cs._coefs
+    c = cs._coefs
+    return CylSplineCoefs(np.asarray(c.R_grid, dtype=np.float64).copy(),
+                          np.asarray(c.z_grid, dtype=np.float64).copy(),
+                          {m: v.detach().cpu().numpy() for m, v in grids.items()},
+                          dict(c.params))
 
 
 class _Writer:
@@ -122,7 +136,7 @@ class _Writer:
         mods = self.mod_lines(k, center, scale)
         if isinstance(pot, (MultipolePotentialGPU, CylSplinePotentialGPU)):
             coefs = (current_multipole_coefs(pot) if isinstance(pot, MultipolePotentialGPU)
-                     else pot._coefs)
+                     else current_cylspline_coefs(pot))
             body = coefs_text(coefs).splitlines()[1:]          # drop its own [Potential]
             at = next(i for i, ln in enumerate(body) if ln.strip().lower() == "coefficients")
             self.sections.append(head + body[:at] + mods + body[at:])
@@ -134,7 +148,7 @@ class _Writer:
                 if not isinstance(p, (MultipolePotentialGPU, CylSplinePotentialGPU)):
                     raise ValueError("Evolving snapshots must be Multipole or CylSpline to export")
                 coefs = (current_multipole_coefs(p) if isinstance(p, MultipolePotentialGPU)
-                         else p._coefs)
+                         else current_cylspline_coefs(p))
                 f = self.side_file(k, f"snap{i}.coef")
                 f.write_text(coefs_text(coefs))
                 lines.append(f"{_fmt(t)}\t{f.name}")

@@ -882,11 +882,74 @@ class CylSplinePotentialGPU(_Component):
     def node_gradients(self, grad_nodes: torch.Tensor):
         """{m: dL/dPhi_m} on the input coefficient grid from dL/d(node table), through
         the node-derivative splines, the log-scaling and the z mirroring of the table
-        builder (the outer asymptote, Rscale and the grids are held fixed)."""
+        builder (the outer asymptote, Rscale and the grids are held fixed), at the node
+        values set by set_node_tables() when there were any."""
         from .diff_tables import cylspline_node_vjp
         if self._coefs is None:
             raise ValueError("node_gradients() needs the coefficients the object was built from")
-        return cylspline_node_vjp(self.tables, self._coefs, grad_nodes)
+        phi = self.__dict__.get("_phi_nodes")
+        if phi is not None:
+            phi = {m: v.detach().cpu().numpy() for m, v in phi.items()}
+        return cylspline_node_vjp(self.tables, self._coefs, grad_nodes, phi=phi)
+
+    def set_node_tables(self, phi: dict) -> None:
+        """Replace the harmonic grids Phi_m(R, z) -- {m: (nR, nz) device tensors on the
+        coefficient file's grid} -- rebuilding the node and cell tables on the GPU, in
+        place (CUDA graphs captured over this potential stay valid): the z mirroring,
+        the log-scaling and the node-derivative splines run as device operations.  The
+        grids, Rscale, the log-scaling choice and the outer asymptote (fitted at
+        construction) are kept, as node_gradients() holds them.  Not differentiable
+        itself: use node_gradients() on the adjoint's table gradient."""
+        from .diff_tables import _spline_deriv_matrix
+        t = self.tables
+        keys = sorted(int(m) for m in self._coefs.phi)
+        if sorted(int(m) for m in phi) != keys:
+            raise ValueError(f"set_node_tables() needs the harmonics {keys}")
+        shape = np.asarray(self._coefs.phi[keys[0]]).shape
+        dev = next(iter(phi.values())).device
+        dev = dev if dev.type == "cuda" else _cuda_device()
+        f64 = dict(dtype=torch.float64, device=dev)
+        grids = {}
+        for m in keys:
+            v = phi[m] if m in phi else phi[str(m)]
+            if tuple(v.shape) != tuple(shape):
+                raise ValueError(f"harmonic {m}: shape {tuple(v.shape)}, expected {shape}")
+            v = v.detach().to(**f64)
+            if np.asarray(self._coefs.z_grid)[0] == 0:          # half-space grid: mirror
+                v = torch.cat([v[:, 1:].flip(1), v], dim=1)
+            grids[m] = v
+        if t.log_scaling:
+            p0 = grids[0]
+            if not bool((p0 < 0).all()):
+                raise ValueError("the m=0 grid must stay negative (the tables are log-scaled)")
+            fs = {m: (torch.log(-p0) if m == 0 else g / p0) for m, g in grids.items()}
+        else:
+            fs = grids
+        mats = self.__dict__.setdefault("_deriv_mats", {})
+        if dev not in mats:
+            nR = len(t.lR_grid)
+            DR = _spline_deriv_matrix(t.lR_grid, ((1, np.zeros(nR)), "natural"))
+            Dz = _spline_deriv_matrix(t.lz_grid, "natural")
+            mats[dev] = (torch.from_numpy(DR).to(**f64), torch.from_numpy(Dz).to(**f64))
+        DR, Dz = mats[dev]
+        nodes = []
+        for m in t.m_arr:
+            f = fs[int(m)]
+            fy = f @ Dz.T
+            nodes.append(torch.stack([f, DR @ f, fy, DR @ fy], dim=-1))
+        nd = torch.stack(nodes, 0)[torch.as_tensor(t.harmonic_order(), device=dev)]
+        corners = [nd[:, :-1, :-1], nd[:, :-1, 1:], nd[:, 1:, :-1], nd[:, 1:, 1:]]
+        rec = torch.stack(corners, dim=3).permute(1, 2, 0, 4, 3).reshape(-1, 16).contiguous()
+        r32 = torch.zeros((rec.shape[0], 20), dtype=torch.float32, device=dev)
+        r32.view(torch.float64)[:, 0] = rec[:, 0]
+        r32[:, 2:5] = (rec[:, 1:4] - rec[:, 0:1]).to(torch.float32)
+        r32[:, 5:17] = rec[:, 4:16].to(torch.float32)
+        self._phi_nodes = {m: (phi[m] if m in phi else phi[str(m)]).detach().to(**f64).clone()
+                           for m in keys}
+        self._cell_override = (rec.reshape(-1), r32.reshape(-1))
+        for cdev, (_, keep) in self.__dict__.get("_dev_cache", {}).items():
+            keep[0].copy_(rec.reshape(-1).to(cdev), non_blocking=True)
+            keep[1].copy_(r32.reshape(-1).to(cdev), non_blocking=True)
 
     @classmethod
     def from_file(cls, path, **kw) -> "CylSplinePotentialGPU":
@@ -894,8 +957,12 @@ class CylSplinePotentialGPU(_Component):
 
     def _upload(self, dev):
         t = self.tables
-        cells = torch.from_numpy(self._cells).to(dev)
-        cells32 = torch.from_numpy(self._cells32).to(dev)
+        over = self.__dict__.get("_cell_override")
+        if over is not None:
+            cells, cells32 = over[0].to(dev).clone(), over[1].to(dev).clone()
+        else:
+            cells = torch.from_numpy(self._cells).to(dev)
+            cells32 = torch.from_numpy(self._cells32).to(dev)
         m = torch.from_numpy(self._m).to(dev)
         lR = torch.from_numpy(np.ascontiguousarray(t.lR_grid)).to(dev)
         lz = torch.from_numpy(np.ascontiguousarray(t.lz_grid)).to(dev)

@@ -597,3 +597,50 @@ def test_adjoint_step_kernels_match_torch():
     for a, b in ((vh, evh), (x, exx)):
         assert float((a - b).abs().max()) <= 1e-15 * float(b.abs().max())
     assert _lib.lib.agb_adjoint_kick(None, None, None, None, 3, 0.1, 0.1, st) != 0
+
+
+def test_cylspline_set_node_tables_on_device():
+    """CylSpline grids replaced on the GPU: the same grids give the same tables; new
+    grids give a fresh host-built object's values inside the grid (the outer asymptote
+    is kept from construction), in place under a captured leapfrog graph, and
+    node_gradients() differentiates at the new grids."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.coefs import CylSplineCoefs
+    from agama_gpu_b200.integrate import Leapfrog
+    coefs = cs_coefs(golden("cs_cfg1"))
+    cs = agb.CylSplinePotentialGPU(coefs)
+    rng = np.random.default_rng(3)
+    R = rng.uniform(0.5, 40.0, 4000)
+    ph = rng.uniform(0, 2 * np.pi, 4000)
+    z = rng.uniform(-20.0, 20.0, 4000)
+    x = torch.from_numpy(np.stack([R * np.cos(ph), R * np.sin(ph), z], 1)).cuda()
+    x0, v0 = _disk_ics(200, 23)
+    integ = Leapfrog(cs, 0.002, graph_steps=5)
+    xa, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)          # captures the graph
+    f0 = cs.force(x)
+    grids = {m: torch.from_numpy(np.asarray(v, dtype=np.float64)).cuda() for m, v in coefs.phi.items()}
+    cs.set_node_tables(grids)
+    f1 = cs.force(x)
+    assert float((f1 - f0).abs().max()) <= 1e-12 * float(f0.abs().max())
+    # m != 0 scaled; m = 0 changed only at interior nodes away from R = 0 and the outer
+    # boundary, so that a fresh build keeps the same Rscale and outer asymptote
+    new = {m: np.asarray(v, dtype=np.float64) * (1.3 if m != 0 else 1.0) for m, v in coefs.phi.items()}
+    bump = 1.0 + 0.02 * np.exp(-np.asarray(coefs.R_grid)[1:-1, None] / 5.0)
+    new[0] = new[0].copy()
+    new[0][1:-1, 1:-1] *= bump
+    ref = agb.CylSplinePotentialGPU(CylSplineCoefs(coefs.R_grid, coefs.z_grid, new, dict(coefs.params)))
+    cs.set_node_tables({m: torch.from_numpy(v).cuda() for m, v in new.items()})
+    for prec, tol in (("fp64", 1e-11), ("mixed", 2e-6)):
+        fm = cs._launch(x, 0.0, 1, True, precision=prec)[1]
+        fr = ref._launch(x, 0.0, 1, True, precision=prec)[1]
+        assert float((fm - fr).abs().max()) <= tol * float(fr.abs().max()), prec
+    xb, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)
+    xc, _, _ = Leapfrog(ref, 0.002, use_graph=False).run(x0, v0, 10, checkpoint_every=64)
+    assert not torch.equal(xa, xb)
+    assert float((xb - xc).abs().max()) <= 1e-10 * float(xc.abs().max())
+    g = cs.table_vjp(x, 0.0, None, torch.ones_like(x))
+    gr = ref.table_vjp(x, 0.0, None, torch.ones_like(x))
+    a, b = cs.node_gradients(g), ref.node_gradients(gr)
+    for m in a:
+        assert np.abs(a[m] - b[m]).max() <= 1e-8 * max(np.abs(b[m]).max(), 1e-300), m
