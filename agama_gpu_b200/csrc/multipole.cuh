@@ -757,7 +757,16 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
     const double cph = (Rc > 1.0e-300) ? px / Rc : 1.0;
     const double sph = (Rc > 1.0e-300) ? py / Rc : 0.0;
 
-    // monopole (FP64) and the log-scaling factor F(log r) with derivatives
+    MPSums t = {};
+    if (c.structure == AGB_STRUCT_EVEN)
+        mp_harmonics_reg<MODE, R, 2>(c, k, s, cth, sth, cph, sph, t);
+    else if (c.structure == AGB_STRUCT_ALL)
+        mp_harmonics_reg<MODE, R, 1>(c, k, s, cth, sth, cph, sph, t);
+    else
+        mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
+
+    // monopole (FP64) and the log-scaling factor F(log r) with derivatives, after the
+    // walk so that its values are not live across it (FP64 kernel 7.22 -> 6.96 ms)
     double c0, c0s, c0ss;
     mp_quintic0(c, k, s, c0, c0s, c0ss);
     const double dc0 = c0s * inv_dlogr;
@@ -774,14 +783,6 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
     } else {
         mono = MP0 * c0; dmono = MP0 * dc0; d2mono = MP0 * d2c0;
     }
-
-    MPSums t = {};
-    if (c.structure == AGB_STRUCT_EVEN)
-        mp_harmonics_reg<MODE, R, 2>(c, k, s, cth, sth, cph, sph, t);
-    else if (c.structure == AGB_STRUCT_ALL)
-        mp_harmonics_reg<MODE, R, 1>(c, k, s, cth, sth, cph, sph, t);
-    else
-        mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
 
     mp_finish<MODE>(t, inv_dlogr, F, dF, d2F, mono, dmono, d2mono, px, py, pz, inv_r, Rc,
                     cth, sth, cph, sph, o);
