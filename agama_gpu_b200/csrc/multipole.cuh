@@ -286,23 +286,35 @@ __device__ __forceinline__ void mp_col_acc(MPCol<R>& g, const R a[6], const R sp
     constexpr bool NEED_B = MODE != AGB_MODE_POT;
     constexpr bool NEED_D = MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS;
     constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
-    // C = sum a_j s^j: Horner in FP32 (one instruction less); two short chains in
-    // FP64, where the longer dependent DFMA chain costs more than it saves
-    R C;
-    if (std::is_same<R, float>::value)
-        C = fma(fma(fma(fma(fma(a[5], sp[1], a[4]), sp[1], a[3]), sp[1], a[2]), sp[1], a[1]), sp[1], a[0]);
-    else
+    // C = sum a_j s^j.  FP32: one Horner pass carries C, C' and C''/2 together
+    // (5 + 4 + 3 FMAs against 5 + 5 + 5 for separate sums); the C''/2 sum is doubled
+    // once per group in mp_col_finish.  FP64: two short chains per sum, where the
+    // longer dependent DFMA chain costs more than it saves
+    R C, dC = R(0), d2C = R(0);
+    if (std::is_same<R, float>::value) {
+        const R x = sp[1];
+        R p = fma(a[5], x, a[4]), d = a[5], e = a[5];
+        d = fma(d, x, p); p = fma(p, x, a[3]);
+        if (NEED_D) e = fma(e, x, d);
+        d = fma(d, x, p); p = fma(p, x, a[2]);
+        if (NEED_D) e = fma(e, x, d);
+        d = fma(d, x, p); p = fma(p, x, a[1]);
+        if (NEED_D) e = fma(e, x, d);
+        d = fma(d, x, p); p = fma(p, x, a[0]);
+        C = p;
+        dC = d;
+        d2C = e;
+    } else {
         C = fma(a[2], sp[2], fma(a[1], sp[1], a[0])) + fma(a[5], sp[5], fma(a[4], sp[4], a[3] * sp[3]));
+        if (NEED_B) dC = fma(a[2], dw[2], a[1]) + fma(a[5], dw[5], fma(a[4], dw[4], a[3] * dw[3]));
+        if (NEED_D) d2C = fma(a[3], ew[3], R(2) * a[2]) + fma(a[5], ew[5], a[4] * ew[4]);
+    }
     g.V = fma(C, Y, g.V);
     if (NEED_B) {
-        const R dC = fma(a[2], dw[2], a[1]) + fma(a[5], dw[5], fma(a[4], dw[4], a[3] * dw[3]));
         g.VR = fma(dC, Y, g.VR);
         if (MODE == AGB_MODE_HESS) g.VRT = fma(dC, dY, g.VRT);
     }
-    if (NEED_D) {
-        const R d2C = fma(a[3], ew[3], R(2) * a[2]) + fma(a[5], ew[5], a[4] * ew[4]);
-        g.VRR = fma(d2C, Y, g.VRR);
-    }
+    if (NEED_D) g.VRR = fma(d2C, Y, g.VRR);
     if (MODE == AGB_MODE_DENS || MODE == AGB_MODE_HESS) g.L = fma(ll1 * C, Y, g.L);
     if (NEED_ANG) g.VT = fma(C, dY, g.VT);
 }
@@ -313,6 +325,8 @@ __device__ __forceinline__ void mp_col_finish(MPCol<R>& g, R inv_sth, R q1, R np
 {
     if (MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS) g.VP = fma(g.V, inv_sth, q1 * g.VT);
     if (MODE == AGB_MODE_HESS) g.VTT = np1 * (fma(-cot, g.VT, m2 * g.V) - g.L);
+    if ((MODE == AGB_MODE_HESS || MODE == AGB_MODE_DENS) && std::is_same<R, float>::value)
+        g.VRR *= R(2);                                          // the FP32 walk sums C''/2
 }
 
 template <int MODE, typename R, int PAR>
