@@ -130,6 +130,10 @@ def _load():
     lib.agb_eval_workspace_bytes.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
         ctypes.c_int64, ctypes.c_int]
+    lib.agb_eval_wave_points.restype = ctypes.c_int64
+    lib.agb_eval_wave_points.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_int, ctypes.c_int]
     lib.agb_eval_ws.restype = ctypes.c_int
     lib.agb_eval_ws.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
@@ -163,7 +167,7 @@ lib = _load()
 # symbols the header declares (checked by tests/test_capi.py)
 EXPORTED = [
     "agb_last_error", "agb_version", "agb_measure_fma_peak", "agb_launch_count", "agb_launch_count_reset", "agb_eval",
-    "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_static", "agb_eval_vjp",
+    "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_wave_points", "agb_eval_static", "agb_eval_vjp",
     "agb_eval_vjp_force", "agb_multipole_adjoint_force",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
     "agb_multipole_adjoint", "agb_cylspline_table_vjp", "agb_adjoint_kick", "agb_reverse_drift",

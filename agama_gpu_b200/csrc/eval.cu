@@ -270,10 +270,11 @@ static int grid_for(long long n)
 // of the host pipeline 2 waves give the shortest end-to-end step (6.44 against 6.72 ms).
 static int default_waves(long long n) { return n > (1LL << 21) ? 1 : 2; }
 
-template <int MODE, typename R, bool AN = false>
-static void launch_eval(EvalArgs& a, cudaStream_t st)
+// resident blocks per SM of one instantiation (queried once)
+template <int MODE, typename R, bool AN>
+static int eval_blocks_per_sm()
 {
-    static int per_sm = 0;    // resident blocks per SM of this instantiation
+    static int per_sm = 0;
     if (per_sm == 0) {
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_eval_kernel<MODE, R, AN>, 256, 0)
@@ -281,6 +282,21 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
             b = 1;
         per_sm = b;
     }
+    return per_sm;
+}
+
+// points that one wave of resident threads holds (one point per thread)
+template <int MODE, typename R, bool AN = false>
+static long long eval_wave_points()
+{
+    (void)grid_for(1);        // reads the SM count once
+    return (long long)g_num_sms * eval_blocks_per_sm<MODE, R, AN>() * 256;
+}
+
+template <int MODE, typename R, bool AN = false>
+static void launch_eval(EvalArgs& a, cudaStream_t st)
+{
+    const int per_sm = eval_blocks_per_sm<MODE, R, AN>();
     (void)grid_for(a.n);      // reads the SM count once
     const long long want = (a.n + 255) / 256;
     const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
@@ -618,6 +634,30 @@ extern "C" size_t agb_eval_workspace_bytes(const agb_component* comps, int n_com
     for (int L = 0; L < n_leaves; ++L)
         if (leaves[L].comp < 0 || leaves[L].comp >= n_comps) return 0;
     return ws_bytes_staged(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
+}
+
+extern "C" int64_t agb_eval_wave_points(const agb_component* comps, int n_comps,
+                                        const agb_leaf* leaves, int n_leaves, int mode,
+                                        int precision)
+{
+    if (!comps || !leaves || n_leaves < 1 || n_comps < 1) return 0;
+    bool an = true;
+    for (int L = 0; L < n_leaves; ++L) {
+        if (leaves[L].comp < 0 || leaves[L].comp >= n_comps) return 0;
+        const int k = comps[leaves[L].comp].kind;
+        if (k == AGB_KIND_MULTIPOLE || k == AGB_KIND_CYLSPLINE) an = false;
+    }
+    const bool mixed = precision == AGB_PREC_MIXED;
+    switch (mode) {
+    case AGB_MODE_POT:  return mixed ? eval_wave_points<AGB_MODE_POT, float>() : eval_wave_points<AGB_MODE_POT, double>();
+    case AGB_MODE_GRAD: return mixed ? eval_wave_points<AGB_MODE_GRAD, float>() : eval_wave_points<AGB_MODE_GRAD, double>();
+    case AGB_MODE_HESS: return mixed ? eval_wave_points<AGB_MODE_HESS, float>() : eval_wave_points<AGB_MODE_HESS, double>();
+    case AGB_MODE_DENS: return mixed ? eval_wave_points<AGB_MODE_DENS, float>() : eval_wave_points<AGB_MODE_DENS, double>();
+    case AGB_MODE_VJP:
+        if (an) return eval_wave_points<AGB_MODE_VJP, double, true>();
+        return mixed ? eval_wave_points<AGB_MODE_VJP, float>() : eval_wave_points<AGB_MODE_VJP, double>();
+    default: return 0;
+    }
 }
 
 extern "C" int agb_eval(const agb_component* comps, int n_comps, const agb_leaf* leaves,

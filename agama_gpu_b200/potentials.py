@@ -413,8 +413,9 @@ class _GPUPotBase:
                   t: float = 0.0, chunk_points: Optional[int] = None, out=None, device=None):
         """``eval`` for positions and results in HOST memory, pipelined.
 
-        The points go through the GPU in chunks of ``chunk_points`` (default: N/4,
-        clamped to [2^17, 2^20] points, so a chunk still fills the GPU): while chunk i
+        The points go through the GPU in chunks of about ``chunk_points`` (default: N/3,
+        clamped to [2^17, 2^20] points, so a chunk still fills the GPU; large calls round
+        the chunks to whole waves of the kernel's resident threads): while chunk i
         is evaluated, chunk i+1 is copied in and chunk i-1's results are copied
         out (three CUDA streams, two device buffers per stream stage), so the
         PCIe transfers hide behind the kernel.  xyz: (N,3) float64 CPU tensor or
@@ -451,7 +452,7 @@ class _GPUPotBase:
                           or h.device.type != "cpu" or not h.is_contiguous()):
                     raise ValueError(f"out buffer must be a contiguous float64 CPU tensor {shape}")
         if chunk_points is None:
-            chunk_points = min(1 << 20, max(1 << 17, -(-n // 4)))
+            chunk_points = min(1 << 20, max(1 << 17, -(-n // 3)))
         chunk = max(1, min(int(chunk_points), max(n, 1)))
         pipe = _host_pipe(dev)
         with pipe["lock"]:
@@ -461,11 +462,19 @@ class _GPUPotBase:
         # everything the launches need is prepared before the first copy is queued (the
         # tree's arguments at t once, one workspace for the largest chunk), so each chunk
         # costs the host one C call and the first kernel follows its copy directly
-        bounds = _chunk_bounds(n, chunk)
         prec = _PRECISIONS[self.precision or _default_precision]
         cargs = self._c_args(t, dev)
+        wave = int(_lib.lib.agb_eval_wave_points(cargs[0], cargs[1], cargs[2], cargs[3], mode,
+                                                 prec))
+        bounds = _chunk_bounds(n, chunk, wave)
         sizes = sorted({hi - lo for lo, hi in bounds})
+        chunk = max(sizes)                 # the device buffers hold the largest chunk
         flags = {m: self._flags(mode, prec, m) for m in sizes}
+        if wave and len(bounds) > 2:
+            # chunks in whole waves: one resident block per slot, so every thread of
+            # a launch takes the same number of passes (unless a tuned shape is set)
+            flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 else f | (1 << _lib.OUT_GRID_SHIFT)
+                     for m, f in flags.items()}
         nws = max((int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3],
                                                          m, flags[m])) for m in sizes), default=0)
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
@@ -517,11 +526,35 @@ class _GPUPotBase:
         return res[0] if len(res) == 1 else tuple(res)
 
 
-def _chunk_bounds(n: int, chunk: int):
+def _chunk_bounds(n: int, chunk: int, wave: int = 0):
     """Chunk ranges of eval_host.  The first copy-in and the last copy-out cannot overlap
-    a kernel, so the chunks ramp up (chunk/4, chunk/2: each copy-in then hides behind
-    the previous, half-as-long kernel) and down (chunk/2, chunk/4, chunk/8: each
-    copy-out hides behind the next kernel) around full-size chunks in between."""
+    a kernel, so the chunks ramp up and down around full-size chunks in between.
+
+    With ``wave`` (the points one wave of the kernel's resident threads holds) and enough
+    points, every chunk but the last is a whole number of waves: a launch takes as many
+    passes of its threads as its largest block needs, so a chunk of 11.1 waves costs 12
+    passes.  In waves, with c = round(chunk / wave) (14 for 2^20 points on 148 SMs x 2
+    blocks x 256 threads): ramp-up c/7, 3c/7 (each copy-in hides behind the previous
+    kernel: a copy-in takes ~0.4 of a kernel's time per point), full chunks of c, ramp-down
+    5c/7, 2c/7, then the remainder of 2 to 3 waves, whose copy-out is the only one
+    exposed.  On the 4M-point composite (mixed, 1 B200) this layout takes the
+    end-to-end step 5.68 -> 5.29 ms.  Otherwise: chunk/4, chunk/2, full chunks, chunk/2,
+    chunk/4, chunk/8."""
+    if wave > 0 and chunk >= wave:
+        c = max(1, round(chunk / wave))
+        head = [max(1, round(c / 7)), max(1, round(3 * c / 7))]
+        tail = [max(1, round(5 * c / 7)), max(1, round(2 * c / 7))]
+        body_waves = n // wave - sum(head) - sum(tail) - 2
+        if body_waves >= c:
+            k = -(-body_waves // c)
+            body = [body_waves // k + (1 if i < body_waves % k else 0) for i in range(k)]
+            sizes = [u * wave for u in head + body + tail]
+            sizes.append(n - sum(sizes))
+            out, lo = [], 0
+            for m in sizes:
+                out.append((lo, lo + m))
+                lo += m
+            return out
     if n <= 2 * chunk:
         return [(lo, min(n, lo + chunk)) for lo in range(0, n, chunk)]
     head = [max(1, chunk // 4), max(1, chunk // 2)]

@@ -207,6 +207,18 @@ int agb_eval_ws(const agb_component* comps, int n_comps,
                 int out_flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Points that one wave of the evaluator's resident threads holds on the current
+ * device (SMs x resident blocks x 256) for the kernel this tree, mode and
+ * precision select; 0 for bad arguments.  A call of n points with
+ * AGB_OUT_GRID(1) takes ceil(n / wave) passes of its threads over the points, so
+ * callers that split work into several calls (the pipelined host path) size the
+ * calls in multiples of it.  No reference counterpart: the reference evaluates
+ * one host array per call.
+ */
+int64_t agb_eval_wave_points(const agb_component* comps, int n_comps,
+                             const agb_leaf* leaves, int n_leaves, int mode, int precision);
+
+/*
  * Vector-Jacobian product of the composite w.r.t. positions (the backward of
  * a potential/force evaluation):  g_xyz = g_phi * grad(Phi) - H g_force,
  * H the Hessian of Phi (F = -grad Phi, dF/dx = -H).  One fused launch: every

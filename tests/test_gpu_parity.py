@@ -306,6 +306,37 @@ def test_eval_host_pipeline_matches_eval(pinned):
     assert float((out - f_dev).abs().max()) <= 1e-14 * float(f_dev.abs().max())
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_eval_host_wave_chunks_match_eval(precision):
+    """Large calls split into whole waves of the kernel's resident threads, launched one
+    block per slot: same results as one device call (Phi+F and Phi+F+H)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    from agama_gpu_b200.potentials import _PRECISIONS, _chunk_bounds
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    pot = (agb.MultipolePotentialGPU(nfw_multipole(lmax=8, n_nodes=50, seed=1, amp=0.3))
+           + agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3))
+    pot.set_precision(precision)
+    n = 700_001
+    xyz = torch.from_numpy(hernquist_points(n, 10.0, 3)).pin_memory()
+    cargs = pot._c_args(0.0, torch.device("cuda"))
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for mode in (_lib.MODE_GRAD, _lib.MODE_HESS):
+        wave = int(_lib.lib.agb_eval_wave_points(*cargs[:4], mode, _PRECISIONS[precision]))
+        assert wave > 0 and wave % (sms * 256) == 0
+        sizes = [h - l for l, h in _chunk_bounds(n, 160_000, wave)]
+        assert len(sizes) > 3 and all(m % wave == 0 for m in sizes[:-1])   # the wave layout
+    p, f = pot.eval(xyz.cuda(), pot=True, acc=True)
+    hp, hf = pot.eval_host(xyz, pot=True, acc=True, chunk_points=160_000)
+    for h, g in ((hp, p), (hf, f)):
+        assert float((h - g.cpu()).abs().max()) <= 1e-14 * float(g.abs().max())
+    p, f, d = pot.eval(xyz.cuda(), pot=True, acc=True, der=True)
+    hp, hf, hd = pot.eval_host(xyz, pot=True, acc=True, der=True, chunk_points=160_000)
+    for h, g in ((hp, p), (hf, f), (hd, d)):
+        assert float((h - g.cpu()).abs().max()) <= 1e-14 * float(g.abs().max())
+
+
 def test_cylspline_mixed_precision():
     """CylSpline bar (mmax 6, 32x32 sinh grid), exponential-disk points: the FP32
     Hermite path against FP64 -- force within the 1e-6 gate, the rest stated."""
