@@ -20,7 +20,7 @@
 #pragma once
 #include "agb_dev.cuh"
 
-#define AGB_BIN_TILE 4096          // points per block in passes 1 and 3
+#define AGB_BIN_TILE_MAX 4096      // points per block in passes 1 and 3 (at most)
 #define AGB_MAX_BINS 8192
 
 struct BinKey {
@@ -49,14 +49,14 @@ __device__ __forceinline__ int bin_of(const BinKey& b, double x, double y, doubl
 }
 
 __global__ void __launch_bounds__(256)
-bin_count(const double* __restrict__ xyz, long long n, BinKey b, int n_bins,
+bin_count(const double* __restrict__ xyz, long long n, int tile, BinKey b, int n_bins,
           int* __restrict__ keys, int* __restrict__ counts)
 {
     extern __shared__ int hist[];
     for (int q = threadIdx.x; q < n_bins; q += blockDim.x) hist[q] = 0;
     __syncthreads();
-    const long long lo = (long long)blockIdx.x * AGB_BIN_TILE;
-    const long long hi = min(lo + (long long)AGB_BIN_TILE, n);
+    const long long lo = (long long)blockIdx.x * tile;
+    const long long hi = min(lo + (long long)tile, n);
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const int k = bin_of(b, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]) +
                       (int)(i >> b.log_block) * (b.n_int + 2);
@@ -93,7 +93,7 @@ bin_scan(const int* __restrict__ counts, int* __restrict__ cursor, int n_bins)
 }
 
 __global__ void __launch_bounds__(256)
-bin_scatter(const double* __restrict__ xyz, long long n, int n_bins,
+bin_scatter(const double* __restrict__ xyz, long long n, int tile, int n_bins,
             int* __restrict__ keys, int* __restrict__ cursor,
             int* __restrict__ perm, double* __restrict__ xyz_sorted)
 {
@@ -102,8 +102,8 @@ bin_scatter(const double* __restrict__ xyz, long long n, int n_bins,
     int* base = sm + n_bins;     // this block's reserved start in each bin
     for (int q = threadIdx.x; q < n_bins; q += blockDim.x) hist[q] = 0;
     __syncthreads();
-    const long long lo = (long long)blockIdx.x * AGB_BIN_TILE;
-    const long long hi = min(lo + (long long)AGB_BIN_TILE, n);
+    const long long lo = (long long)blockIdx.x * tile;
+    const long long hi = min(lo + (long long)tile, n);
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&hist[keys[i]], 1);
     __syncthreads();
     for (int q = threadIdx.x; q < n_bins; q += blockDim.x) {

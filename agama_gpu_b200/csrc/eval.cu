@@ -564,13 +564,20 @@ static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t
     }
     if (cudaMemsetAsync(counts, 0, 4 * (size_t)b.n_bins, st) != cudaSuccess)
         return set_err(AGB_ERR_DEVICE, "agb_eval: memset of bin counts failed");
-    const int tiles = (int)((n + AGB_BIN_TILE - 1) / AGB_BIN_TILE);
-    bin_count<<<tiles, 256, smem1, st>>>(xyz, n, b.key, b.n_bins, keys, counts);
+    // points per block: the largest power of two from 512 to 4096 that still gives
+    // every SM 4 blocks (each thread's atomics and loads are sequential, so small calls
+    // need many blocks in flight; 0.5M points: 1024 blocks instead of 128)
+    (void)grid_for(1);
+    const long long per4 = n / ((long long)g_num_sms * 4);
+    int tile = 512;
+    while (tile < AGB_BIN_TILE_MAX && 2LL * tile <= per4) tile <<= 1;
+    const int tiles = (int)((n + tile - 1) / tile);
+    bin_count<<<tiles, 256, smem1, st>>>(xyz, n, tile, b.key, b.n_bins, keys, counts);
     int rc = check_launch("bin_count");
     if (rc) return rc;
     bin_scan<<<1, 1024, 0, st>>>(counts, cursor, b.n_bins);
     if ((rc = check_launch("bin_scan"))) return rc;
-    bin_scatter<<<tiles, 256, smem3, st>>>(xyz, n, b.n_bins, keys, cursor, perm, xs);
+    bin_scatter<<<tiles, 256, smem3, st>>>(xyz, n, tile, b.n_bins, keys, cursor, perm, xs);
     if ((rc = check_launch("bin_scatter"))) return rc;
     a.xyz = xs;
     a.perm = perm;
