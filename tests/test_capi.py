@@ -54,6 +54,11 @@ def test_argument_errors_need_no_gpu():
     assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, ctypes.c_void_p(16),
                              None, None, 0, None) == 0
     assert _lib.lib.agb_eval_workspace_bytes(comps, 1, leaves, 1, 10**6, 0) == 0   # no Multipole
+    # the wave size: 0 for bad arguments, before any CUDA call
+    assert _lib.lib.agb_eval_wave_points(None, 0, None, 0, 1, 0) == 0
+    leaves[0].comp = 3
+    assert _lib.lib.agb_eval_wave_points(comps, 1, leaves, 1, 1, 0) == 0
+    leaves[0].comp = 0
     # lmax beyond the kernel's limit
     comps[0].kind = _lib.KIND_MULTIPOLE
     comps[0].lmax = 40
