@@ -470,7 +470,7 @@ class _GPUPotBase:
         sizes = sorted({hi - lo for lo, hi in bounds})
         chunk = max(sizes)                 # the device buffers hold the largest chunk
         flags = {m: self._flags(mode, prec, m) for m in sizes}
-        if wave and len(bounds) > 2:
+        if wave and len(bounds) > 2 and all((hi - lo) % wave == 0 for lo, hi in bounds[:-1]):
             # chunks in whole waves: one resident block per slot, so every thread of
             # a launch takes the same number of passes (unless a tuned shape is set)
             flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 else f | (1 << _lib.OUT_GRID_SHIFT)
