@@ -327,16 +327,9 @@ extern "C" void agb_batch_destroy(agb_batch* plan)
 template <int MODE, typename R>
 static int launch_batch(const BatchArgs& a, cudaStream_t st)
 {
-    static int per_sm = 0;    // resident blocks per SM of this instantiation
-    if (per_sm == 0) {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_batch_kernel<MODE, R>, 256, 0)
-            != cudaSuccess || b < 1)
-            b = 1;
-        per_sm = b;
-    }
-    (void)grid_for(1);        // reads the SM count once
-    const long long grid = std::min<long long>((long long)g_num_sms * per_sm, a.n_tiles);
+    static std::atomic<int> cache[AGB_MAX_DEVICES];   // resident blocks per SM, per device
+    const int per_sm = blocks_per_sm(cache, agb_batch_kernel<MODE, R>, 256);
+    const long long grid = std::min<long long>((long long)num_sms() * per_sm, a.n_tiles);
     agb_batch_kernel<MODE, R><<<(int)std::max<long long>(grid, 1), 256, 0, st>>>(a);
     return check_launch("agb_batch_kernel");
 }

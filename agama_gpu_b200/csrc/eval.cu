@@ -7,8 +7,11 @@
 // in FP64, then writes the outputs once.  This replaces the reference's chain
 // of one launch per component plus CuPy elementwise passes for shifts, scales,
 // negation, lerps and sums (gpu_potential.py:1439-1918).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <stdio.h>
 #include <string.h>
 #include <stdarg.h>
@@ -249,18 +252,51 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-static int g_num_sms = 0;
+// Values fixed for the life of a device (its SM count, the resident blocks of one
+// kernel) are read on the device current at the call and cached per device index.
+// Host threads making their first call at the same time store the same value, so
+// relaxed atomics are enough.
+#define AGB_MAX_DEVICES 64
+
+static int current_device()
+{
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= AGB_MAX_DEVICES) d = 0;
+    return d;
+}
+
+static std::atomic<int> g_num_sms[AGB_MAX_DEVICES];
+
+static int num_sms()
+{
+    const int dev = current_device();
+    int v = g_num_sms[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        g_num_sms[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// resident blocks per SM of `kernel` at `threads` threads, cached per device in `cache`
+template <typename K>
+static int blocks_per_sm(std::atomic<int>* cache, K kernel, int threads)
+{
+    const int dev = current_device();
+    int b = cache[dev].load(std::memory_order_relaxed);
+    if (b == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b < 1)
+            b = 1;
+        cache[dev].store(b, std::memory_order_relaxed);
+    }
+    return b;
+}
 
 static int grid_for(long long n)
 {
-    if (g_num_sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_num_sms <= 0) g_num_sms = 148;
-    }
     const long long blocks = (n + 255) / 256;
-    const long long cap = (long long)g_num_sms * 64;
+    const long long cap = (long long)num_sms() * 64;
     return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
@@ -270,37 +306,28 @@ static int grid_for(long long n)
 // of the host pipeline 2 waves give the shortest end-to-end step (6.44 against 6.72 ms).
 static int default_waves(long long n) { return n > (1LL << 21) ? 1 : 2; }
 
-// resident blocks per SM of one instantiation (queried once)
+// resident blocks per SM of one instantiation
 template <int MODE, typename R, bool AN>
 static int eval_blocks_per_sm()
 {
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, agb_eval_kernel<MODE, R, AN>, 256, 0)
-            != cudaSuccess || b < 1)
-            b = 1;
-        per_sm = b;
-    }
-    return per_sm;
+    static std::atomic<int> per_sm[AGB_MAX_DEVICES];
+    return blocks_per_sm(per_sm, agb_eval_kernel<MODE, R, AN>, 256);
 }
 
 // points that one wave of resident threads holds (one point per thread)
 template <int MODE, typename R, bool AN = false>
 static long long eval_wave_points()
 {
-    (void)grid_for(1);        // reads the SM count once
-    return (long long)g_num_sms * eval_blocks_per_sm<MODE, R, AN>() * 256;
+    return (long long)num_sms() * eval_blocks_per_sm<MODE, R, AN>() * 256;
 }
 
 template <int MODE, typename R, bool AN = false>
 static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
     const int per_sm = eval_blocks_per_sm<MODE, R, AN>();
-    (void)grid_for(a.n);      // reads the SM count once
     const long long want = (a.n + 255) / 256;
     const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
-    const long long slots = (long long)g_num_sms * per_sm * (w ? w : default_waves(a.n));
+    const long long slots = (long long)num_sms() * per_sm * (w ? w : default_waves(a.n));
     const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
     a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
     agb_eval_kernel<MODE, R, AN><<<(int)grid, 256, 0, st>>>(a);
@@ -452,7 +479,7 @@ static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, 
     return b;
 }
 
-static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+static constexpr size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static size_t ws_bytes(const BinPlan& b, int64_t n)
 {
@@ -542,7 +569,7 @@ static int pack_args(EvalArgs& a, const agb_component* comps, int n_comps, const
     return AGB_OK;
 }
 
-static unsigned long long g_bin_attr_set = 0;     // one bit per device
+static std::atomic<unsigned long long> g_bin_attr_set{0};     // one bit per device
 
 // Sort the points by interval into the workspace; sets a.xyz / a.perm.
 static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t n, char* ws,
@@ -554,21 +581,19 @@ static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t
     int* counts = (int*)(ws + 2 * al256(4 * (size_t)n) + al256(24 * (size_t)n));
     int* cursor = (int*)((char*)counts + al256(4 * (size_t)b.n_bins));
     const size_t smem1 = 4 * (size_t)b.n_bins, smem3 = 8 * (size_t)b.n_bins;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(g_bin_attr_set & bit)) {
+    const unsigned long long bit = 1ull << current_device();
+    if (!(g_bin_attr_set.load(std::memory_order_acquire) & bit)) {
+        // idempotent: two threads doing this at once set the same attributes
         cudaFuncSetAttribute(bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * AGB_MAX_BINS);
         cudaFuncSetAttribute(bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * AGB_MAX_BINS);
-        g_bin_attr_set |= bit;
+        g_bin_attr_set.fetch_or(bit, std::memory_order_release);
     }
     if (cudaMemsetAsync(counts, 0, 4 * (size_t)b.n_bins, st) != cudaSuccess)
         return set_err(AGB_ERR_DEVICE, "agb_eval: memset of bin counts failed");
     // points per block: the largest power of two from 512 to 4096 that still gives
     // every SM 4 blocks (each thread's atomics and loads are sequential, so small calls
     // need many blocks in flight; 0.5M points: 1024 blocks instead of 128)
-    (void)grid_for(1);
-    const long long per4 = n / ((long long)g_num_sms * 4);
+    const long long per4 = n / ((long long)num_sms() * 4);
     int tile = 512;
     while (tile < AGB_BIN_TILE_MAX && 2LL * tile <= per4) tile <<= 1;
     const int tiles = (int)((n + tile - 1) / tile);
@@ -590,7 +615,7 @@ static thread_local const double* g_vjp_force = nullptr;
 static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* leaves, int n_leaves,
                      const double* xyz, int64_t n, int mode, int precision, double* phi,
                      double* grad, double* hess, double* rho, int out_flags, void* workspace,
-                     size_t workspace_bytes, bool own_ws, void* stream)
+                     size_t workspace_bytes, bool own_ws, void* stream, bool fixed_ws = false)
 {
     int rc = validate(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess, rho);
     if (rc) return rc;
@@ -615,6 +640,10 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
             if (cudaMallocAsync(&ws, need, st) != cudaSuccess)
                 return set_err(AGB_ERR_DEVICE, "agb_eval: cannot allocate %zu bytes of scratch", need);
         } else if (!ws || workspace_bytes < need) {
+            if (fixed_ws)
+                return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_static: needs %zu bytes of scratch, "
+                               "more than its fixed %zu (use agb_eval or agb_eval_ws)", need,
+                               workspace_bytes);
             return set_err(AGB_ERR_ARG, "agb_eval_ws: workspace of %zu bytes is smaller than the "
                            "%zu bytes agb_eval_workspace_bytes asks for", workspace_bytes, need);
         }
@@ -826,8 +855,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
     }
     if (!rc) {
         // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
-        (void)grid_for(n);               // reads the SM count once
-        const int grid = (int)std::min<long long>((long long)g_num_sms * 2, (n + 255) / 256);
+        const int grid = (int)std::min<long long>((long long)num_sms() * 2, (n + 255) / 256);
         const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
         g.chunk = ((groups + warps - 1) / warps) * 32;
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
@@ -939,15 +967,80 @@ extern "C" int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf
 // (AGB_STATIC_SCRATCH_BYTES = 32 MiB), which every GPU that loads this library
 // holds until the process exits; it limits one call to AGB_STATIC_MAX_POINTS
 // points.  Host code cannot use the array's name as a device address: the
-// address is fetched with cudaGetSymbolAddress once per device, on the first
-// call made with that device current, and that first call should be made
-// before any stream capture begins.  All calls share the one array and it
+// address is fetched with cudaGetSymbolAddress once per device (and once more
+// after a device reset replaced its context), on the first call made with that
+// device current, and that first call should be made before any stream capture
+// begins.  All calls share the one array and it
 // keeps whatever the last call left there (the bin counts that must start at
 // zero are cleared by every call), so calls whose work overlaps on the GPU
 // (other streams, other host threads) race on it: serialise them.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_static_scratch[AGB_STATIC_SCRATCH_BYTES];
-static void* g_static_scratch_addr[64] = {nullptr};
+
+// The largest call must fit: keys, permutation and sorted positions of
+// AGB_STATIC_MAX_POINTS points plus the two bin arrays at their maximum
+// (output staging is used only when it fits as well).
+static_assert(2 * al256(4 * (size_t)AGB_STATIC_MAX_POINTS) + al256(24 * (size_t)AGB_STATIC_MAX_POINTS)
+              + 2 * al256(4 * (size_t)AGB_MAX_BINS) <= (size_t)AGB_STATIC_SCRATCH_BYTES,
+              "agb_eval_static: the fixed scratch array cannot hold a call of AGB_STATIC_MAX_POINTS");
+
+// Id of the CUDA context current on this thread (0 when the driver cannot say).
+// The driver entry points come through the runtime, so the library needs no
+// link-time dependency on libcuda.
+typedef CUresult (*agb_ctx_current_fn)(CUcontext*);
+typedef CUresult (*agb_ctx_id_fn)(CUcontext, unsigned long long*);
+
+static unsigned long long current_context_id()
+{
+    static std::once_flag once;
+    static agb_ctx_current_fn get_current = nullptr;
+    static agb_ctx_id_fn get_id = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q)
+                == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = (agb_ctx_current_fn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q)
+                == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = (agb_ctx_id_fn)f;
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+        get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// The array's device address per device, with the context it was looked up in.
+// A device reset (cudaDeviceReset) destroys the primary context and the module
+// with it; the next call sees a new context id and looks the address up again.
+struct StaticScratchSlot {
+    std::mutex lock;
+    unsigned long long ctx;
+    void* addr;
+};
+static StaticScratchSlot g_static_slot[AGB_MAX_DEVICES];
+
+static int static_scratch_address(int dev, void** out)
+{
+    StaticScratchSlot& s = g_static_slot[dev];
+    std::lock_guard<std::mutex> guard(s.lock);
+    const unsigned long long ctx = current_context_id();
+    if (!s.addr || ctx == 0 || ctx != s.ctx) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_err(AGB_ERR_DEVICE, "agb_eval_static: cudaGetSymbolAddress failed: %s",
+                           cudaGetErrorString(e));
+        s.addr = p;
+        s.ctx = current_context_id();    // the lookup made the primary context current
+    }
+    *out = s.addr;
+    return AGB_OK;
+}
 
 extern "C" int agb_eval_static(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                                int n_leaves, const double* xyz, int64_t n, int mode,
@@ -959,31 +1052,15 @@ extern "C" int agb_eval_static(const agb_component* comps, int n_comps, const ag
                        "limit of %d points (use agb_eval or agb_eval_ws)", (long long)n,
                        AGB_STATIC_MAX_POINTS);
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= AGB_MAX_DEVICES)
         return set_err(AGB_ERR_DEVICE, "agb_eval_static: no usable current CUDA device");
-    if (!g_static_scratch_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess || !p)
-            return set_err(AGB_ERR_DEVICE, "agb_eval_static: cudaGetSymbolAddress failed: %s",
-                           cudaGetErrorString(e));
-        g_static_scratch_addr[dev] = p;
-    }
-    // the sort scratch this call cannot do without (output staging is used only
-    // when it fits as well)
-    size_t need = 0;
-    if (comps && leaves && n_comps >= 1 && n_leaves >= 1) {
-        bool ok = true;
-        for (int L = 0; L < n_leaves; ++L)
-            ok = ok && leaves[L].comp >= 0 && leaves[L].comp < n_comps;
-        if (ok) need = ws_bytes(plan_binning(comps, leaves, n_leaves, n, out_flags), n);
-    }
-    if (need > (size_t)AGB_STATIC_SCRATCH_BYTES)
-        return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_static: needs %zu bytes of scratch, more "
-                       "than its fixed %d", need, AGB_STATIC_SCRATCH_BYTES);
+    void* scratch = nullptr;
+    const int rc = static_scratch_address(dev, &scratch);
+    if (rc) return rc;
+    // eval_impl checks the scratch this call needs against the array's size
     return eval_impl(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess,
-                     rho, out_flags, g_static_scratch_addr[dev], (size_t)AGB_STATIC_SCRATCH_BYTES,
-                     false, stream);
+                     rho, out_flags, scratch, (size_t)AGB_STATIC_SCRATCH_BYTES, false, stream,
+                     true);
 }
 
 // ---------------------------------------------------------------------------

@@ -129,6 +129,26 @@ def composite_spec(lmax_main: int = 32, n_nodes: int = 100, n_snap: int = 16,
                 nfw=dict(mass=1.5e11, scaleRadius=10.0))
 
 
+def config4_unit_specs(n_units: int = 512, seed: int = 4) -> list:
+    """The uneven batch: per unit an NFW-based Multipole with lmax ~ U{2..32}, rs ~
+    U[2,30] kpc, nodes ~ U{30..120}, M ~ logU[1e10,1e12] and N ~ logU[1e3, 5e5]
+    Hernquist(a = rs) points (seed 1000 + unit).  Returns [{index, coefs (keyword
+    arguments of nfw_multipole), n_points, a}].  The expected total is about 40M
+    points: E[N] = (5e5 - 1e3) / ln(500) = 80k per unit."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for u in range(n_units):
+        lmax = int(rng.integers(2, 33))
+        rs = float(rng.uniform(2.0, 30.0))
+        n_nodes = int(rng.integers(30, 121))
+        M = float(10 ** rng.uniform(10, 12))
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        out.append(dict(index=u, coefs=dict(lmax=lmax, n_nodes=n_nodes, M=M, rs=rs, seed=u,
+                                            amp=0.05),
+                        n_points=n, a=rs))
+    return out
+
+
 def build_composite(spec: dict, interpolate: bool = True):
     """The time-dependent composite of ``composite_spec``: Multipole + MiyamotoNagai +
     DiskAnsatz + Shifted NFW on a (T,4) track + Evolving Multipole snapshots."""

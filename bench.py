@@ -38,6 +38,8 @@ G = 4.30091727067736e-06
 # launches) at 1M points (profiles/eval_kernel_composite_1M_full.txt), scaled linearly
 # with the point count
 TRAFFIC_BYTES_PER_POINT = 32.58
+# wall-clock budget of the reference arm's timed steps (seconds)
+REF_BUDGET_S = 150.0
 
 
 def measured_hbm_peak():
@@ -132,33 +134,64 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _config(n_points: int, world: int) -> dict:
+    """The workload description both arms print (the driver compares them)."""
+    return {"workload": WORKLOAD, "points_per_gpu": n_points,
+            "l2": "flushed (256 MiB write) between timed steps",
+            "parallelism": f"points sharded, {world} rank(s), no data-path collective"}
+
+
+def reference_unavailable(why: str) -> None:
+    print(json.dumps({"impl": "reference", "unavailable": why}))
+
+
 def run_reference(args):
-    """The reference's CPU implementation of the path, timed on the host cores."""
-    from agama_gpu_b200.synthetic import build_composite, composite_spec, hernquist_points
-    from oracle import cpu
-    spec = composite_spec()
-    pot = build_composite(spec)
-    n_sample = args.cpu_sample
-    xyz = hernquist_points(n_sample, 10.0, 12345)
+    """The reference's CPU implementation of the path, timed on the host cores.
+
+    The potential is the reference's own config-2 tree: built by its classes and
+    table builders and recorded where its sources are (oracle/ref_tree.py), then
+    evaluated here by its kernel code compiled for the host (its two .cu files and
+    its ElementwiseKernel bodies, OpenMP over all cores) with the call structure of
+    its ``eval(xyz, pot=True, acc=True, t)``: a potential pass and a force pass over
+    every component, outputs summed, the Shifted centre and the Evolving bracket
+    from its splines.  This repository's package is not imported.  Each step
+    evaluates the step's points at one time; warm-up steps use an eighth of them."""
+    from oracle import ref_tree
+    if not ref_tree.available("config2"):
+        return reference_unavailable("the recorded reference tree (oracle/_ref/tree_config2.npz) "
+                                     "is absent: run __graft_entry__.build() where the reference "
+                                     "sources are")
+    tree = ref_tree.load("config2")
     threads = os.cpu_count() or 1
-    kind = "reference" if cpu.ref_available() else "port"
+    xyz = ref_tree.hernquist_points(args.n, 10.0, 1000)      # rank 0's points of the GPU arm
     ts = step_times(args.warmup + args.steps)
-    for k in range(args.warmup):
-        cpu.eval_potential_reference(pot, 1, xyz, ts[k], threads)
     t0 = time.perf_counter()
+    for k in range(args.warmup):
+        tree.eval(xyz[: max(1, args.n // 8)], pot=True, acc=True, t=ts[k], nthreads=threads)
+    warm = time.perf_counter() - t0
+    # bound the run: the timed steps evaluate at most what fits in REF_BUDGET_S at
+    # the warm-up rate (all N points unless the host is slow)
+    rate = args.warmup * max(1, args.n // 8) / max(warm, 1e-9) if args.warmup else 1e300
+    n = int(min(args.n, max(250_000, rate * REF_BUDGET_S / max(args.steps, 1))))
+    sub = xyz[:n]
+    times = []
     for k in range(args.steps):
-        cpu.eval_potential_reference(pot, 1, xyz, ts[args.warmup + k], threads)
-    dt = (time.perf_counter() - t0) / args.steps
-    value = n_sample / dt
-    sample = (f"{n_sample} Hernquist points per step, Phi+F of the full composite; expansions "
-              f"by the reference's kernels compiled for the host (OpenMP), analytic terms restated")
+        t1 = time.perf_counter()
+        tree.eval(sub, pot=True, acc=True, t=ts[args.warmup + k], nthreads=threads)
+        times.append(time.perf_counter() - t1)
+    dt = float(np.mean(times))
+    value = n / dt
+    sample = (f"{n} of the workload's {args.n} Hernquist points per step (Phi+F at the step's "
+              f"time): the reference's recorded config-2 tree, its kernel code compiled for "
+              f"the host, {threads} OpenMP threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pts/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "n_points": n_sample, "device": "host CPU"},
-            "cpu_baseline": {"value": value, "unit": "pts/s", "cores": threads, "kind": kind,
-                             "sample": sample},
+            "config": _config(args.n, args.gpus),
+            "sample_points_per_step": n,
+            "cpu_baseline": {"value": value, "unit": "pts/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "pts/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -237,19 +270,14 @@ def batched_units(dev, n_units: int, steps: int, warmup: int, lf_steps: int, pre
     import torch
     import agama_gpu_b200 as agb
     from agama_gpu_b200.integrate import Leapfrog
-    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
-    rng = np.random.default_rng(4)
+    from agama_gpu_b200.synthetic import config4_unit_specs, hernquist_points, nfw_multipole
     units, counts, xs, flops = [], [], [], 0.0
-    for u in range(n_units):
-        lmax = int(rng.integers(2, 33))
-        rs = rng.uniform(2.0, 30.0)
-        mp = agb.MultipolePotentialGPU(nfw_multipole(
-            lmax=lmax, n_nodes=int(rng.integers(30, 121)), M=10 ** rng.uniform(10, 12), rs=rs,
-            seed=u, amp=0.05))
-        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+    for spec in config4_unit_specs(n_units):
+        mp = agb.MultipolePotentialGPU(nfw_multipole(**spec["coefs"]))
+        n = spec["n_points"]
         units.append(mp)
         counts.append(n)
-        xs.append(hernquist_points(n, rs, 1000 + u))
+        xs.append(hernquist_points(n, spec["a"], 1000 + spec["index"]))
         flops += n * (48.0 * mp.tables.n_lm + 64.0)
     batch = agb.BatchedPotentialGPU(units, counts, precision=precision)
     x = torch.from_numpy(np.concatenate(xs)).to(dev)
@@ -347,19 +375,28 @@ def cylspline_leg(dev, n: int, steps: int, warmup: int):
             "mixed_force_max_rel_in_grid": err}
 
 
-def cpu_baseline_leg(pot, xyz: np.ndarray, t: float, n_sample: int):
-    from oracle import cpu
+def cpu_baseline_leg(xyz: np.ndarray, t: float, n_sample: int):
+    """The reference's recorded config-2 tree on the host cores (as the reference arm),
+    on the first n_sample of the step's points: median of 5 after 2 warm-ups."""
+    from oracle import ref_tree
+    if not ref_tree.available("config2"):
+        return {"value": None, "unit": "pts/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: the recorded reference tree is absent"}
+    tree = ref_tree.load("config2")
     threads = os.cpu_count() or 1
-    sub = xyz[:n_sample]
-    cpu.eval_potential_reference(pot, 1, sub[:1000], t, threads)
-    reps = 3
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        cpu.eval_potential_reference(pot, 1, sub, t, threads)
-    dt = (time.perf_counter() - t0) / reps
-    return {"value": n_sample / dt, "unit": "pts/s", "cores": threads,
-            "kind": "reference" if cpu.ref_available() else "port",
-            "sample": f"{n_sample} of the step's points, Phi+F, median of {reps} after a warm-up"}
+    sub = np.ascontiguousarray(xyz[:n_sample])
+    for _ in range(2):
+        tree.eval(sub, pot=True, acc=True, t=t, nthreads=threads)
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        tree.eval(sub, pot=True, acc=True, t=t, nthreads=threads)
+        runs.append(time.perf_counter() - t0)
+    dt = float(np.median(runs))
+    return {"value": n_sample / dt, "unit": "pts/s", "cores": threads, "kind": "reference",
+            "sample": f"{n_sample} of the step's points, Phi+F through the reference's recorded "
+                      f"config-2 tree and its host-compiled kernel code, median of 5 after 2 "
+                      f"warm-ups"}
 
 
 def main():
@@ -551,9 +588,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "points_per_gpu": N, "precision": "mixed",
-                   "l2": "flushed (256 MiB write) between timed steps",
-                   "parallelism": f"points sharded, {world} rank(s), no data-path collective"},
+        "config": _config(N, world),
+        "precision": "mixed (FP32 harmonic sums, FP64 elsewhere); plain FP64 in `fp64`",
         "fp64": {"value": world * N / (ms64 * 1e-3), "unit": "pts/s", "ms_per_step": ms64},
         "speedup_mixed_vs_fp64": ms64 / ms32,
         "step_breakdown_ms": {"eval_kernel_mixed": k32, "eval_kernel_fp64": k64,
@@ -592,7 +628,7 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_leg(pot, xyz_np, t_chk, args.cpu_sample)
+        line["cpu_baseline"] = cpu_baseline_leg(xyz_np, t_chk, args.cpu_sample)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -326,8 +326,9 @@ int agb_cylspline_table_vjp(const agb_component* comp, const agb_leaf* leaf,
  * inside this library (held on every GPU that loads it), so one call takes at
  * most AGB_STATIC_MAX_POINTS points; larger calls fail with
  * AGB_ERR_UNSUPPORTED.  The first call on a device looks up the array's
- * address (make it before any stream capture).  All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller.
+ * address (make it before any stream capture); after a device reset the next
+ * call looks it up again.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.
  */
 #define AGB_STATIC_SCRATCH_BYTES (32 * 1024 * 1024)
 #define AGB_STATIC_MAX_POINTS 1000000

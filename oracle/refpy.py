@@ -14,10 +14,11 @@ Imports the reference wrapper (``gpu_potential.py`` and
   into a host C++ library under ``oracle/_ref/``.
 
 With that, the reference's classes (Composite, Evolving, Shifted, Scaled, the
-factory) run as-is on numpy input.  This module needs the reference sources
-(``AGB_REFERENCE`` or ``/root/reference``) and is used only to generate golden
-vectors and by CPU tests that skip when the sources are absent.  The product
-never imports it.
+factory) run as-is on numpy input.  This module needs the reference sources:
+the directory named by ``AGB_REFERENCE``, else the checkout this recipe was
+written against (``DEFAULT_REFERENCE``; the one place that names it).  It is
+used only to generate golden vectors and reference-built tables and by CPU
+tests that skip when the sources are absent.  The product never imports it.
 """
 from __future__ import annotations
 
@@ -33,7 +34,8 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF_DIR = Path(os.environ.get("AGB_REFERENCE", "/root/reference"))
+DEFAULT_REFERENCE = "/root/reference"
+REF_DIR = Path(os.environ.get("AGB_REFERENCE", DEFAULT_REFERENCE))
 REF_LIB = HERE / "_ref" / "libref.so"
 
 
@@ -138,9 +140,28 @@ def _run_raw(name, args):
 # ---------------------------------------------------------------------------
 _EW = []          # (name, in_params, out_param, body)
 _ew_lib = None
+_RECORD = None    # list receiving (kernel name, scalar arguments) of each call, when set
+
+
+class record_calls:
+    """Context manager: collect the (name, scalars) of every ElementwiseKernel call
+    the reference's code makes inside the block (the kernel still runs)."""
+
+    def __enter__(self):
+        global _RECORD
+        self.calls = []
+        _RECORD = self.calls
+        return self.calls
+
+    def __exit__(self, *exc):
+        global _RECORD
+        _RECORD = None
+        return False
 
 
 def _ew_source():
+    # one OpenMP loop over points per kernel body, as the reference's kernels
+    # compiled for the host are (ref_driver.cpp)
     out = ["#include <cmath>", "#include <cstdlib>", "using std::abs;", "typedef double T;"]
     for name, ins, outp, body in _EW:
         arrays = ins[:3]
@@ -150,6 +171,7 @@ def _ew_source():
         sig = ", ".join([f"const double* __{a}" for a in arrays] +
                         [f"double {s}" for s in scalars] + [f"double* __{oname}", "long n"])
         lines = [f'extern "C" void ew_{name}({sig}) {{',
+                 "  #pragma omp parallel for schedule(static)",
                  "  for (long i = 0; i < n; i++) {",
                  *[f"    const double {a} = __{a}[i];" for a in arrays]]
         if raw:
@@ -174,7 +196,8 @@ def ew_lib():
             cpp = d / f"ref_analytic_{h}.cpp"
             cpp.write_text(src)
             cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-            subprocess.run([cxx, "-O2", "-fPIC", "-shared", "-o", str(so), str(cpp)], check=True)
+            subprocess.run([cxx, "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-o",
+                            str(so), str(cpp)], check=True)
         _ew_lib = ctypes.CDLL(str(so))
     return _ew_lib
 
@@ -197,6 +220,8 @@ class _EWKernel:
             out = args[n_in]
         else:
             out = np.empty(n, dtype=np.float64)
+        if _RECORD is not None:
+            _RECORD.append((self.name, [float(v) for v in ins[3:]]))
         fn = getattr(ew_lib(), "ew_" + self.name)
         fn(_p(x), _p(y), _p(z), *[_d(s) for s in ins[3:]], _p(out), ctypes.c_long(n))
         return out
@@ -205,11 +230,32 @@ class _EWKernel:
 # ---------------------------------------------------------------------------
 # numpy-backed cupy stand-in
 # ---------------------------------------------------------------------------
+_RAW_RECORD = None    # list receiving (kernel name, arguments) of each launch, when set
+
+
+class record_raw:
+    """Context manager: collect the (name, arguments) of every RawKernel launch the
+    reference's code makes inside the block (the kernel still runs)."""
+
+    def __enter__(self):
+        global _RAW_RECORD
+        self.calls = []
+        _RAW_RECORD = self.calls
+        return self.calls
+
+    def __exit__(self, *exc):
+        global _RAW_RECORD
+        _RAW_RECORD = None
+        return False
+
+
 class _RawKernel:
     def __init__(self, name):
         self.name = name
 
     def __call__(self, grid, block, args):
+        if _RAW_RECORD is not None:
+            _RAW_RECORD.append((self.name, tuple(args)))
         _run_raw(self.name, args)
 
 

@@ -16,7 +16,7 @@ Each case stores its inputs (coefficient arrays, parameters, points), the
 reference's tables and the reference's API outputs (potential, force,
 forceDeriv, density).  Usage (needs the reference sources):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference checkout>]
 """
 from __future__ import annotations
 
@@ -165,10 +165,13 @@ def composite_case(gp, ap, out):
 
 def main():
     ap_ = argparse.ArgumentParser()
-    ap_.add_argument("--reference", default=os.environ.get("AGB_REFERENCE", "/root/reference"))
+    ap_.add_argument("--reference", default=None,
+                     help="reference checkout (default: AGB_REFERENCE, else oracle.refpy's)")
     args = ap_.parse_args()
-    os.environ["AGB_REFERENCE"] = args.reference
+    if args.reference:
+        os.environ["AGB_REFERENCE"] = args.reference
     from oracle import refpy
+    args.reference = str(refpy.REF_DIR)
     from agama_gpu_b200.coefs import read_coefs
     from agama_gpu_b200.synthetic import bar_cylspline, disk_points, nfw_multipole
     gp, ap = refpy.load()

@@ -2,7 +2,8 @@
 import numpy as np
 import pytest
 
-from conftest import REF_DIR, reference_available
+from conftest import reference_available
+from oracle.refpy import REF_DIR
 from agama_gpu_b200.coefs import CylSplineCoefs, MultipoleCoefs, read_coefs, write_coefs
 from agama_gpu_b200.synthetic import bar_cylspline, nfw_multipole
 

@@ -75,6 +75,24 @@ def test_no_alloc_entry_matches_agb_eval_twice():
             assert float((a - b).abs().max()) <= 1e-14 * float(b.abs().max())
 
 
+def test_no_alloc_entry_at_its_maximum_size():
+    """One call of exactly AGB_STATIC_MAX_POINTS points through an lmax-32, 100-node
+    Multipole (interval sort on, the most bins): the sort scratch of the largest
+    allowed call fits the fixed array, and the results equal agb_eval's."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    pot = agb.MultipolePotentialGPU(nfw_multipole(lmax=32, n_nodes=100, seed=9))
+    x = torch.from_numpy(hernquist_points(MAX_POINTS, 10.0, 73)).cuda()
+    L = _lib.lib
+    ref = _run(L.agb_eval, pot, x, 0.0, _lib.MODE_GRAD, _lib.PREC_MIXED)
+    got = _run(L.agb_eval_static, pot, x, 0.0, _lib.MODE_GRAD, _lib.PREC_MIXED)
+    for a, b in zip(got[:2], ref[:2]):
+        assert not torch.isnan(a).any()
+        assert float((a - b).abs().max()) <= 1e-14 * float(b.abs().max())
+
+
 def test_no_alloc_entry_rejects_too_many_points():
     import torch
     from agama_gpu_b200 import _lib
