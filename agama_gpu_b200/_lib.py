@@ -73,6 +73,21 @@ class AgbLeaf(ctypes.Structure):
     ]
 
 
+MAX_LEAF_OPS = 6
+OP_SHIFT, OP_SCALE, OP_EVOLVE = 1, 2, 3
+
+
+class AgbLeafProg(ctypes.Structure):
+    _fields_ = [
+        ("comp", ctypes.c_int32),
+        ("n_ops", ctypes.c_int32),
+        ("op", ctypes.c_int32 * MAX_LEAF_OPS),
+        ("arg", ctypes.c_int32 * MAX_LEAF_OPS),
+        ("slot", ctypes.c_int32),
+        ("pair", ctypes.c_int32),
+    ]
+
+
 def _load():
     if not LIB_PATH.exists():
         raise ImportError(
@@ -159,6 +174,32 @@ def _load():
     lib.agb_batch_tiles.argtypes = [ctypes.c_void_p]
     lib.agb_batch_destroy.restype = None
     lib.agb_batch_destroy.argtypes = [ctypes.c_void_p]
+    lib.agb_time_plan_create.restype = ctypes.c_int
+    lib.agb_time_plan_create.argtypes = [ctypes.POINTER(AgbLeafProg), ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_void_p)]
+    lib.agb_time_plan_destroy.restype = None
+    lib.agb_time_plan_destroy.argtypes = [ctypes.c_void_p]
+    lib.agb_time_plan_leaves_host.restype = ctypes.c_int
+    lib.agb_time_plan_leaves_host.argtypes = [ctypes.c_void_p, ctypes.c_double,
+                                              ctypes.POINTER(AgbLeaf)]
+    lib.agb_time_plan_leaves.restype = ctypes.c_int
+    lib.agb_time_plan_leaves.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                         ctypes.c_void_p]
+    lib.agb_eval_timed_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_eval_timed_workspace_bytes.argtypes = [ctypes.POINTER(AgbComponent), ctypes.c_int,
+                                                   ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]
+    lib.agb_eval_timed.restype = ctypes.c_int
+    lib.agb_eval_timed.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.agb_leapfrog_kick_drift.restype = ctypes.c_int
+    lib.agb_leapfrog_kick_drift.argtypes = [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+        ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     return lib
 
 
@@ -172,7 +213,9 @@ EXPORTED = [
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
     "agb_multipole_adjoint", "agb_cylspline_table_vjp", "agb_adjoint_kick", "agb_reverse_drift",
     "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
-    "agb_batch_destroy",
+    "agb_batch_destroy", "agb_time_plan_create", "agb_time_plan_destroy",
+    "agb_time_plan_leaves_host", "agb_time_plan_leaves", "agb_eval_timed_workspace_bytes",
+    "agb_eval_timed", "agb_leapfrog_kick_drift",
     "agb_multipole_potential", "agb_multipole_force", "agb_multipole_hess",
     "agb_multipole_density", "agb_cylspl_potential", "agb_cylspl_force", "agb_cylspl_hess",
 ]

@@ -59,6 +59,7 @@ struct EvalArgs {
     const int* dest;         // binned calls: sorted position of input point i
     const double* gphi;      // VJP mode: dL/dPhi [N] (may be null)
     const double* gforce;    // VJP mode: dL/dF [N,3] (may be null)
+    const DevLeaf* dleaves;  // leaves in device memory (agb_eval_timed), else null
     DevComp comps[AGB_MAX_COMPONENTS];
     DevLeaf leaves[AGB_MAX_LEAVES];
 };

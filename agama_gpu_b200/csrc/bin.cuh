@@ -25,6 +25,7 @@
 
 struct BinKey {
     double sigma, g0, g1, g2;     // frame of the keyed Multipole leaf
+    const DevLeaf* leaf;          // or, when set, that leaf in device memory
     double logr_min, inv_dlogr;
     int n_int;
     // Output blocks: the key of point i is (i >> log_block) * (n_int + 2) + its
@@ -53,6 +54,10 @@ bin_count(const double* __restrict__ xyz, long long n, int tile, BinKey b, int n
           int* __restrict__ keys, int* __restrict__ counts)
 {
     extern __shared__ int hist[];
+    if (b.leaf) {                 // the leaf's frame at this call's time (agb_eval_timed)
+        b.sigma = b.leaf->sigma;
+        b.g0 = b.leaf->g0; b.g1 = b.leaf->g1; b.g2 = b.leaf->g2;
+    }
     for (int q = threadIdx.x; q < n_bins; q += blockDim.x) hist[q] = 0;
     __syncthreads();
     const long long lo = (long long)blockIdx.x * tile;

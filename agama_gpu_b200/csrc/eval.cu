@@ -24,6 +24,7 @@
 #include "mp_grad.cuh"
 #include "cs_grad.cuh"
 #include "adjoint_steps.cuh"
+#include "time_plan.cuh"
 
 // ---------------------------------------------------------------------------
 // errors and launch accounting
@@ -88,6 +89,10 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 // internal mode of agb_eval_vjp_force: the VJP plus the force of the same leaves
 // (written to the `hess` pointer as [N,3]) from the same per-point sums
 #define AGB_MODE_VJPF 5
+// threads per block of the wide (mixed-precision) fused Multipole adjoint
+#ifndef AGB_ADJ_WIDE_THREADS
+#define AGB_ADJ_WIDE_THREADS 384
+#endif
 
 __host__ __device__ constexpr int stage_rec(int mode)
 {
@@ -128,7 +133,10 @@ unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage,
 // with up to 255 registers beats two blocks with heavy spilling.
 // analytic-only Hessian modes: 3 blocks per SM (80 registers) measured 1.2 % faster per
 // backward leapfrog step than 2 (and than 4, which spills more)
-template <int MODE, typename R, bool AN = false>
+// DYN: the leaves come from device memory (agb_eval_timed: computed by
+// time_leaves_kernel from a device-resident time), copied to shared memory once
+// per block; otherwise they are kernel parameters.
+template <int MODE, typename R, bool AN = false, bool DYN = false>
 __global__ void __launch_bounds__(256, ((MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP ||
                                        MODE == AGB_MODE_VJPF) && !AN) ? 1 : (AN ? 3 : 2))
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
@@ -136,6 +144,11 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
     // the VJP modes evaluate every component with its Hessian and contract at the end
     constexpr bool VJP = MODE == AGB_MODE_VJP || MODE == AGB_MODE_VJPF;
     constexpr int CM = VJP ? AGB_MODE_HESS : MODE;
+    __shared__ DevLeaf dyn_leaves[DYN ? AGB_MAX_LEAVES : 1];
+    if (DYN) {
+        for (int q = threadIdx.x; q < a.n_leaves; q += blockDim.x) dyn_leaves[q] = a.dleaves[q];
+        __syncthreads();
+    }
     // a contiguous range of (interval-sorted) points per block: consecutive
     // iterations of a block reuse the same interval's table records from L1
     const long long lo = (long long)blockIdx.x * a.chunk;
@@ -151,7 +164,7 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
         double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
         double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int L = 0; L < a.n_leaves; ++L) {
-            const DevLeaf& lf = a.leaves[L];
+            const DevLeaf& lf = DYN ? dyn_leaves[L] : a.leaves[L];
             const DevComp& c = a.comps[lf.comp];
             const double lx = lf.sigma * x - lf.g0;
             const double ly = lf.sigma * y - lf.g1;
@@ -160,7 +173,7 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
                 std::is_same<R, float>::value && lf.pad == 1) {
                 // this leaf and the next share grid, columns and transform (pack_args);
                 // FP32 walks only (the FP64 walk holds twice the state and would spill)
-                const DevLeaf& lf2 = a.leaves[L + 1];
+                const DevLeaf& lf2 = DYN ? dyn_leaves[L + 1] : a.leaves[L + 1];
                 PointOut o1, o2;
                 o1.phi = o2.phi = 0.0;
                 o1.g[0] = o1.g[1] = o1.g[2] = 0.0;
@@ -307,11 +320,11 @@ static int grid_for(long long n)
 static int default_waves(long long n) { return n > (1LL << 21) ? 1 : 2; }
 
 // resident blocks per SM of one instantiation
-template <int MODE, typename R, bool AN>
+template <int MODE, typename R, bool AN, bool DYN = false>
 static int eval_blocks_per_sm()
 {
     static std::atomic<int> per_sm[AGB_MAX_DEVICES];
-    return blocks_per_sm(per_sm, agb_eval_kernel<MODE, R, AN>, 256);
+    return blocks_per_sm(per_sm, agb_eval_kernel<MODE, R, AN, DYN>, 256);
 }
 
 // points that one wave of resident threads holds (one point per thread)
@@ -321,16 +334,16 @@ static long long eval_wave_points()
     return (long long)num_sms() * eval_blocks_per_sm<MODE, R, AN>() * 256;
 }
 
-template <int MODE, typename R, bool AN = false>
+template <int MODE, typename R, bool AN = false, bool DYN = false>
 static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
-    const int per_sm = eval_blocks_per_sm<MODE, R, AN>();
+    const int per_sm = eval_blocks_per_sm<MODE, R, AN, DYN>();
     const long long want = (a.n + 255) / 256;
     const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
     const long long slots = (long long)num_sms() * per_sm * (w ? w : default_waves(a.n));
     const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
     a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
-    agb_eval_kernel<MODE, R, AN><<<(int)grid, 256, 0, st>>>(a);
+    agb_eval_kernel<MODE, R, AN, DYN><<<(int)grid, 256, 0, st>>>(a);
 }
 
 static bool analytic_only(const EvalArgs& a)
@@ -369,6 +382,16 @@ static int launch_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
 static int launch_eval_mode(int mode, int precision, EvalArgs& a, cudaStream_t st)
 {
     const bool mixed = precision == AGB_PREC_MIXED;
+    if (a.dleaves) {        // leaves computed on the device (agb_eval_timed)
+        switch (mode) {
+        case AGB_MODE_POT:  mixed ? launch_eval<AGB_MODE_POT, float, false, true>(a, st)  : launch_eval<AGB_MODE_POT, double, false, true>(a, st); break;
+        case AGB_MODE_GRAD: mixed ? launch_eval<AGB_MODE_GRAD, float, false, true>(a, st) : launch_eval<AGB_MODE_GRAD, double, false, true>(a, st); break;
+        case AGB_MODE_HESS: mixed ? launch_eval<AGB_MODE_HESS, float, false, true>(a, st) : launch_eval<AGB_MODE_HESS, double, false, true>(a, st); break;
+        case AGB_MODE_DENS: mixed ? launch_eval<AGB_MODE_DENS, float, false, true>(a, st) : launch_eval<AGB_MODE_DENS, double, false, true>(a, st); break;
+        default: return set_err(AGB_ERR_ARG, "agb_eval_timed: mode %d is not supported", mode);
+        }
+        return check_launch("agb_eval_kernel");
+    }
     switch (mode) {
     case AGB_MODE_POT:  mixed ? launch_eval<AGB_MODE_POT, float>(a, st)  : launch_eval<AGB_MODE_POT, double>(a, st); break;
     case AGB_MODE_GRAD: mixed ? launch_eval<AGB_MODE_GRAD, float>(a, st) : launch_eval<AGB_MODE_GRAD, double>(a, st); break;
@@ -444,6 +467,7 @@ struct BinPlan {
     bool on;
     BinKey key;
     int n_bins;
+    int leaf;          // the keyed leaf
 };
 
 static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, int n_leaves,
@@ -464,6 +488,7 @@ static BinPlan plan_binning(const agb_component* comps, const agb_leaf* leaves, 
     if (best < 0 || best_lm < 2) return b;
     const agb_component& c = comps[leaves[best].comp];
     b.on = true;
+    b.leaf = best;
     b.key.sigma = leaves[best].sigma;
     b.key.g0 = leaves[best].gamma[0]; b.key.g1 = leaves[best].gamma[1]; b.key.g2 = leaves[best].gamma[2];
     b.key.logr_min = c.p[0];
@@ -746,6 +771,339 @@ extern "C" int agb_eval_ws(const agb_component* comps, int n_comps, const agb_le
 }
 
 // ---------------------------------------------------------------------------
+// time plans: leaves computed on the device from a device-resident step
+// ---------------------------------------------------------------------------
+struct agb_time_plan {
+    int n;
+    int device;
+    agb_leaf_prog progs[AGB_MAX_LEAVES];
+    int max_comp[AGB_MAX_LEAVES];     // largest component index a program can pick
+    int evo_lo[AGB_MAX_LEAVES];       // EVOLVE: first snapshot component (else comp)
+    double* table_dev;
+    double* table_host;
+    int64_t n_table;
+};
+
+static bool tp_increasing(const double* x, int n)
+{
+    for (int i = 1; i < n; ++i)
+        if (!(x[i] > x[i - 1])) return false;
+    return true;
+}
+
+// size in doubles of an op's data block (0: malformed), checked against the table
+static int64_t tp_op_size(int op, const double* d, int64_t avail)
+{
+    if (avail < 1) return 0;
+    if (op == AGB_OP_SHIFT) {
+        if (d[0] == 0.0) return avail >= 4 ? 4 : 0;
+        if (d[0] != 1.0 || avail < 16) return 0;
+        const double T = d[1];
+        if (!(T >= 2.0 && T <= 1.0e7) || T != (double)(int64_t)T) return 0;
+        const int64_t need = 16 + (int64_t)T + 12 * ((int64_t)T - 1);
+        if (need > avail || !tp_increasing(d + 16, (int)T)) return 0;
+        return need;
+    }
+    if (op == AGB_OP_SCALE) {
+        if (d[0] == 0.0) return (avail >= 3 && d[1] != 0.0) ? 3 : 0;
+        if (d[0] != 1.0 || avail < 14) return 0;
+        const double T = d[1];
+        if (!(T >= 2.0 && T <= 1.0e7) || T != (double)(int64_t)T) return 0;
+        if (d[8] != 0.0 && d[8] != 1.0) return 0;
+        const int64_t need = 14 + (int64_t)T + 4 * ((int64_t)T - 1) * (d[8] != 0.0 ? 2 : 1);
+        if (need > avail || !tp_increasing(d + 14, (int)T)) return 0;
+        return need;
+    }
+    if (op == AGB_OP_EVOLVE) {
+        if (avail < 3) return 0;
+        const double n = d[0];
+        if (!(n >= 1.0 && n <= 1.0e6) || n != (double)(int64_t)n) return 0;
+        if (d[1] != 0.0 && d[1] != 1.0) return 0;
+        const int64_t need = 2 + (int64_t)n;
+        if (need > avail || !tp_increasing(d + 2, (int)n)) return 0;
+        return need;
+    }
+    return 0;
+}
+
+extern "C" int agb_time_plan_create(const agb_leaf_prog* progs, int n_progs, const double* table,
+                                    int64_t n_table, agb_time_plan** out)
+{
+    if (!out) return set_err(AGB_ERR_ARG, "agb_time_plan_create: out is null");
+    *out = nullptr;
+    if (!progs || n_progs < 1 || n_progs > AGB_MAX_LEAVES)
+        return set_err(AGB_ERR_ARG, "agb_time_plan_create: %d programs (1..%d)", n_progs, AGB_MAX_LEAVES);
+    if (n_table < 0 || (n_table > 0 && !table))
+        return set_err(AGB_ERR_ARG, "agb_time_plan_create: bad table");
+    agb_time_plan* p = (agb_time_plan*)calloc(1, sizeof(agb_time_plan));
+    if (!p) return set_err(AGB_ERR_DEVICE, "agb_time_plan_create: out of host memory");
+    p->n = n_progs;
+    for (int i = 0; i < n_progs; ++i) {
+        const agb_leaf_prog& g = progs[i];
+        int evolves = 0, maxc = g.comp;
+        if (g.comp < 0 || g.n_ops < 0 || g.n_ops > AGB_MAX_LEAF_OPS || g.slot < 0 || g.slot > 1) {
+            free(p);
+            return set_err(AGB_ERR_ARG, "agb_time_plan_create: program %d: bad comp, op count or slot", i);
+        }
+        for (int k = 0; k < g.n_ops; ++k) {
+            const int64_t at = g.arg[k];
+            const int64_t sz = (at >= 0 && at < n_table) ? tp_op_size(g.op[k], table + at, n_table - at) : 0;
+            if (sz == 0) {
+                free(p);
+                return set_err(AGB_ERR_ARG, "agb_time_plan_create: program %d op %d (kind %d) has "
+                               "malformed table data at %lld", i, k, g.op[k], (long long)at);
+            }
+            if (g.op[k] == AGB_OP_EVOLVE) {
+                const int n = (int)table[at];
+                const bool interp = table[at + 1] != 0.0;
+                if (++evolves > 1 || (g.slot == 1 && (!interp || n < 2))) {
+                    free(p);
+                    return set_err(AGB_ERR_ARG, "agb_time_plan_create: program %d: one EVOLVE op "
+                                   "at most, slot 1 needs interpolation of >= 2 snapshots", i);
+                }
+                maxc = g.comp + n - 1;
+            }
+        }
+        p->progs[i] = g;
+        p->progs[i].pair = 0;           // decided per call (agb_eval_timed)
+        p->max_comp[i] = maxc;
+    }
+    p->n_table = n_table;
+    const size_t bytes = sizeof(double) * (size_t)(n_table > 0 ? n_table : 1);
+    p->table_host = (double*)malloc(bytes);
+    if (!p->table_host) {
+        free(p);
+        return set_err(AGB_ERR_DEVICE, "agb_time_plan_create: out of host memory");
+    }
+    if (n_table > 0) memcpy(p->table_host, table, bytes);
+    // without any CUDA device the plan serves agb_time_plan_leaves_host only
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev < 1) {
+        cudaGetLastError();
+        p->device = -1;
+        *out = p;
+        return AGB_OK;
+    }
+    cudaGetDevice(&p->device);
+    if (cudaMalloc(&p->table_dev, bytes) != cudaSuccess) {
+        free(p->table_host);
+        free(p);
+        return set_err(AGB_ERR_DEVICE, "agb_time_plan_create: cannot allocate %zu bytes", bytes);
+    }
+    if (n_table > 0) {
+        if (cudaMemcpy(p->table_dev, table, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(p->table_dev);
+            free(p->table_host);
+            free(p);
+            return set_err(AGB_ERR_DEVICE, "agb_time_plan_create: upload of the table failed");
+        }
+    }
+    *out = p;
+    return AGB_OK;
+}
+
+extern "C" void agb_time_plan_destroy(agb_time_plan* p)
+{
+    if (!p) return;
+    if (p->table_dev) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cur != p->device) cudaSetDevice(p->device);
+        cudaFree(p->table_dev);
+        if (cur != p->device) cudaSetDevice(cur);
+    }
+    free(p->table_host);
+    free(p);
+}
+
+extern "C" int agb_time_plan_leaves_host(const agb_time_plan* p, double t, agb_leaf* leaves)
+{
+    if (!p || !leaves) return set_err(AGB_ERR_ARG, "agb_time_plan_leaves_host: null argument");
+    for (int i = 0; i < p->n; ++i) {
+        DevLeaf o;
+        tp_leaf(p->progs[i], p->table_host, t, o);
+        leaves[i].comp = o.comp;
+        leaves[i].reserved = 0;
+        leaves[i].sigma = o.sigma;
+        leaves[i].gamma[0] = o.g0; leaves[i].gamma[1] = o.g1; leaves[i].gamma[2] = o.g2;
+        leaves[i].ampl = o.ampl;
+    }
+    return AGB_OK;
+}
+
+static int launch_time_leaves(const agb_time_plan* p, const int* pair, const int64_t* step,
+                              double t0, double dt, double off, DevLeaf* out, cudaStream_t st)
+{
+    static thread_local TimeLeafArgs ta;
+    memset(&ta, 0, sizeof(ta));
+    ta.n = p->n;
+    for (int i = 0; i < p->n; ++i) {
+        ta.progs[i] = p->progs[i];
+        ta.progs[i].pair = pair ? pair[i] : 0;
+    }
+    ta.table = p->table_dev;
+    ta.step = (const long long*)step;
+    ta.t0 = t0; ta.dt = dt; ta.off = off;
+    ta.out = out;
+    time_leaves_kernel<<<1, 32, 0, st>>>(ta);
+    return check_launch("time_leaves_kernel");
+}
+
+extern "C" int agb_time_plan_leaves(const agb_time_plan* p, const int64_t* step, double t0,
+                                    double dt, double off, agb_leaf* leaves_dev, void* stream)
+{
+    if (!p || !leaves_dev) return set_err(AGB_ERR_ARG, "agb_time_plan_leaves: null argument");
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device)
+        return set_err(AGB_ERR_ARG, "agb_time_plan_leaves: plan lives on device %d, current is %d",
+                       p->device, cur);
+    static_assert(sizeof(agb_leaf) == sizeof(DevLeaf), "agb_leaf and DevLeaf must share a layout");
+    return launch_time_leaves(p, nullptr, step, t0, dt, off, (DevLeaf*)leaves_dev,
+                              (cudaStream_t)stream);
+}
+
+// The component a program uses at any time, as a static leaf (for validation and
+// for choosing the sort key: an EVOLVE program stands for its first snapshot).
+static void tp_template_leaves(const agb_time_plan* p, agb_leaf* lv)
+{
+    for (int i = 0; i < p->n; ++i) {
+        memset(&lv[i], 0, sizeof(agb_leaf));
+        lv[i].comp = p->progs[i].comp;
+        lv[i].sigma = 1.0;
+        lv[i].ampl = 1.0;
+    }
+}
+
+static bool tp_same_ops(const agb_leaf_prog& a, const agb_leaf_prog& b)
+{
+    if (a.n_ops != b.n_ops || a.comp != b.comp) return false;
+    for (int k = 0; k < a.n_ops; ++k)
+        if (a.op[k] != b.op[k] || a.arg[k] != b.arg[k]) return false;
+    return true;
+}
+
+// one harmonic walk may serve programs L and L+1 (the two slots of one Evolving):
+// the same modifier chain, and every snapshot a Multipole of one grid and column
+// structure with an FP32 table
+static void tp_pairs(const agb_time_plan* p, const agb_component* comps, int precision, int* pair)
+{
+    for (int i = 0; i < p->n; ++i) pair[i] = 0;
+    if (precision != AGB_PREC_MIXED) return;
+    for (int L = 0; L + 1 < p->n; ++L) {
+        const agb_leaf_prog& a = p->progs[L];
+        const agb_leaf_prog& b = p->progs[L + 1];
+        if (!tp_same_ops(a, b) || a.slot != 0 || b.slot != 1 || p->max_comp[L] == a.comp) continue;
+        const agb_component& c0 = comps[a.comp];
+        bool ok = c0.kind == AGB_KIND_MULTIPOLE &&
+                  (c0.structure == AGB_STRUCT_EVEN || c0.structure == AGB_STRUCT_ALL);
+        for (int c = a.comp + 1; ok && c <= p->max_comp[L]; ++c) {
+            const agb_component& q = comps[c];
+            ok = q.kind == AGB_KIND_MULTIPOLE && q.structure == c0.structure &&
+                 q.lmax == c0.lmax && q.n_lm == c0.n_lm && q.n_int == c0.n_int &&
+                 q.layout == c0.layout && q.p[0] == c0.p[0] && q.p[1] == c0.p[1] &&
+                 q.p[2] == c0.p[2] && q.table32 != nullptr;
+        }
+        ok = ok && c0.table32 != nullptr;
+        if (ok) {
+            pair[L] = 1;
+            ++L;
+        }
+    }
+}
+
+static const size_t TP_LEAF_BYTES = 256 * ((sizeof(DevLeaf) * AGB_MAX_LEAVES + 255) / 256);
+
+extern "C" size_t agb_eval_timed_workspace_bytes(const agb_component* comps, int n_comps,
+                                                 const agb_time_plan* p, int64_t n, int out_flags)
+{
+    if (!comps || !p || n_comps < 1) return 0;
+    for (int i = 0; i < p->n; ++i)
+        if (p->max_comp[i] >= n_comps) return 0;
+    agb_leaf lv[AGB_MAX_LEAVES];
+    tp_template_leaves(p, lv);
+    return TP_LEAF_BYTES + ws_bytes_staged(plan_binning(comps, lv, p->n, n, out_flags), n);
+}
+
+extern "C" int agb_eval_timed(const agb_component* comps, int n_comps, const agb_time_plan* p,
+                              const int64_t* step, double t0, double dt, double off,
+                              const double* xyz, int64_t n, int mode, int precision, double* phi,
+                              double* grad, double* hess, double* rho, int out_flags,
+                              void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (!p) return set_err(AGB_ERR_ARG, "agb_eval_timed: plan is null");
+    if (mode != AGB_MODE_POT && mode != AGB_MODE_GRAD && mode != AGB_MODE_HESS &&
+        mode != AGB_MODE_DENS)
+        return set_err(AGB_ERR_ARG, "agb_eval_timed: mode %d is not supported", mode);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device)
+        return set_err(AGB_ERR_ARG, "agb_eval_timed: plan lives on device %d, current is %d",
+                       p->device, cur);
+    for (int i = 0; i < p->n; ++i)
+        if (p->max_comp[i] >= n_comps)
+            return set_err(AGB_ERR_ARG, "agb_eval_timed: program %d uses component %d of %d", i,
+                           p->max_comp[i], n_comps);
+    if (n_comps > AGB_MAX_COMPONENTS)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_eval_timed: more than %d components",
+                       AGB_MAX_COMPONENTS);
+    agb_leaf lv[AGB_MAX_LEAVES];
+    tp_template_leaves(p, lv);
+    int rc = validate(comps, n_comps, lv, p->n, xyz, n, mode, precision, phi, grad, hess, rho);
+    if (rc) return rc;
+    if (n == 0) return AGB_OK;
+    if (!workspace || ((uintptr_t)workspace & 255u) || workspace_bytes < TP_LEAF_BYTES)
+        return set_err(AGB_ERR_ARG, "agb_eval_timed: workspace of at least "
+                       "agb_eval_timed_workspace_bytes() bytes, 256-byte aligned, is required");
+    cudaStream_t st = (cudaStream_t)stream;
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n; a.out_flags = out_flags; a.soa = 0; a.xyz = xyz; a.perm = nullptr;
+    a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    for (int c = 0; c < n_comps; ++c)
+        if ((rc = comp_to_dev(comps[c], a.comps[c], precision))) return rc;
+    a.n_leaves = p->n;
+    DevLeaf* dl = (DevLeaf*)workspace;
+    a.dleaves = dl;
+    int pair[AGB_MAX_LEAVES];
+    tp_pairs(p, comps, precision, pair);
+    if ((rc = launch_time_leaves(p, pair, step, t0, dt, off, dl, st))) return rc;
+    char* ws = (char*)workspace + TP_LEAF_BYTES;
+    const size_t room = workspace_bytes - TP_LEAF_BYTES;
+    BinPlan b = plan_binning(comps, lv, p->n, n, out_flags);
+    if (b.on) {
+        b.key.leaf = dl + b.leaf;
+        const size_t staged = ws_bytes_staged(b, n);
+        const size_t need = ws_bytes(b, n);
+        if (room < need)
+            return set_err(AGB_ERR_ARG, "agb_eval_timed: workspace of %zu bytes is smaller than "
+                           "the %zu bytes agb_eval_timed_workspace_bytes asks for",
+                           workspace_bytes, need + TP_LEAF_BYTES);
+        if ((rc = run_binning(a, b, xyz, n, ws, st))) return rc;
+        if (room >= staged) {
+            a.stage = (double*)(ws + ws_bytes(b, n));
+            a.dest = (const int*)ws;
+        }
+    }
+    return launch_mode(mode, precision, a, st);
+}
+
+extern "C" int agb_leapfrog_kick_drift(double* x, double* v, const double* F, int64_t n,
+                                       double h1, double h2, double dt, int flags, int64_t* step,
+                                       void* stream)
+{
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_leapfrog_kick_drift: negative count");
+    if (flags & ~15) return set_err(AGB_ERR_ARG, "agb_leapfrog_kick_drift: unknown flags %d", flags);
+    if ((flags & 8) && !step) return set_err(AGB_ERR_ARG, "agb_leapfrog_kick_drift: step is null");
+    if (n == 0 && !(flags & 8)) return AGB_OK;
+    if (n > 0 && (!x || !v || !F)) return set_err(AGB_ERR_ARG, "agb_leapfrog_kick_drift: null array");
+    const long long m = 3LL * n;
+    kick_drift_kernel<<<grid_for(m > 0 ? m : 1), 256, 0, (cudaStream_t)stream>>>(
+        x, v, F, m, h1, h2, dt, flags, (long long*)step);
+    return check_launch("kick_drift_kernel");
+}
+
+// ---------------------------------------------------------------------------
 // gradient w.r.t. one Multipole leaf's quintic coefficients
 // ---------------------------------------------------------------------------
 extern "C" size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* comp,
@@ -854,20 +1212,29 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
         g.perm = tmp.perm;
     }
     if (!rc) {
-        // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
-        const int grid = (int)std::min<long long>((long long)num_sms() * 2, (n + 255) / 256);
-        const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
-        g.chunk = ((groups + warps - 1) / warps) * 32;
+        // per warp: the (U, V) tile, plus the interval accumulator when all warps' fit.
+        // The mixed walk runs 12 warps per block (168 registers) when their tiles and
+        // accumulators fit in shared memory, else 8 (255 registers) like FP64.
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
         const size_t acc = (size_t)g.c.n_lm * 6 * sizeof(double);
-        int dev = 0, optin = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        int optin = 0;
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                   current_device()) != cudaSuccess)
             optin = 48 * 1024;
-        g.staged = (size_t)8 * (tile + acc) <= (size_t)optin;
+        const int wide = AGB_ADJ_WIDE_THREADS / 32;
+        const bool use_wide = precision == AGB_PREC_MIXED && AGB_ADJ_WIDE_THREADS > 256 &&
+                              (size_t)wide * (tile + acc) <= (size_t)optin;
+        const int wpb = use_wide ? wide : 8;
+        const int threads = wpb * 32;
+        const int grid = (int)std::min<long long>((long long)num_sms() * (use_wide ? 1 : 2),
+                                                  (n + threads - 1) / threads);
+        const long long warps = (long long)grid * wpb, groups = (n + 31) / 32;
+        g.chunk = ((groups + warps - 1) / warps) * 32;
+        g.staged = (size_t)wpb * (tile + acc) <= (size_t)optin;
         g.warp_smem = g.staged ? (int)(tile + acc) : tile;
-        const size_t smem = (size_t)8 * g.warp_smem;
-        const void* fn = precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
+        const size_t smem = (size_t)wpb * g.warp_smem;
+        const void* fn = use_wide ? (const void*)mp_adjoint_kernel<float, AGB_ADJ_WIDE_THREADS>
+                       : precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
                                                      : (const void*)mp_adjoint_kernel<double>;
         if (smem > (size_t)optin)
             rc = set_err(AGB_ERR_UNSUPPORTED, "agb_multipole_adjoint: needs %zu bytes of shared "
@@ -877,7 +1244,8 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
             rc = set_err(AGB_ERR_DEVICE, "agb_multipole_adjoint: cannot reserve %zu bytes of shared "
                          "memory", smem);
         if (!rc) {
-            if (precision == AGB_PREC_MIXED) mp_adjoint_kernel<float><<<grid, 256, smem, st>>>(g);
+            if (use_wide) mp_adjoint_kernel<float, AGB_ADJ_WIDE_THREADS><<<grid, threads, smem, st>>>(g);
+            else if (precision == AGB_PREC_MIXED) mp_adjoint_kernel<float><<<grid, 256, smem, st>>>(g);
             else mp_adjoint_kernel<double><<<grid, 256, smem, st>>>(g);
             rc = check_launch("mp_adjoint_kernel");
         }

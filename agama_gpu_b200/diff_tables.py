@@ -12,7 +12,7 @@ A grid that had to be resampled to log-uniform is not supported here.
 """
 from __future__ import annotations
 
-from typing import Tuple
+from typing import Optional, Tuple
 
 import numpy as np
 import torch
@@ -77,15 +77,17 @@ def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) 
     return quintic_poly_torch(logr, f, df, float(tables.dlogr))
 
 
-def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int,
+def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: Optional[int],
              nodes=None) -> Tuple[torch.Tensor, torch.Tensor]:
     """Carry dL/dpoly back to the node tables in the coefficient file's column order.
 
     Returns (dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_cols); columns
     the table builder pruned (all-zero) get zero (build with prune_threshold=0
-    to differentiate every harmonic).  ``nodes`` = (phi, dphi_dr) in the builder's
-    order when the tables were replaced on the device (set_node_tables), else the
-    builder's own node values are used.
+    to differentiate every harmonic).  n_file_cols=None returns them in the
+    builder's harmonic order instead, (nR, n_lm) like ``tables.node_phi``.
+    ``nodes`` = (phi, dphi_dr) in the builder's order when the tables were
+    replaced on the device (set_node_tables), else the builder's own node values
+    are used.
     """
     dev = grad_poly.device
     if nodes is None:
@@ -96,6 +98,8 @@ def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: int,
         dphi = nodes[1].detach().to(dev, torch.float64).requires_grad_(True)
     poly = multipole_poly_from_nodes(tables, phi, dphi)
     gphi, gdphi = torch.autograd.grad(poly, (phi, dphi), grad_outputs=grad_poly.to(torch.float64))
+    if n_file_cols is None:
+        return gphi, gdphi
     cols = torch.as_tensor(np.asarray(tables.node_cols), dtype=torch.long, device=dev)
     out_p = torch.zeros((phi.shape[0], n_file_cols), dtype=torch.float64, device=dev)
     out_d = torch.zeros_like(out_p)

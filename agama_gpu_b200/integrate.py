@@ -124,7 +124,8 @@ class Leapfrog:
     """
 
     def __init__(self, pot, dt: float, t0: float = 0.0, precision: Optional[str] = None,
-                 use_graph: Optional[bool] = None, graph_steps: int = 16, scheme="leapfrog"):
+                 use_graph: Optional[bool] = None, graph_steps: int = 16, scheme="leapfrog",
+                 device_time: Optional[bool] = None):
         self.pot = pot
         self.dt = float(dt)
         self.h = 0.5 * self.dt
@@ -141,15 +142,80 @@ class Leapfrog:
             self._sub = sub                 # (dt_j, h_j, end offset within the step)
         self.precision = precision
         self.static = is_static(pot)
-        self.use_graph = self.static if use_graph is None else (use_graph and self.static)
+        self._want_graph = use_graph
+        self._device_time = device_time
+        self._timed_cache = {}
         self.graph_steps = int(graph_steps)
         self._graph = None
         self._graph_key = None
+        self._step_dev = None
+
+    # -- time on the device ----------------------------------------------------------
+    def _timed(self, x: torch.Tensor) -> bool:
+        """Forces of this time-dependent potential come from agb_eval_timed: the
+        leaves are computed on the device from a device step counter, so steps can
+        be captured in CUDA graphs (device_time=False keeps the host leaves)."""
+        if self.static or self._device_time is False or not x.is_cuda:
+            return False
+        hit = self._timed_cache.get(x.device)
+        if hit is None:
+            hit = hasattr(self.pot, "_time_plan") and self.pot._time_plan(x.device) is not None
+            self._timed_cache[x.device] = hit
+        return hit
+
+    def _graphs(self, x: torch.Tensor) -> bool:
+        ok = x.is_cuda and (self.static or self._timed(x))
+        return ok if self._want_graph is None else (bool(self._want_graph) and ok)
+
+    @property
+    def use_graph(self) -> bool:
+        """Whether steps are captured in CUDA graphs (static potentials, and
+        time-dependent ones whose leaves the device evaluates)."""
+        if self._want_graph is False:
+            return False
+        return self.static or any(self._timed_cache.values())
+
+    def _counter(self, x: torch.Tensor) -> torch.Tensor:
+        if self._step_dev is None or self._step_dev.device != x.device:
+            self._step_dev = torch.zeros((), dtype=torch.int64, device=x.device)
+        return self._step_dev
+
+    def _set_step(self, x: torch.Tensor, n: int) -> None:
+        if self._timed(x):
+            self._counter(x).fill_(int(n))
 
     # -- single steps -------------------------------------------------------------
     def _force_into(self, x: torch.Tensor, t: float, F: torch.Tensor) -> None:
         self.pot._launch(x, t, _lib.MODE_GRAD, False, precision=self.precision,
                          out=(None, F, None, None))
+
+    def _force_at(self, x: torch.Tensor, n: int, off: float, F: torch.Tensor) -> None:
+        """F at t = (t0 + n dt) + off: on the device from the step counter (which holds
+        n) when the leaves are device-evaluated, else with the host leaves at t."""
+        if self._timed(x):
+            self.pot._launch_timed(x, self._counter(x), self.t0, self.dt, off, _lib.MODE_GRAD,
+                                   False, precision=self.precision, out=(None, F, None, None))
+        else:
+            self._force_into(x, self.t0 + n * self.dt + off, F)
+
+    def _kd(self, x, v, F, h1: float, h2: float, dt: float, flags: int) -> None:
+        """v = fma(h1, F, v) [1]; v = fma(h2, F, v) [2]; x = fma(dt, v, x) [4]; the
+        device step counter += 1 [8]: one launch (agb_leapfrog_kick_drift) on the GPU,
+        the same updates with torch on the CPU."""
+        if x.is_cuda:
+            step = self._counter(x) if (flags & 8) else None
+            rc = _lib.lib.agb_leapfrog_kick_drift(
+                x.data_ptr(), v.data_ptr(), F.data_ptr(), x.shape[0], h1, h2, dt, flags,
+                None if step is None else step.data_ptr(),
+                torch.cuda.current_stream(x.device).cuda_stream)
+            _lib.check(rc, "agb_leapfrog_kick_drift")
+            return
+        if flags & 1:
+            v.add_(F, alpha=h1)
+        if flags & 2:
+            v.add_(F, alpha=h2)
+        if flags & 4:
+            x.add_(v, alpha=dt)
 
     def _t(self, g: int) -> float:
         """Time at the end of substep g - 1 (= at the start of substep g)."""
@@ -157,60 +223,57 @@ class Leapfrog:
         return self.t0 + n * self.dt + (self._sub[j - 1][2] if j else 0.0)
 
     def _substep(self, x, v, F, g: int) -> None:
-        dtj, hj, off = self._sub[g % self.S]
-        v.add_(F, alpha=hj)
-        x.add_(v, alpha=dtj)
-        self._force_into(x, self.t0 + (g // self.S) * self.dt + off, F)
-        v.add_(F, alpha=hj)
+        n, j = divmod(int(g), self.S)
+        dtj, hj, off = self._sub[j]
+        self._kd(x, v, F, 0.0, hj, dtj, 6)
+        self._force_at(x, n, off, F)
+        inc = 8 if (j == self.S - 1 and self._timed(x)) else 0
+        self._kd(x, v, F, hj, 0.0, 0.0, 1 | inc)
 
-    def _step(self, x, v, F, t) -> None:
-        """One step from time t (all S substeps)."""
-        if self.S == 1:
-            v.add_(F, alpha=self.h)
-            x.add_(v, alpha=self.dt)
-            self._force_into(x, t + self.dt, F)
-            v.add_(F, alpha=self.h)
-            return
-        for dtj, hj, off in self._sub:
-            v.add_(F, alpha=hj)
-            x.add_(v, alpha=dtj)
-            self._force_into(x, t + off, F)
-            v.add_(F, alpha=hj)
+    def _step(self, x, v, F, n: int) -> None:
+        """One step from step index n, time t0 + n dt (all S substeps); with device
+        leaves the step counter must hold n and ends at n + 1."""
+        for g in range(int(n) * self.S, (int(n) + 1) * self.S):
+            self._substep(x, v, F, g)
 
     def _advance(self, x, v, F, n0: int, n_steps: int) -> None:
         """n_steps steps from step index n0 (time t0 + n0 dt)."""
         if n_steps <= 0:
             return
-        if not self.use_graph:
+        self._set_step(x, n0)
+        if not self._graphs(x):
             for k in range(n_steps):
-                self._step(x, v, F, self.t0 + (n0 + k) * self.dt)
+                self._step(x, v, F, n0 + k)
             return
         key = (x.data_ptr(), v.data_ptr(), F.data_ptr(), x.shape[0],
                getattr(self.pot, "plan_generation", 0))
         if self._graph is None or self._graph_key != key:
-            self._capture(x, v, F)
+            self._capture(x, v, F, n0)
             self._graph_key = key
         full, rest = divmod(n_steps, self.graph_steps)
         for _ in range(full):
-            self._graph.replay()
+            self._graph.replay()        # advances the device step counter itself
         for k in range(rest):
-            self._step(x, v, F, self.t0)          # static potential: t does not matter
+            self._step(x, v, F, n0 + full * self.graph_steps + k)
 
-    def _capture(self, x, v, F) -> None:
-        # warm-up on a side stream (allocator pools, lazy module loading), then capture
+    def _capture(self, x, v, F, n0: int) -> None:
+        # warm-up on a side stream (allocator pools, lazy module loading), then capture;
+        # x, v, F and the step counter are restored after each
         xs, vs, Fs = x.clone(), v.clone(), F.clone()
         s = torch.cuda.Stream(device=x.device)
         s.wait_stream(torch.cuda.current_stream(x.device))
         with torch.cuda.stream(s):
-            for _ in range(2):
-                self._step(x, v, F, self.t0)
+            for k in range(2):
+                self._step(x, v, F, n0 + k)
         torch.cuda.current_stream(x.device).wait_stream(s)
         x.copy_(xs); v.copy_(vs); F.copy_(Fs)
+        self._set_step(x, n0)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            for _ in range(self.graph_steps):
-                self._step(x, v, F, self.t0)
+            for k in range(self.graph_steps):
+                self._step(x, v, F, n0 + k)
         x.copy_(xs); v.copy_(vs); F.copy_(Fs)
+        self._set_step(x, n0)
         self._graph = g
 
     # -- forward with checkpoints ------------------------------------------------------
@@ -224,7 +287,8 @@ class Leapfrog:
         x, v, F = self._buffers(x0)
         x.copy_(x0.detach())
         v.copy_(v0.detach())
-        self._force_into(x, self.t0, F)
+        self._set_step(x, 0)
+        self._force_at(x, 0, 0.0, F)
         S = self.S
         G = int(n_steps) * S
         if checkpoint_every is None:
@@ -237,14 +301,9 @@ class Leapfrog:
             # every substep's positions in one allocation [substep][particle][3]; the
             # adjoint re-computes nothing and needs no velocities
             store = torch.empty((G + 1,) + tuple(x.shape), dtype=torch.float64, device=x.device)
-            if S == 1:
-                for n in range(n_steps):
-                    store[n].copy_(x)
-                    self._step(x, v, F, self.t0 + n * self.dt)
-            else:
-                for g in range(G):
-                    store[g].copy_(x)
-                    self._substep(x, v, F, g)
+            for g in range(G):
+                store[g].copy_(x)
+                self._substep(x, v, F, g)
             store[G].copy_(x)
             ckpts = [(g, store[g], None) for g in range(G)]
             ckpts.append((G, store[G], v.clone()))
@@ -388,7 +447,9 @@ class Leapfrog:
                 X = torch.empty((last - s,) + tuple(xs.shape), dtype=torch.float64, device=xs.device)
                 x, v = xs.clone(), vs.clone()
                 F = torch.empty_like(x)
-                self._force_into(x, self._t(s), F)
+                n_s, j_s = divmod(s, S)
+                self._set_step(x, n_s)
+                self._force_at(x, n_s, self._sub[j_s - 1][2] if j_s else 0.0, F)
                 for g in range(s, last):
                     self._substep(x, v, F, g)
                     X[g - s].copy_(x)
@@ -407,9 +468,11 @@ class Leapfrog:
 
 class _LeapfrogFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x0, v0, integrator, n_steps, checkpoint_every):
+    def forward(ctx, x0, v0, integrator, n_steps, checkpoint_every, reconstruct, tracked,
+                *nodes):
         x, v, ckpts = integrator.run(x0, v0, n_steps, checkpoint_every)
         ctx.integrator, ctx.n_steps, ctx.ckpts = integrator, n_steps, ckpts
+        ctx.reconstruct, ctx.tracked = reconstruct, tracked
         return x, v
 
     @staticmethod
@@ -418,16 +481,28 @@ class _LeapfrogFn(torch.autograd.Function):
             gx = torch.zeros_like(ctx.ckpts[0][1])
         if gv is None:
             gv = torch.zeros_like(ctx.ckpts[0][1])
-        lx, lv = ctx.integrator.adjoint(ctx.ckpts, ctx.n_steps, gx, gv)
-        return lx, lv, None, None, None
+        integ = ctx.integrator
+        node_grads = [None] * sum(len(p) for _, p in ctx.tracked)
+        if any(ctx.needs_input_grad[7:]):
+            lx, lv, tg = integ.adjoint(ctx.ckpts, ctx.n_steps, gx, gv, table_grads=True,
+                                       reconstruct=ctx.reconstruct)
+            node_grads = integ.pot._node_param_grads(tg, ctx.tracked)
+        else:
+            lx, lv = integ.adjoint(ctx.ckpts, ctx.n_steps, gx, gv, reconstruct=ctx.reconstruct)
+        ctx.ckpts = None
+        return (lx, lv, None, None, None, None, None, *node_grads)
 
 
 def leapfrog(pot, x0: torch.Tensor, v0: torch.Tensor, dt: float, n_steps: int, t0: float = 0.0,
              checkpoint_every: Optional[int] = 64, precision: Optional[str] = None,
-             use_graph: Optional[bool] = None, scheme="leapfrog"):
+             use_graph: Optional[bool] = None, scheme="leapfrog", reconstruct: str = "recompute"):
     """(x_T, v_T) after n_steps steps of ``scheme`` (leapfrog, or a composition of
-    leapfrog substeps such as "yoshida4"); differentiable w.r.t. (x0, v0) through the
-    checkpointed adjoint."""
+    leapfrog substeps such as "yoshida4"); differentiable w.r.t. (x0, v0) and w.r.t.
+    the node tensors of the potential (pot.node_parameters()) through the
+    checkpointed adjoint: loss.backward() fills their .grad (under torch.distributed,
+    summed over the ranks)."""
     integ = Leapfrog(pot, dt, t0=t0, precision=precision, use_graph=use_graph, scheme=scheme)
     k = None if checkpoint_every is None else int(checkpoint_every)
-    return _LeapfrogFn.apply(x0, v0, integ, int(n_steps), k)
+    tracked = pot._tracked_nodes() if hasattr(pot, "_tracked_nodes") else []
+    nodes = [q for _, ps in tracked for q in ps]
+    return _LeapfrogFn.apply(x0, v0, integ, int(n_steps), k, reconstruct, tracked, *nodes)

@@ -107,6 +107,30 @@ def _sq(a: torch.Tensor, single: bool):
 Leaf = Tuple["_Component", float, np.ndarray, float]
 
 
+class _TimePlan:
+    """A device time plan (agb_time_plan) with the components its programs index."""
+
+    def __init__(self, handle, comps, progs, table):
+        self.handle, self.comps, self.progs, self.table = handle, comps, progs, table
+        self._arrays = {}
+
+    def component_array(self, dev):
+        a = self._arrays.get(dev)
+        if a is None:
+            a = (_lib.AgbComponent * len(self.comps))(*[c._device_component(dev) for c in self.comps])
+            self._arrays[dev] = a
+        return a
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib.agb_time_plan_destroy(h)
+            except Exception:       # interpreter shutdown
+                pass
+            self.handle = None
+
+
 class _GPUPotBase:
     """``+`` composition, the evaluation API and the flattening into leaves.
 
@@ -164,6 +188,193 @@ class _GPUPotBase:
             c._device_component(dev)
         done.add(dev)
 
+    # -- time-dependent leaves on the device --------------------------------------
+    def _time_slots(self):
+        """The tree as leaf slots for device-evaluated time dependence: a list of
+        (owner, [components], [(modifier, op kind)] innermost first, slot), where a
+        fixed leaf has one component and an Evolving slot all its snapshots (owner is
+        the Evolving).  None when the tree has a structure the device programs do not
+        cover (an Evolving whose snapshots are not single components)."""
+        if isinstance(self, _Component):
+            return [(None, [self], [], 0)]
+        if isinstance(self, CompositePotentialGPU):
+            out = []
+            for c in self._components:
+                sub = c._time_slots()
+                if sub is None:
+                    return None
+                out.extend(sub)
+            return out
+        if isinstance(self, EvolvingPotentialGPU):
+            if not all(isinstance(q, _Component) for q in self._pots):
+                return None
+            op = [(self, _lib.OP_EVOLVE)]
+            if self._interpolate and len(self._pots) > 1:
+                return [(self, list(self._pots), op, 0), (self, list(self._pots), op, 1)]
+            return [(self, list(self._pots), op, 0)]
+        kind = _lib.OP_SHIFT if isinstance(self, ShiftedPotentialGPU) else _lib.OP_SCALE
+        sub = self._inner._time_slots()
+        if sub is None:
+            return None
+        return [(o, comps, ops + [(self, kind)], sl) for o, comps, ops, sl in sub]
+
+    def _time_data(self) -> np.ndarray:
+        raise NotImplementedError
+
+    def _time_programs(self):
+        """(component list, program array, table) of the device time plan, or None."""
+        slots = self._time_slots()
+        if slots is None or not 0 < len(slots) <= _lib.MAX_LEAVES:
+            return None
+        comps, where = [], {}
+        data, at = [], {}
+        n_data = 0
+        progs = (_lib.AgbLeafProg * len(slots))()
+        for i, (owner, members, ops, sl) in enumerate(slots):
+            key = id(owner) if owner is not None else id(members[0])
+            if key not in where:
+                where[key] = len(comps)
+                comps.extend(members)
+            pg = progs[i]
+            pg.comp = where[key]
+            pg.n_ops = len(ops)
+            pg.slot = sl
+            if len(ops) > _lib.MAX_LEAF_OPS:
+                return None
+            for k, (mod, kind) in enumerate(ops):
+                if id(mod) not in at:
+                    d = np.ascontiguousarray(mod._time_data(), dtype=np.float64)
+                    at[id(mod)] = n_data
+                    data.append(d)
+                    n_data += d.size
+                pg.op[k] = kind
+                pg.arg[k] = at[id(mod)]
+        if len(comps) > _lib.MAX_COMPONENTS:
+            return None
+        table = np.concatenate(data) if data else np.zeros(1)
+        return comps, progs, table
+
+    def _time_plan(self, dev: torch.device):
+        """The device time plan of this tree on dev (cached), or None."""
+        cache = self.__dict__.setdefault("_tplans", {})
+        if dev in cache:
+            return cache[dev]
+        built = self._time_programs()
+        plan = None
+        if built is not None:
+            comps, progs, table = built
+            with torch.cuda.device(dev):
+                h = ctypes.c_void_p()
+                rc = _lib.lib.agb_time_plan_create(progs, len(progs), table.ctypes.data,
+                                                   table.size, ctypes.byref(h))
+                _lib.check(rc, "agb_time_plan_create")
+            plan = _TimePlan(h, comps, progs, table)
+        cache[dev] = plan
+        return plan
+
+    def _launch_timed(self, arr: torch.Tensor, step: Optional[torch.Tensor], t0: float, dt: float,
+                      off: float, mode: int, want_phi: bool, precision: Optional[str] = None,
+                      out=None):
+        """_launch at t = (t0 + step * dt) + off with step a device int64 scalar (None:
+        0), the leaves computed on the device (graph-capturable)."""
+        n = arr.shape[0]
+        dev = arr.device
+        plan = self._time_plan(dev)
+        if plan is None:
+            raise ValueError("this potential tree has no device time plan")
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        self._preload(dev)
+        if not torch.cuda.is_current_stream_capturing():
+            for c in plan.comps:
+                if c.__dict__.get("_node_params"):
+                    c._sync_nodes()
+        carr = plan.component_array(dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        phi = grad = hess = rho = None
+        if out is not None:
+            phi, grad, hess, rho = out
+        else:
+            if mode == _lib.MODE_DENS:
+                rho = torch.empty(n, **f64)
+            else:
+                if want_phi or mode == _lib.MODE_POT:
+                    phi = torch.empty(n, **f64)
+                if mode in (_lib.MODE_GRAD, _lib.MODE_HESS):
+                    grad = torch.empty((n, 3), **f64)
+                if mode == _lib.MODE_HESS:
+                    hess = torch.empty((n, 6), **f64)
+        if n == 0:
+            return phi, grad, hess, rho
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+        flags = self._flags(mode, prec, n)
+        nws = int(_lib.lib.agb_eval_timed_workspace_bytes(carr, len(plan.comps), plan.handle, n,
+                                                          flags))
+        ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = _lib.lib.agb_eval_timed(carr, len(plan.comps), plan.handle, ptr(step), float(t0),
+                                     float(dt), float(off), arr.data_ptr(), n, mode, prec,
+                                     ptr(phi), ptr(grad), ptr(hess), ptr(rho), flags, ws.data_ptr(),
+                                     nws, ctypes.c_void_p(stream))
+        _lib.check(rc, "agb_eval_timed")
+        return phi, grad, hess, rho
+
+    def _time_leaves_host(self, t: float):
+        """The plan's leaves at t by the library's host evaluation of the programs:
+        [(component, sigma, gamma, ampl)] (one per program)."""
+        built = self._time_programs()
+        if built is None:
+            raise ValueError("this potential tree has no device time plan")
+        comps, progs, table = built
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib.agb_time_plan_create(progs, len(progs), table.ctypes.data, table.size,
+                                                 ctypes.byref(h)), "agb_time_plan_create")
+        try:
+            lv = (_lib.AgbLeaf * len(progs))()
+            _lib.check(_lib.lib.agb_time_plan_leaves_host(h, float(t), lv), "agb_time_plan_leaves_host")
+        finally:
+            _lib.lib.agb_time_plan_destroy(h)
+        return [(comps[q.comp], q.sigma, np.array(q.gamma[:]), q.ampl) for q in lv]
+
+    # -- node tables as torch tensors ----------------------------------------
+    def node_parameters(self) -> List[torch.Tensor]:
+        """The node tables of every Multipole and CylSpline in the tree as leaf tensors
+        with requires_grad (each component's node_parameters(), in tree order; a
+        component used twice appears once).  They ARE the potential's node values:
+        an in-place change (an optimizer step) is picked up by the next evaluation,
+        and the differentiable entry points (autograd.potential_and_force, leapfrog,
+        stream.integrate_releases_autograd) take them as inputs, so loss.backward()
+        fills their .grad."""
+        out, seen = [], set()
+        for c in self._all_components():
+            if id(c) not in seen:
+                seen.add(id(c))
+                out.extend(c.node_parameters())
+        return out
+
+    def _tracked_nodes(self) -> List[Tuple["_Component", List[torch.Tensor]]]:
+        """[(component, its node tensors)] for the tree's components whose
+        node_parameters() were requested, in tree order."""
+        out, seen = [], set()
+        for c in self._all_components():
+            p = c.__dict__.get("_node_params")
+            if p and id(c) not in seen:
+                seen.add(id(c))
+                out.append((c, list(p)))
+        return out
+
+    def _node_param_grads(self, table_grads: dict, tracked) -> List[torch.Tensor]:
+        """Gradients of the tracked node tensors (flattened like tracked) from
+        {component: table gradient} (Multipole dL/dpoly, CylSpline dL/d(node table));
+        zeros for a component without an entry (not in use at the times evaluated)."""
+        out = []
+        for comp, params in tracked:
+            g = table_grads.get(comp)
+            if g is None:
+                out.extend(torch.zeros_like(q) for q in params)
+            else:
+                out.extend(comp._grads_of_nodes(g))
+        return out
+
     def _c_args(self, t: float, dev: torch.device, leaves=None):
         """(component array, n_comps, leaf array, n_leaves) of the tree at time t
         (or of the given leaves)."""
@@ -172,6 +383,9 @@ class _GPUPotBase:
             leaves = self._leaves(float(t))
         if not leaves:
             raise ValueError("potential has no components")
+        for c, _, _, _ in leaves:
+            if c.__dict__.get("_node_params") and not torch.cuda.is_current_stream_capturing():
+                c._sync_nodes()
         if len(leaves) > _lib.MAX_LEAVES:
             raise ValueError(f"{len(leaves)} leaf components exceed the fused kernel's "
                              f"limit of {_lib.MAX_LEAVES}")
@@ -630,6 +844,36 @@ class _Component(_GPUPotBase):
             c.p[i] = float(v)
         return c, ()
 
+    def node_parameters(self, device=None) -> List[torch.Tensor]:
+        """Node tables as leaf tensors (expansions only; analytic profiles have none)."""
+        return []
+
+    def _track_nodes(self, tensors: List[torch.Tensor]) -> List[torch.Tensor]:
+        self._node_params = tensors
+        self._node_params_version = tuple(q._version for q in tensors)
+        return list(tensors)
+
+    def _sync_nodes(self) -> None:
+        """Rebuild the device tables when the node tensors changed in place."""
+        p = self.__dict__.get("_node_params")
+        if not p:
+            return
+        ver = tuple(q._version for q in p)
+        if ver != self.__dict__.get("_node_params_version"):
+            self._apply_nodes(p)
+            self._node_params_version = tuple(q._version for q in p)
+
+    def _refresh_tracked(self, values: List[torch.Tensor]) -> None:
+        """After set_node_tables(): copy the new values into the tracked tensors."""
+        p = self.__dict__.get("_node_params")
+        if not p:
+            return
+        with torch.no_grad():
+            for q, v in zip(p, values):
+                if q.data_ptr() != v.data_ptr():
+                    q.copy_(v.to(q.device))
+        self._node_params_version = tuple(q._version for q in p)
+
 
 # ---------------------------------------------------------------------------
 # Multipole
@@ -775,6 +1019,34 @@ class MultipolePotentialGPU(_Component):
 
     _n_file_cols = None
 
+    def node_parameters(self, device=None) -> List[torch.Tensor]:
+        """[Phi_lm(r_i), dPhi_lm/dr(r_i)]: the node tables, (nR, n_lm) each in the
+        builder's harmonic order (the layout of tables.node_phi and of
+        set_node_tables), as FP64 CUDA leaf tensors with requires_grad.  The same
+        tensors on every call.  The radial grid, invPhi0 and the extrapolation
+        constants stay those of construction (as in node_gradients)."""
+        p = self.__dict__.get("_node_params")
+        if p:
+            return list(p)
+        dev = torch.device(device) if device is not None else _cuda_device()
+        if self._nodes is not None:
+            phi, dphi = self._nodes
+        else:
+            phi = torch.from_numpy(np.ascontiguousarray(self.tables.node_phi))
+            dphi = torch.from_numpy(np.ascontiguousarray(self.tables.node_dphi_dr))
+        return self._track_nodes([phi.detach().to(dev, torch.float64).clone().requires_grad_(True),
+                                  dphi.detach().to(dev, torch.float64).clone().requires_grad_(True)])
+
+    def _apply_nodes(self, p) -> None:
+        self._set_nodes(p[0], p[1])
+
+    def _grads_of_nodes(self, grad_poly: torch.Tensor) -> List[torch.Tensor]:
+        """[dL/dPhi nodes, dL/d(dPhi/dr) nodes] in the layout of node_parameters()."""
+        from .diff_tables import node_vjp
+        g0, g1 = node_vjp(self.tables, grad_poly, None, nodes=self._nodes)
+        dev = self._node_params[0].device
+        return [g0.to(dev), g1.to(dev)]
+
     def _device_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor):
         """(FP64 interval-major, FP32) device tables of this object's layout from node
         tables (nR, n_lm) in the builder's harmonic order, computed with torch on
@@ -802,11 +1074,15 @@ class MultipolePotentialGPU(_Component):
         extrapolation constants are kept from construction (the same constants that
         node_gradients() holds fixed).  Not differentiable itself: use
         node_gradients() on the adjoint's table gradient."""
+        self._set_nodes(phi, dphi_dr)
+        self._refresh_tracked([phi.detach(), dphi_dr.detach()])
+
+    def _set_nodes(self, phi: torch.Tensor, dphi_dr: torch.Tensor) -> None:
         if phi.shape != self.tables.node_phi.shape or dphi_dr.shape != phi.shape:
             raise ValueError(f"node tables must have shape {self.tables.node_phi.shape}")
         dev = phi.device if phi.device.type == "cuda" else _cuda_device()
-        phi = phi.detach().to(dev, torch.float64)
-        dphi_dr = dphi_dr.detach().to(dev, torch.float64)
+        phi = phi.detach().to(dev, torch.float64).clone()
+        dphi_dr = dphi_dr.detach().to(dev, torch.float64).clone()
         im, p32 = self._device_tables(phi, dphi_dr)
         self._nodes = (phi, dphi_dr)
         self._node_tables = (im, p32)
@@ -925,6 +1201,40 @@ class CylSplinePotentialGPU(_Component):
             phi = {m: v.detach().cpu().numpy() for m, v in phi.items()}
         return cylspline_node_vjp(self.tables, self._coefs, grad_nodes, phi=phi)
 
+    def _node_keys(self) -> List[int]:
+        return sorted(int(m) for m in self._coefs.phi)
+
+    def node_parameters(self, device=None) -> List[torch.Tensor]:
+        """The harmonic grids Phi_m(R, z) on the coefficient file's grid, one FP64 CUDA
+        leaf tensor with requires_grad per m in ascending order (the layout of
+        set_node_tables).  The same tensors on every call.  The grids, Rscale and the
+        outer asymptote stay those of construction (as in node_gradients)."""
+        p = self.__dict__.get("_node_params")
+        if p:
+            return list(p)
+        if self._coefs is None:
+            raise ValueError("node_parameters() needs the coefficients the object was built from")
+        dev = torch.device(device) if device is not None else _cuda_device()
+        cur = self.__dict__.get("_phi_nodes")
+        out = []
+        for m in self._node_keys():
+            if cur is not None:
+                v = cur[m]
+            else:
+                v = self._coefs.phi[m] if m in self._coefs.phi else self._coefs.phi[str(m)]
+                v = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
+            out.append(v.detach().to(dev, torch.float64).clone().requires_grad_(True))
+        return self._track_nodes(out)
+
+    def _apply_nodes(self, p) -> None:
+        self._set_grids(dict(zip(self._node_keys(), p)))
+
+    def _grads_of_nodes(self, grad_nodes: torch.Tensor) -> List[torch.Tensor]:
+        """dL/dPhi_m per m (ascending), the layout of node_parameters()."""
+        d = self.node_gradients(grad_nodes)
+        dev = self._node_params[0].device
+        return [torch.as_tensor(np.ascontiguousarray(d[m]), device=dev) for m in self._node_keys()]
+
     def set_node_tables(self, phi: dict) -> None:
         """Replace the harmonic grids Phi_m(R, z) -- {m: (nR, nz) device tensors on the
         coefficient file's grid} -- rebuilding the node and cell tables on the GPU, in
@@ -933,6 +1243,11 @@ class CylSplinePotentialGPU(_Component):
         grids, Rscale, the log-scaling choice and the outer asymptote (fitted at
         construction) are kept, as node_gradients() holds them.  Not differentiable
         itself: use node_gradients() on the adjoint's table gradient."""
+        self._set_grids(phi)
+        keys = self._node_keys()
+        self._refresh_tracked([self._phi_nodes[m] for m in keys])
+
+    def _set_grids(self, phi: dict) -> None:
         from .diff_tables import _spline_deriv_matrix
         t = self.tables
         keys = sorted(int(m) for m in self._coefs.phi)
@@ -1064,6 +1379,11 @@ class EvolvingPotentialGPU(_GPUPotBase):
         self._times = np.asarray(times, dtype=np.float64)
         self._interpolate = interpolate
 
+    def _time_data(self) -> np.ndarray:
+        """AGB_OP_EVOLVE data: [n, interpolate, times]."""
+        interp = 1.0 if (self._interpolate and len(self._pots) > 1) else 0.0
+        return np.concatenate([[float(len(self._times)), interp], self._times])
+
     def _bracket(self, t: float):
         times = self._times
         n = len(times)
@@ -1130,6 +1450,15 @@ class ShiftedPotentialGPU(_GPUPotBase):
         else:
             raise ValueError("Center must be (3,) or (T, 4) or (T, 7).")
 
+    def _time_data(self) -> np.ndarray:
+        """AGB_OP_SHIFT data: [0, c] static, or [1, T, t0, tN, p0, pN, v0, vN, x, c]."""
+        if self._is_static:
+            return np.concatenate([[0.0], self._center_static])
+        sp = self._spline
+        T = len(sp.x)
+        return np.concatenate([[1.0, float(T), self._t0, self._tN], self._pos0, self._posN,
+                               self._vel0, self._velN, sp.x, np.asarray(sp.c).reshape(-1)])
+
     def _center_at(self, t: float) -> np.ndarray:
         if self._is_static:
             return self._center_static
@@ -1192,6 +1521,21 @@ class ScaledPotentialGPU(_GPUPotBase):
         else:
             self._ampl_spl = None
         self._ampl_val = float(ampl)
+
+    def _time_data(self) -> np.ndarray:
+        """AGB_OP_SCALE data: [0, scale, ampl] static, or [1, T, t0, tN, scale0, scaleN,
+        dscale0, dscaleN, has_ampl, ampl, ampl0, amplN, dampl0, damplN, x, cs(, ca)]."""
+        if self._is_static:
+            return np.array([0.0, self._scale_val, self._ampl_val])
+        sp = self._scale_spl
+        has = self._ampl_spl is not None
+        ends = [self._ampl0, self._amplN, self._dampl0, self._damplN] if has else [0.0] * 4
+        parts = [[1.0, float(len(sp.x)), self._t0, self._tN, self._scale0, self._scaleN,
+                  self._dscale0, self._dscaleN, 1.0 if has else 0.0, self._ampl_val] + ends,
+                 sp.x, np.asarray(sp.c).reshape(-1)]
+        if has:
+            parts.append(np.asarray(self._ampl_spl.c).reshape(-1))
+        return np.concatenate(parts)
 
     def _sa(self, t: float):
         """(s, a) = (1/scale(t), ampl(t))."""

@@ -209,7 +209,8 @@ def particle_spray(pot, x_p, v_p, mass: float, t_end: float, n_steps: int, dt: f
     t_start = float(t_end) - n_steps * dt
 
     # 1. progenitor orbit backwards from t_end, recorded at every step boundary
-    back = Leapfrog(pot, -dt, t0=float(t_end), precision=precision, use_graph=False, scheme=scheme)
+    back = Leapfrog(pot, -dt, t0=float(t_end), precision=precision, use_graph=False, scheme=scheme,
+                    device_time=False)
     xb, vb, Fb = back._buffers(xp)
     xb.copy_(xp)
     vb.copy_(vp)
@@ -218,7 +219,7 @@ def particle_spray(pot, x_p, v_p, mass: float, t_end: float, n_steps: int, dt: f
     rec[n_steps, 0].copy_(xb[0])
     rec[n_steps, 1].copy_(vb[0])
     for n in range(n_steps):
-        back._step(xb, vb, Fb, back.t0 + n * back.dt)
+        back._step(xb, vb, Fb, n)
         rec[n_steps - 1 - n, 0].copy_(xb[0])
         rec[n_steps - 1 - n, 1].copy_(vb[0])
     times = t_start + dt * np.arange(n_steps + 1, dtype=np.float64)
@@ -261,7 +262,7 @@ def integrate_releases(pot, x_release: torch.Tensor, v_release: torch.Tensor, re
         raise ValueError(f"x_release and v_release must be ({N}, 3)")
     dev = x_release.device
     integ = Leapfrog(pot, dt, t0=float(t_start), precision=precision, use_graph=False,
-                     scheme=scheme)
+                     scheme=scheme, device_time=False)
     S = integ.S
     x = torch.empty((N, 3), dtype=torch.float64, device=dev)
     v = torch.empty_like(x)
@@ -291,3 +292,39 @@ def integrate_releases(pot, x_release: torch.Tensor, v_release: torch.Tensor, re
     return Stream(x=x, v=v, t_release=t_release, x_release=x_rel, v_release=v_rel, track=None,
                   r_jacobi=None, _integ=integ, _counts=counts, _store=st,
                   _offsets=[int(o) for o in offsets[:-1]])
+
+
+class _ReleasesFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x_release, v_release, pot, release_steps, t_start, n_steps, dt, scheme,
+                precision, tracked, *nodes):
+        st = integrate_releases(pot, x_release, v_release, release_steps, t_start, n_steps, dt,
+                                scheme=scheme, precision=precision, store=True)
+        ctx.stream, ctx.tracked, ctx.pot = st, tracked, pot
+        return st.x.clone(), st.v.clone()
+
+    @staticmethod
+    def backward(ctx, gx, gv):
+        st = ctx.stream
+        gx = torch.zeros_like(st.x) if gx is None else gx
+        gv = torch.zeros_like(st.v) if gv is None else gv
+        node_grads = [None] * sum(len(p) for _, p in ctx.tracked)
+        if any(ctx.needs_input_grad[10:]):
+            lx, lv, tg = st.adjoint(gx, gv, table_grads=True)
+            node_grads = ctx.pot._node_param_grads(tg, ctx.tracked)
+        else:
+            lx, lv = st.adjoint(gx, gv)
+        ctx.stream = None
+        return (lx, lv, None, None, None, None, None, None, None, None, *node_grads)
+
+
+def integrate_releases_autograd(pot, x_release: torch.Tensor, v_release: torch.Tensor,
+                                release_steps, t_start: float, n_steps: int, dt: float,
+                                scheme="leapfrog", precision: Optional[str] = None):
+    """(x, v) at t_start + n_steps dt of the particles released as in
+    ``integrate_releases``, differentiable w.r.t. x_release, v_release and the node
+    tensors of the potential (pot.node_parameters()) through ``Stream.adjoint``."""
+    tracked = pot._tracked_nodes() if hasattr(pot, "_tracked_nodes") else []
+    nodes = [q for _, ps in tracked for q in ps]
+    return _ReleasesFn.apply(x_release, v_release, pot, release_steps, float(t_start),
+                             int(n_steps), float(dt), scheme, precision, tracked, *nodes)

@@ -368,6 +368,97 @@ int     agb_batch_tiles(const agb_batch* plan);
 void    agb_batch_destroy(agb_batch* plan);
 
 /*
+ * Time-dependent leaves evaluated on the device.  The reference evaluates the
+ * Shifted centre, the Scaled factors and the Evolving bracket on the host at
+ * every call (gpu_potential.py:1716-1734, :1845-1871, :1559-1612), so the
+ * time is a host value baked into every launch.  A time plan instead holds, per
+ * leaf slot, a program of modifier operations and their tables (splines as
+ * breakpoints and cubic coefficients, snapshot times) in device memory; a small
+ * kernel turns a device-resident step counter into the leaves at
+ *     t = (t0 + step * dt) + off
+ * right before the evaluation kernel, so a sequence of launches can be captured
+ * once in a CUDA graph and replayed at every step.  The device arithmetic is
+ * that of the host path operation by operation (no contraction into FMA, the
+ * spline evaluated as sum c_k s^k with s^k by repeated multiplication, the
+ * bracket by the same bisection), so the leaves equal the host's bit for bit.
+ * No counterpart in the reference.
+ *
+ * A program starts from (comp, sigma 1, gamma 0, ampl 1) and applies its ops,
+ * innermost modifier first:
+ *   AGB_OP_SHIFT   gamma += sigma * c(t)
+ *   AGB_OP_SCALE   (s, a) = (1/scale(t), ampl(t)); sigma *= s; ampl = (a*s)*ampl
+ *   AGB_OP_EVOLVE  bracket t in the snapshot times: comp += chosen snapshot,
+ *                  ampl *= its weight; slot 0 takes the lower snapshot with
+ *                  weight 1-alpha (1 at alpha 0, 0 at alpha 1), slot 1 the
+ *                  upper with alpha; with interpolation off (or one snapshot)
+ *                  slot 0 takes the nearest with weight 1
+ * Table data at arg[k] (doubles):
+ *   SHIFT   [0, cx, cy, cz] (static) or
+ *           [1, T, t0, tN, p0[3], pN[3], v0[3], vN[3], x[T], c[4][T-1][3]]
+ *   SCALE   [0, scale, ampl] (static) or
+ *           [1, T, t0, tN, scale0, scaleN, dscale0, dscaleN, has_ampl, ampl,
+ *            ampl0, amplN, dampl0, damplN, x[T], cs[4][T-1] (, ca[4][T-1])]
+ *   EVOLVE  [n, interpolate, times[n]]
+ * (c: cubic coefficients, highest power first, of the centre, scale and
+ * amplitude splines; outside [t0, tN] a spline is extended linearly from its
+ * end value and slope.)  pair = 1 lets this slot and the next share one
+ * harmonic walk (both Multipoles of one grid and column structure, the same
+ * transform), as agb_eval does for the two snapshots of an Evolving.
+ */
+#define AGB_OP_SHIFT  1
+#define AGB_OP_SCALE  2
+#define AGB_OP_EVOLVE 3
+#define AGB_MAX_LEAF_OPS 6
+
+typedef struct agb_leaf_prog {
+    int32_t comp;                     /* component index (EVOLVE: of snapshot 0) */
+    int32_t n_ops;
+    int32_t op[AGB_MAX_LEAF_OPS];     /* AGB_OP_*, innermost first */
+    int32_t arg[AGB_MAX_LEAF_OPS];    /* offset of the op's data in the table */
+    int32_t slot;                     /* EVOLVE: 0 lower / nearest, 1 upper */
+    int32_t pair;
+} agb_leaf_prog;
+
+typedef struct agb_time_plan agb_time_plan;
+/* validates the programs against the table (host arrays) and copies both to
+   the current device (one allocation, owned by the plan) */
+int agb_time_plan_create(const agb_leaf_prog* progs, int n_progs, const double* table,
+                         int64_t n_table, agb_time_plan** out);
+void agb_time_plan_destroy(agb_time_plan* plan);
+/* the same programs evaluated on the host at time t (the device kernel's
+   arithmetic, for checking): leaves[n_progs] */
+int agb_time_plan_leaves_host(const agb_time_plan* plan, double t, agb_leaf* leaves);
+/* the device leaves at t = (t0 + (*step) * dt) + off, written to leaves_dev
+   [n_progs] (device); step is a device int64 (NULL: step 0) */
+int agb_time_plan_leaves(const agb_time_plan* plan, const int64_t* step, double t0, double dt,
+                         double off, agb_leaf* leaves_dev, void* stream);
+/*
+ * agb_eval_ws with the plan's leaves at t = (t0 + (*step) * dt) + off computed on
+ * the device in the same stream: no host value of t enters a launch.  The
+ * workspace (agb_eval_timed_workspace_bytes) holds the device leaves and the
+ * interval-sort scratch.
+ */
+size_t agb_eval_timed_workspace_bytes(const agb_component* comps, int n_comps,
+                                      const agb_time_plan* plan, int64_t n, int out_flags);
+int agb_eval_timed(const agb_component* comps, int n_comps, const agb_time_plan* plan,
+                   const int64_t* step, double t0, double dt, double off,
+                   const double* xyz, int64_t n, int mode, int precision,
+                   double* phi, double* grad, double* hess, double* rho, int out_flags,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Leapfrog vector updates of one (sub)step boundary, one launch, in place:
+ *   v = fma(h1, F, v)   if flags & 1   (closing half-kick of the last substep)
+ *   v = fma(h2, F, v)   if flags & 2   (opening half-kick of the next one)
+ *   x = fma(dt, v, x)   if flags & 4   (drift)
+ *   (*step)++           if flags & 8   (step counter of agb_eval_timed; thread 0)
+ * x, v, F are [n, 3] device arrays.  No counterpart in the reference (it has no
+ * integrator).
+ */
+int agb_leapfrog_kick_drift(double* x, double* v, const double* F, int64_t n, double h1,
+                            double h2, double dt, int flags, int64_t* step, void* stream);
+
+/*
  * Kernel-signature entries.  Arguments are those of the reference kernels, in
  * order, with SoA x, y, z device arrays, the reference's harmonic-major poly
  * layout and lm_l/lm_m arrays sorted as gpu_potential.py:516 sorts them.
