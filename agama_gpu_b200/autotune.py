@@ -157,7 +157,7 @@ def apply_cached(pot, n: int, mode: str = "force", t: float = 0.0,
     return True
 
 
-def tune_batch(batch, xyz, tiles=(512, 1024, 2048, 4096), precision: Optional[str] = None,
+def tune_batch(batch, xyz, tiles=(1024, 2048, 4096, 8192), precision: Optional[str] = None,
                reps: int = 3) -> Dict:
     """Pick the work-queue tile size of a BatchedPotentialGPU on its own points."""
     arr, _ = prep_xyz(xyz)

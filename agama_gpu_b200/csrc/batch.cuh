@@ -16,7 +16,7 @@
 // interval of the unit's heaviest Multipole (the per-call binning of agb_eval,
 // done here per tile with no global scratch), so a warp's lanes read the same
 // interval's coefficients.
-#define AGB_BATCH_SORT_MAX 4096        // largest tile that is sorted
+#define AGB_BATCH_SORT_MAX 8192        // largest tile that is sorted (34 KB of shared memory)
 #define AGB_BATCH_MAX_BINS 256         // most intervals (+2) of a sorted unit
 
 struct BatchTile {

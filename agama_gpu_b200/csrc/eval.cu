@@ -89,10 +89,6 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 // internal mode of agb_eval_vjp_force: the VJP plus the force of the same leaves
 // (written to the `hess` pointer as [N,3]) from the same per-point sums
 #define AGB_MODE_VJPF 5
-// threads per block of the wide (mixed-precision) fused Multipole adjoint
-#ifndef AGB_ADJ_WIDE_THREADS
-#define AGB_ADJ_WIDE_THREADS 384
-#endif
 
 __host__ __device__ constexpr int stage_rec(int mode)
 {
@@ -165,12 +161,17 @@ agb_eval_kernel(const __grid_constant__ EvalArgs a)
         double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int L = 0; L < a.n_leaves; ++L) {
             const DevLeaf& lf = DYN ? dyn_leaves[L] : a.leaves[L];
+            // a zero-weight leaf (the unused snapshot of an Evolving bracket at a snapshot
+            // time) contributes nothing: skipped, so its partner is walked alone, as the
+            // host flattening evaluates it
+            if (lf.ampl == 0.0) continue;
             const DevComp& c = a.comps[lf.comp];
             const double lx = lf.sigma * x - lf.g0;
             const double ly = lf.sigma * y - lf.g1;
             const double lz = lf.sigma * z - lf.g2;
             if ((MODE == AGB_MODE_POT || MODE == AGB_MODE_GRAD) && !AN &&
-                std::is_same<R, float>::value && lf.pad == 1) {
+                std::is_same<R, float>::value && lf.pad == 1 &&
+                (DYN ? dyn_leaves[L + 1] : a.leaves[L + 1]).ampl != 0.0) {
                 // this leaf and the next share grid, columns and transform (pack_args);
                 // FP32 walks only (the FP64 walk holds twice the state and would spill)
                 const DevLeaf& lf2 = DYN ? dyn_leaves[L + 1] : a.leaves[L + 1];
@@ -1212,29 +1213,22 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
         g.perm = tmp.perm;
     }
     if (!rc) {
-        // per warp: the (U, V) tile, plus the interval accumulator when all warps' fit.
-        // The mixed walk runs 12 warps per block (168 registers) when their tiles and
-        // accumulators fit in shared memory, else 8 (255 registers) like FP64.
+        // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
+        // (256 threads at 255 registers; 384 threads at 168 registers spilled and
+        // made the backward step 22 % slower)
+        const int grid = (int)std::min<long long>((long long)num_sms() * 2, (n + 255) / 256);
+        const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
+        g.chunk = ((groups + warps - 1) / warps) * 32;
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
         const size_t acc = (size_t)g.c.n_lm * 6 * sizeof(double);
         int optin = 0;
         if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                    current_device()) != cudaSuccess)
             optin = 48 * 1024;
-        const int wide = AGB_ADJ_WIDE_THREADS / 32;
-        const bool use_wide = precision == AGB_PREC_MIXED && AGB_ADJ_WIDE_THREADS > 256 &&
-                              (size_t)wide * (tile + acc) <= (size_t)optin;
-        const int wpb = use_wide ? wide : 8;
-        const int threads = wpb * 32;
-        const int grid = (int)std::min<long long>((long long)num_sms() * (use_wide ? 1 : 2),
-                                                  (n + threads - 1) / threads);
-        const long long warps = (long long)grid * wpb, groups = (n + 31) / 32;
-        g.chunk = ((groups + warps - 1) / warps) * 32;
-        g.staged = (size_t)wpb * (tile + acc) <= (size_t)optin;
+        g.staged = (size_t)8 * (tile + acc) <= (size_t)optin;
         g.warp_smem = g.staged ? (int)(tile + acc) : tile;
-        const size_t smem = (size_t)wpb * g.warp_smem;
-        const void* fn = use_wide ? (const void*)mp_adjoint_kernel<float, AGB_ADJ_WIDE_THREADS>
-                       : precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
+        const size_t smem = (size_t)8 * g.warp_smem;
+        const void* fn = precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
                                                      : (const void*)mp_adjoint_kernel<double>;
         if (smem > (size_t)optin)
             rc = set_err(AGB_ERR_UNSUPPORTED, "agb_multipole_adjoint: needs %zu bytes of shared "
@@ -1244,8 +1238,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
             rc = set_err(AGB_ERR_DEVICE, "agb_multipole_adjoint: cannot reserve %zu bytes of shared "
                          "memory", smem);
         if (!rc) {
-            if (use_wide) mp_adjoint_kernel<float, AGB_ADJ_WIDE_THREADS><<<grid, threads, smem, st>>>(g);
-            else if (precision == AGB_PREC_MIXED) mp_adjoint_kernel<float><<<grid, 256, smem, st>>>(g);
+            if (precision == AGB_PREC_MIXED) mp_adjoint_kernel<float><<<grid, 256, smem, st>>>(g);
             else mp_adjoint_kernel<double><<<grid, 256, smem, st>>>(g);
             rc = check_launch("mp_adjoint_kernel");
         }

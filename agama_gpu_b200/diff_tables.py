@@ -96,8 +96,11 @@ def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: Optional[int],
     else:
         phi = nodes[0].detach().to(dev, torch.float64).requires_grad_(True)
         dphi = nodes[1].detach().to(dev, torch.float64).requires_grad_(True)
-    poly = multipole_poly_from_nodes(tables, phi, dphi)
-    gphi, gdphi = torch.autograd.grad(poly, (phi, dphi), grad_outputs=grad_poly.to(torch.float64))
+    # also called from the backward of an autograd.Function, where grad mode is off
+    with torch.enable_grad():
+        poly = multipole_poly_from_nodes(tables, phi, dphi)
+        gphi, gdphi = torch.autograd.grad(poly, (phi, dphi),
+                                          grad_outputs=grad_poly.to(torch.float64))
     if n_file_cols is None:
         return gphi, gdphi
     cols = torch.as_tensor(np.asarray(tables.node_cols), dtype=torch.long, device=dev)

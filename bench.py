@@ -378,6 +378,45 @@ def timedep_leapfrog(dev, n: int, n_steps: int, graph_steps: int = 16):
     return out
 
 
+def timedep_leapfrog(dev, n: int, n_steps: int, graph_steps: int = 16):
+    """Leapfrog in the time-dependent config-2 composite (mixed precision), n Hernquist
+    particles, dt = 1e-3: per-step time with the steps captured in CUDA graphs (the
+    leaves computed on the device from a device step counter), stepped eagerly with
+    device leaves, and stepped eagerly with the leaves computed on the host per step;
+    the three trajectories are compared bit for bit."""
+    import torch
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import build_composite, composite_spec, hernquist_points
+    pot = build_composite(composite_spec())
+    pot.set_precision("mixed")
+    xyz = hernquist_points(n, 10.0, 77)
+    x0 = torch.from_numpy(xyz).to(dev)
+    v0 = torch.from_numpy(np.random.default_rng(7).normal(0.0, 120.0, xyz.shape)).to(dev)
+    out = {"particles": n, "steps": n_steps, "graph_steps": graph_steps}
+    res = {}
+    for name, kw in (("graph", dict(graph_steps=graph_steps)),
+                     ("eager_device_leaves", dict(use_graph=False)),
+                     ("eager_host_leaves", dict(use_graph=False, device_time=False))):
+        integ = Leapfrog(pot, 1e-3, t0=0.1, **kw)
+        integ.run(x0, v0, 2 * graph_steps, checkpoint_every=2 * graph_steps)   # capture, warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        xT, vT, _ = integ.run(x0, v0, n_steps, checkpoint_every=n_steps)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name + "_ms_per_step"] = e0.elapsed_time(e1) / n_steps
+        res[name] = (xT, vT)
+        if name == "graph":
+            out["graph_captured"] = bool(integ.use_graph and integ._graph is not None)
+    xg, vg = res["graph"]
+    out["bit_equal_graph_vs_eager"] = bool(torch.equal(xg, res["eager_device_leaves"][0]) and
+                                           torch.equal(vg, res["eager_device_leaves"][1]))
+    out["bit_equal_graph_vs_host_leaves"] = bool(torch.equal(xg, res["eager_host_leaves"][0]) and
+                                                 torch.equal(vg, res["eager_host_leaves"][1]))
+    return out
+
+
 def cylspline_leg(dev, n: int, steps: int, warmup: int):
     """CylSpline bar (mmax 6: m=0 Miyamoto-Nagai + m=2,4,6 with seeded phases, 32x32
     sinh grid), 1M exponential-disk points (Rd 3, hz 0.3): Phi+F in FP64 and mixed."""
@@ -605,6 +644,7 @@ def main():
 
     cyl = cylspline_leg(dev, 1_000_000, max(3, args.steps), 3)
     timedep = timedep_leapfrog(dev, 1_000_000, 64) if args.adj_steps > 0 else None
+    timedep = timedep_leapfrog(dev, 1_000_000, 64) if args.adj_steps > 0 else None
     batched = None
     if args.batch_units > 0:
         torch.cuda.empty_cache()
@@ -641,6 +681,7 @@ def main():
         "adjoint": adj,
         "batched": batched,
         "cylspline": cyl,
+        "timedep_leapfrog": timedep,
         "timedep_leapfrog": timedep,
         "e2e": {"value": world * N / (e2e_ms * 1e-3), "unit": "pts/s",
                 "h2d_bytes_per_step": N * 24, "d2h_bytes_per_step": N * 32,

@@ -123,7 +123,7 @@ def test_leapfrog_backward_fills_node_grads():
         picks = torch.topk(flat, 3).indices.tolist() + list(rng.integers(0, flat.numel(), 2))
         for j in picks:
             i0, c0 = divmod(int(j), q.shape[1])
-            v = float(q[i0, c0])
+            v = float(q.detach()[i0, c0])
             h = 1e-5 * max(abs(v), 1e-3 * float(q.abs().max()))
             with torch.no_grad():
                 q[i0, c0] = v + h
@@ -150,9 +150,11 @@ def test_potential_and_force_node_grads_and_in_place_updates():
     rng = np.random.default_rng(4)
     gp = torch.from_numpy(rng.normal(size=200)).cuda()
     gf = torch.from_numpy(rng.normal(size=(200, 3))).cuda()
-    # an in-place update of the node tensors changes the potential
+    # an in-place update of the node tensors changes the potential (the harmonics: the
+    # monopole must stay within the log-scaling's range fixed at construction)
     with torch.no_grad():
-        phi.mul_(1.01)
+        phi[:, 1:].mul_(1.01)
+        dphi[:, 1:].mul_(0.99)
     p1, f1 = autograd.potential_and_force(pot, x, 0.0, precision="fp64")
     mp2, _, pot2 = _pot(lmax=6)
     mp2.set_node_tables(phi.detach(), dphi.detach())
@@ -191,7 +193,7 @@ def test_cylspline_node_grads_through_leapfrog():
         q, g = grids[k], grids[k].grad
         j = int(torch.argmax(g.abs()))
         i0, c0 = divmod(j, q.shape[1])
-        v = float(q[i0, c0])
+        v = float(q.detach()[i0, c0])
         h = 1e-5 * abs(v)
         with torch.no_grad():
             q[i0, c0] = v + h
@@ -223,7 +225,7 @@ def test_stream_releases_backward_fills_node_grads():
     g = dphi.grad
     j = int(torch.argmax(g.abs()))
     i0, c0 = divmod(j, dphi.shape[1])
-    val = float(dphi[i0, c0])
+    val = float(dphi.detach()[i0, c0])
     h = 1e-5 * abs(val)
     out = []
     for s in (1, -1):
