@@ -75,6 +75,7 @@ class AgbLeaf(ctypes.Structure):
 
 MAX_LEAF_OPS = 6
 OP_SHIFT, OP_SCALE, OP_EVOLVE = 1, 2, 3
+ADJ_DRIFT = 1
 
 
 class AgbLeafProg(ctypes.Structure):
@@ -121,6 +122,20 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
         ctypes.c_void_p]
+    lib.agb_multipole_adjoint_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_multipole_adjoint_workspace_bytes.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_int64, ctypes.c_int]
+    lib.agb_adjoint_step_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_adjoint_step_workspace_bytes.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_int, ctypes.c_int64, ctypes.c_int]
+    lib.agb_adjoint_step.restype = ctypes.c_int
+    lib.agb_adjoint_step.argtypes = [
+        ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
+        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+        ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_adjoint.restype = ctypes.c_int
     lib.agb_multipole_adjoint.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
@@ -211,7 +226,8 @@ EXPORTED = [
     "agb_eval_ws", "agb_eval_workspace_bytes", "agb_eval_wave_points", "agb_eval_static", "agb_eval_vjp",
     "agb_eval_vjp_force", "agb_multipole_adjoint_force",
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
-    "agb_multipole_adjoint", "agb_cylspline_table_vjp", "agb_adjoint_kick", "agb_reverse_drift",
+    "agb_multipole_adjoint", "agb_multipole_adjoint_workspace_bytes", "agb_cylspline_table_vjp",
+    "agb_adjoint_step", "agb_adjoint_step_workspace_bytes", "agb_adjoint_kick", "agb_reverse_drift",
     "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy", "agb_time_plan_create", "agb_time_plan_destroy",
     "agb_time_plan_leaves_host", "agb_time_plan_leaves", "agb_eval_timed_workspace_bytes",

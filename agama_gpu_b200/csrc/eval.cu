@@ -86,6 +86,10 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 // workspace the kernel instead writes records in sorted order ("stage") and
 // unpermute_kernel gathers them back, reading one record per point and writing
 // every output array contiguously.
+// blocks per SM of the fused Multipole adjoint's grid (one resident at a time)
+#ifndef AGB_ADJ_WAVES
+#define AGB_ADJ_WAVES 2
+#endif
 // internal mode of agb_eval_vjp_force: the VJP plus the force of the same leaves
 // (written to the `hess` pointer as [N,3]) from the same per-point sums
 #define AGB_MODE_VJPF 5
@@ -1107,6 +1111,18 @@ extern "C" int agb_leapfrog_kick_drift(double* x, double* v, const double* F, in
 // ---------------------------------------------------------------------------
 // gradient w.r.t. one Multipole leaf's quintic coefficients
 // ---------------------------------------------------------------------------
+extern "C" size_t agb_multipole_adjoint_workspace_bytes(const agb_component* comp,
+                                                        const agb_leaf* leaf, int64_t n,
+                                                        int with_force)
+{
+    if (!comp || !leaf) return 0;
+    agb_leaf l = *leaf;
+    l.comp = 0;
+    const BinPlan b = plan_binning(comp, &l, 1, n, 0);
+    if (!b.on) return 0;
+    return ws_bytes(b, n) + al256(8 * (size_t)(with_force ? 6 : 3) * (size_t)n);
+}
+
 extern "C" size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* comp,
                                                           const agb_leaf* leaf, int64_t n)
 {
@@ -1167,13 +1183,24 @@ extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf
 // ---------------------------------------------------------------------------
 // fused adjoint of one Multipole leaf (position VJP + coefficient gradient)
 // ---------------------------------------------------------------------------
+// keep: (agb_adjoint_step) the per-point results stay staged in the workspace, in
+// sorted order, with the sorted position of point i in dest[i]; they are not added
+// to g_xyz / force (which may then be null; with_force sets the record size)
+struct AdjKeep {
+    bool on;
+    bool with_force;
+    const int* dest;
+    const double* stage;
+};
+
 static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* leaf,
                                   const double* xyz, int64_t n, int precision,
                                   const double* g_phi, const double* g_force, double* g_xyz,
                                   double* force, double* g_table, void* workspace,
-                                  size_t workspace_bytes, void* stream)
+                                  size_t workspace_bytes, void* stream, AdjKeep* keep = nullptr)
 {
-    if (!comp || !leaf || !g_table || !g_xyz)
+    const bool keep_on = keep && keep->on;
+    if (!comp || !leaf || !g_table || (!g_xyz && !keep_on))
         return set_err(AGB_ERR_ARG, "agb_multipole_adjoint: null argument");
     if (comp->kind != AGB_KIND_MULTIPOLE || comp->layout != AGB_LAYOUT_INTERVAL_MAJOR ||
         comp->structure == AGB_STRUCT_LIST)
@@ -1195,10 +1222,19 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
     cudaStream_t st = (cudaStream_t)stream;
     agb_leaf l = *leaf;
     l.comp = 0;
-    const BinPlan b = plan_binning(comp, &l, 1, n, 0);
-    const size_t need = ws_bytes(b, n);
-    void* ws = workspace;
+    const BinPlan b = plan_binning(comp, &l, 1, n, keep_on ? AGB_OUT_BIN_ALWAYS : 0);
+    const size_t rec = (force || (keep_on && keep->with_force)) ? 6 : 3;
+    const size_t staged = b.on ? ws_bytes(b, n) + al256(8 * rec * (size_t)n) : 0;
     const bool own = (workspace == nullptr);
+    // with room for them, the per-point results are written in sorted order and added
+    // back in input order by adj_unpermute_add (always for the library's own scratch)
+    const bool stage = b.on && (own || workspace_bytes >= staged);
+    if (keep_on && (!stage || own))
+        return set_err(AGB_ERR_ARG, "agb_adjoint_step: a workspace of "
+                       "agb_adjoint_step_workspace_bytes() bytes is required");
+    g.stage_rec = (int)rec;
+    const size_t need = stage ? staged : ws_bytes(b, n);
+    void* ws = workspace;
     if (need) {
         if (own) {
             if (cudaMallocAsync(&ws, need, st) != cudaSuccess)
@@ -1211,12 +1247,14 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
         rc = run_binning(tmp, b, xyz, n, (char*)ws, st);
         g.xyz = tmp.xyz;
         g.perm = tmp.perm;
+        if (stage) g.stage = (double*)((char*)ws + ws_bytes(b, n));
     }
     if (!rc) {
         // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
         // (256 threads at 255 registers; 384 threads at 168 registers spilled and
         // made the backward step 22 % slower)
-        const int grid = (int)std::min<long long>((long long)num_sms() * 2, (n + 255) / 256);
+        const int grid = (int)std::min<long long>((long long)num_sms() * AGB_ADJ_WAVES,
+                                                  (n + 255) / 256);
         const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
         g.chunk = ((groups + warps - 1) / warps) * 32;
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
@@ -1242,9 +1280,182 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
             else mp_adjoint_kernel<double><<<grid, 256, smem, st>>>(g);
             rc = check_launch("mp_adjoint_kernel");
         }
+        if (!rc && g.stage && keep_on) {
+            keep->dest = (const int*)ws;           // bin_scatter leaves pos of point i in keys[i]
+            keep->stage = g.stage;
+        } else if (!rc && g.stage) {
+            const int* dest = (const int*)ws;       // bin_scatter leaves pos of point i in keys[i]
+            if (force) adj_unpermute_add<6><<<grid_for(n), 256, 0, st>>>(dest, g.stage, n, g_xyz, force);
+            else adj_unpermute_add<3><<<grid_for(n), 256, 0, st>>>(dest, g.stage, n, g_xyz, nullptr);
+            rc = check_launch("adj_unpermute_add");
+        }
     }
     if (need && own) cudaFreeAsync(ws, st);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// one backward step of the leapfrog adjoint in two launches: the fused
+// Multipole adjoint (staged in sorted order), then per particle the analytic
+// leaves' VJP and force at x, the staged Multipole part added, the adjoint
+// kick and (DRIFT) the time-reversed drift -- the work of the analytic VJP
+// launch, adj_unpermute_add, adjoint_kick_kernel and reverse_drift_kernel, with
+// the same arithmetic in the same order
+// ---------------------------------------------------------------------------
+struct AdjStepPtrs {
+    double* x;           // [N,3] positions at the VJP (reverse-drifted in place)
+    double* vh;          // [N,3] half-step velocities (DRIFT)
+    double* lx;          // [N,3] adjoint of x
+    double* lv;          // [N,3] adjoint of v
+    double* gF;          // [N,3] in: cotangent of F at x; out: c lv
+    const int* dest;     // sorted position of point i
+    const double* stage; // [pos][stage_rec] Multipole VJP (and force)
+    long long n;
+    int stage_rec;
+    int drift;
+    double dt, c, k, dt_drift;
+};
+
+__global__ void __launch_bounds__(256, 2)
+adjoint_step_kernel(const __grid_constant__ EvalArgs a, const __grid_constant__ AdjStepPtrs p)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) {
+        const double x = p.x[3 * i], y = p.x[3 * i + 1], z = p.x[3 * i + 2];
+        const double f0 = p.gF[3 * i], f1 = p.gF[3 * i + 1], f2 = p.gF[3 * i + 2];
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int L = 0; L < a.n_leaves; ++L) {
+            const DevLeaf& lf = a.leaves[L];
+            if (lf.ampl == 0.0) continue;
+            PointOut o;
+            o.phi = 0.0; o.rho = 0.0;
+            o.g[0] = o.g[1] = o.g[2] = 0.0;
+            #pragma unroll
+            for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
+            eval_component<AGB_MODE_HESS, double, true, true>(
+                a.comps[lf.comp], lf.sigma * x - lf.g0, lf.sigma * y - lf.g1, lf.sigma * z - lf.g2, o);
+            const double As = lf.ampl * lf.sigma, As2 = As * lf.sigma;
+            g0 += As * o.g[0]; g1 += As * o.g[1]; g2 += As * o.g[2];
+            #pragma unroll
+            for (int q = 0; q < 6; ++q) h[q] += As2 * o.h[q];
+        }
+        // the analytic leaves' VJP (no potential cotangent) and force, as the VJP-force
+        // mode of agb_eval_kernel writes them, then the Multipole part added
+        const double* t = p.stage + (long long)p.stage_rec * __ldg(p.dest + i);
+        double gx[3], F[3];
+        gx[0] = 0.0 * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
+        gx[1] = 0.0 * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
+        gx[2] = 0.0 * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
+        gx[0] += t[0]; gx[1] += t[1]; gx[2] += t[2];
+        if (p.drift) {
+            F[0] = -g0 + t[3]; F[1] = -g1 + t[4]; F[2] = -g2 + t[5];
+        }
+        #pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const long long j = 3 * i + q;
+            const double lxq = p.lx[j] + gx[q];
+            const double lvq = fma(p.dt, lxq, p.lv[j]);
+            p.lx[j] = lxq;
+            p.lv[j] = lvq;
+            p.gF[j] = p.c * lvq;
+            if (p.drift) {
+                const double v = fma(-p.k, F[q], p.vh[j]);
+                p.vh[j] = v;
+                p.x[j] = fma(-p.dt_drift, v, p.x[j]);
+            }
+        }
+    }
+}
+
+static int adjoint_step_check(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                              int n_leaves, int mp_leaf)
+{
+    if (!comps || !leaves || n_comps < 1 || n_leaves < 1 || mp_leaf < 0 || mp_leaf >= n_leaves)
+        return set_err(AGB_ERR_ARG, "agb_adjoint_step: bad component or leaf list");
+    if (n_leaves > AGB_MAX_LEAVES)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_adjoint_step: %d leaves exceed %d", n_leaves,
+                       AGB_MAX_LEAVES);
+    for (int L = 0; L < n_leaves; ++L) {
+        if (leaves[L].comp < 0 || leaves[L].comp >= n_comps)
+            return set_err(AGB_ERR_ARG, "agb_adjoint_step: leaf %d refers to component %d of %d",
+                           L, leaves[L].comp, n_comps);
+        const int kind = comps[leaves[L].comp].kind;
+        if (L == mp_leaf) {
+            if (kind != AGB_KIND_MULTIPOLE)
+                return set_err(AGB_ERR_ARG, "agb_adjoint_step: leaf %d is not a Multipole", L);
+        } else if (kind == AGB_KIND_MULTIPOLE || kind == AGB_KIND_CYLSPLINE) {
+            return set_err(AGB_ERR_UNSUPPORTED, "agb_adjoint_step: leaves other than the "
+                           "Multipole must be analytic");
+        }
+    }
+    return AGB_OK;
+}
+
+extern "C" size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, int n_comps,
+                                                   const agb_leaf* leaves, int n_leaves,
+                                                   int mp_leaf, int64_t n, int flags)
+{
+    if (adjoint_step_check(comps, n_comps, leaves, n_leaves, mp_leaf)) return 0;
+    agb_leaf l = leaves[mp_leaf];
+    l.comp = 0;
+    const BinPlan b = plan_binning(&comps[leaves[mp_leaf].comp], &l, 1, n, AGB_OUT_BIN_ALWAYS);
+    if (!b.on) return 0;
+    return ws_bytes(b, n) + al256(8 * (size_t)((flags & AGB_ADJ_DRIFT) ? 6 : 3) * (size_t)n);
+}
+
+extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                                int n_leaves, int mp_leaf, int precision, double* x, double* vh,
+                                double* lx, double* lv, double* gF, double* g_table, int64_t n,
+                                double dt, double c, double k, double dt_drift, int flags,
+                                void* workspace, size_t workspace_bytes, void* stream)
+{
+    int rc = adjoint_step_check(comps, n_comps, leaves, n_leaves, mp_leaf);
+    if (rc) return rc;
+    if (n < 0) return set_err(AGB_ERR_ARG, "agb_adjoint_step: negative count");
+    if (n == 0) return AGB_OK;
+    const bool drift = (flags & AGB_ADJ_DRIFT) != 0;
+    if (!x || !lx || !lv || !gF || !g_table || (drift && !vh))
+        return set_err(AGB_ERR_ARG, "agb_adjoint_step: null array");
+    AdjKeep keep;
+    keep.on = true;
+    keep.with_force = drift;
+    keep.dest = nullptr;
+    keep.stage = nullptr;
+    rc = multipole_adjoint_impl(&comps[leaves[mp_leaf].comp], &leaves[mp_leaf], x, n, precision,
+                                nullptr, gF, nullptr, nullptr, g_table, workspace,
+                                workspace_bytes, stream, &keep);
+    if (rc) return rc;
+    static thread_local EvalArgs a;
+    memset(&a, 0, sizeof(a));
+    int nl = 0, remap[256];
+    for (int i = 0; i < 256; ++i) remap[i] = -1;
+    int nc = 0;
+    for (int L = 0; L < n_leaves; ++L) {
+        if (L == mp_leaf) continue;
+        const int ci = leaves[L].comp;
+        if (remap[ci] < 0) {
+            if (nc >= AGB_MAX_COMPONENTS)
+                return set_err(AGB_ERR_UNSUPPORTED, "agb_adjoint_step: more than %d components",
+                               AGB_MAX_COMPONENTS);
+            if ((rc = comp_to_dev(comps[ci], a.comps[nc], AGB_PREC_FP64))) return rc;
+            remap[ci] = nc++;
+        }
+        DevLeaf& d = a.leaves[nl++];
+        d.comp = remap[ci];
+        d.sigma = leaves[L].sigma;
+        d.g0 = leaves[L].gamma[0]; d.g1 = leaves[L].gamma[1]; d.g2 = leaves[L].gamma[2];
+        d.ampl = leaves[L].ampl;
+        d.pad = 0;
+    }
+    a.n_leaves = nl;
+    AdjStepPtrs q;
+    q.x = x; q.vh = vh; q.lx = lx; q.lv = lv; q.gF = gF;
+    q.dest = keep.dest; q.stage = keep.stage;
+    q.n = n; q.stage_rec = drift ? 6 : 3; q.drift = drift ? 1 : 0;
+    q.dt = dt; q.c = c; q.k = k; q.dt_drift = dt_drift;
+    adjoint_step_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(a, q);
+    return check_launch("adjoint_step_kernel");
 }
 
 extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,

@@ -323,6 +323,9 @@ struct MPAdjArgs {
     int warp_smem;            // bytes of dynamic shared memory per warp
     int staged;               // 1: interval sums staged in shared memory
     double* force;            // [N,3] or null: this leaf's force added (+=)
+    double* stage;            // binned calls: per sorted position the 3 (6 with force)
+                              // values to add, gathered back by adj_unpermute_add
+    int stage_rec;            // 3, or 6 with the force
     DevComp c;
     DevLeaf leaf;
 };
@@ -741,9 +744,19 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
             multipole_point<AGB_MODE_HESS, R>(c, px, py, pz, o);
         const double As = A * sg, s2 = sg;
         const double* h = o.h;
-        a.gx[3 * i]     += As * (gp * o.g[0] - s2 * (h[0] * gf0 + h[3] * gf1 + h[5] * gf2));
-        a.gx[3 * i + 1] += As * (gp * o.g[1] - s2 * (h[3] * gf0 + h[1] * gf1 + h[4] * gf2));
-        a.gx[3 * i + 2] += As * (gp * o.g[2] - s2 * (h[5] * gf0 + h[4] * gf1 + h[2] * gf2));
+        const double v0 = As * (gp * o.g[0] - s2 * (h[0] * gf0 + h[3] * gf1 + h[5] * gf2));
+        const double v1 = As * (gp * o.g[1] - s2 * (h[3] * gf0 + h[1] * gf1 + h[4] * gf2));
+        const double v2 = As * (gp * o.g[2] - s2 * (h[5] * gf0 + h[4] * gf1 + h[2] * gf2));
+        if (a.stage) {
+            // sorted order: consecutive lanes write consecutive records
+            double* r = a.stage + a.stage_rec * pos;
+            r[0] = v0; r[1] = v1; r[2] = v2;
+            if (a.stage_rec == 6) { r[3] = -As * o.g[0]; r[4] = -As * o.g[1]; r[5] = -As * o.g[2]; }
+            continue;
+        }
+        a.gx[3 * i] += v0;
+        a.gx[3 * i + 1] += v1;
+        a.gx[3 * i + 2] += v2;
         if (a.force) {
             a.force[3 * i] -= As * o.g[0];
             a.force[3 * i + 1] -= As * o.g[1];
@@ -751,4 +764,19 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
         }
     }
     if (swarp) flush();
+}
+
+// the staged records of a binned adjoint added back in input order: point i's
+// record sits at its sorted position dest[i] (coalesced writes, one gather read)
+template <int REC>
+__global__ void __launch_bounds__(256)
+adj_unpermute_add(const int* __restrict__ dest, const double* __restrict__ stage, long long n,
+                  double* __restrict__ gx, double* __restrict__ force)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double* t = stage + (long long)REC * __ldg(dest + i);
+        gx[3 * i] += t[0]; gx[3 * i + 1] += t[1]; gx[3 * i + 2] += t[2];
+        if (REC == 6) { force[3 * i] += t[3]; force[3 * i + 1] += t[4]; force[3 * i + 2] += t[5]; }
+    }
 }

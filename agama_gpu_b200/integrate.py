@@ -149,6 +149,9 @@ class Leapfrog:
         self._graph = None
         self._graph_key = None
         self._step_dev = None
+        # backward steps with table gradients in two launches (agb_adjoint_step) where the
+        # tree allows; False: the separate VJP, kick and drift launches
+        self.fused_adjoint = True
 
     # -- time on the device ----------------------------------------------------------
     def _timed(self, x: torch.Tensor) -> bool:
@@ -415,6 +418,19 @@ class Leapfrog:
             vh.sub_(Fg, alpha=k)
             xc.sub_(vh, alpha=dtg)
 
+        # the whole backward step in two launches (agb_adjoint_step) when the tree is one
+        # regular Multipole and analytic leaves and table gradients are wanted
+        fused_ok = (self.fused_adjoint and tg is not None and on_gpu and
+                    hasattr(self.pot, "_adjoint_step"))
+
+        def fused(xg, g, vh_=None, k_=0.0):
+            if not fused_ok:
+                return False
+            dtg, hg, _ = self._sub[g % S]
+            c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
+            return self.pot._adjoint_step(xg, self._t(g + 1), gF, tg, lx, lv, dtg, c, vh=vh_,
+                                          k=k_, dt_drift=dtg, precision=self.precision)
+
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
             _, xs, vs = at[s]
@@ -428,6 +444,15 @@ class Leapfrog:
                 for g in range(e - 1, s - 1, -1):
                     dtg, hg, _ = self._sub[g % S]
                     need = g > s
+                    if need:
+                        vh_f = vh if vh is not None else at[e][2].clone()
+                        k_f = hg if vh is None else h_next + hg
+                        if fused(xc, g, vh_f, k_f):
+                            vh = vh_f
+                            h_next = hg
+                            continue
+                    elif fused(xc, g):
+                        continue
                     vjp(xc, self._t(g + 1), gF, Fg if need else None)
                     kick(g)
                     if need:
@@ -455,6 +480,8 @@ class Leapfrog:
                     X[g - s].copy_(x)
                     pos[g + 1] = X[g - s]
             for g in range(e - 1, s - 1, -1):
+                if fused(pos[g + 1], g):
+                    continue
                 vjp(pos[g + 1], self._t(g + 1), gF)
                 kick(g)
         if G > 0:

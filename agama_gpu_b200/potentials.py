@@ -525,8 +525,8 @@ class _GPUPotBase:
                 buf = torch.zeros((comp.tables.n_int, comp._n_cols, 6), dtype=torch.float64,
                                   device=dev)
                 acc_dev[comp] = buf
-            nws = int(_lib.lib.agb_multipole_table_vjp_workspace_bytes(ctypes.byref(c),
-                                                                       ctypes.byref(lf), n))
+            nws = int(_lib.lib.agb_multipole_adjoint_workspace_bytes(
+                ctypes.byref(c), ctypes.byref(lf), n, 0 if force_out is None else 1))
             ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
             if force_out is None:
                 rc = _lib.lib.agb_multipole_adjoint(ctypes.byref(c), ctypes.byref(lf),
@@ -541,6 +541,45 @@ class _GPUPotBase:
                                                           buf.data_ptr(), ptr(ws), nws, stream)
                 _lib.check(rc, "agb_multipole_adjoint_force")
         return gx
+
+    def _adjoint_step(self, arr: torch.Tensor, t: float, gF: torch.Tensor, acc_dev: dict,
+                      lx: torch.Tensor, lv: torch.Tensor, dt: float, c: float,
+                      vh: Optional[torch.Tensor] = None, k: float = 0.0, dt_drift: float = 0.0,
+                      precision: Optional[str] = None) -> bool:
+        """One backward leapfrog step in two launches (agb_adjoint_step): the VJP of the
+        tree at arr with cotangent gF of the force, the coefficient gradient of its
+        Multipole added into ``acc_dev`` (device layout, as ``_adjoint_vjp``), the kick
+        lx += gx, lv = fma(dt, lx, lv), gF = c lv, and with ``vh`` the reverse drift
+        vh -= k F(arr), arr -= dt_drift vh, in place.  Returns False (nothing done) when
+        the tree at t is not one regular-structure Multipole plus analytic leaves."""
+        leaves = self._leaves(float(t))
+        mp = [i for i, lf in enumerate(leaves) if lf[0].kind == _lib.KIND_MULTIPOLE]
+        if len(mp) != 1 or any(lf[0].kind == _lib.KIND_CYLSPLINE for lf in leaves):
+            return False
+        comp = leaves[mp[0]][0]
+        if getattr(comp, "_structure", 0) == 0:
+            return False
+        n = arr.shape[0]
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default_precision]
+        cargs = self._c_args(t, dev, leaves)
+        flags = _lib.ADJ_DRIFT if vh is not None else 0
+        nws = int(_lib.lib.agb_adjoint_step_workspace_bytes(*cargs, mp[0], n, flags))
+        if nws == 0:
+            return False
+        buf = acc_dev.get(comp)
+        if buf is None:
+            buf = torch.zeros((comp.tables.n_int, comp._n_cols, 6), dtype=torch.float64,
+                              device=dev)
+            acc_dev[comp] = buf
+        ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        rc = _lib.lib.agb_adjoint_step(
+            *cargs, mp[0], prec, arr.data_ptr(), None if vh is None else vh.data_ptr(),
+            lx.data_ptr(), lv.data_ptr(), gF.data_ptr(), buf.data_ptr(), n, float(dt), float(c),
+            float(k), float(dt_drift), flags, ws.data_ptr(), nws,
+            ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        _lib.check(rc, "agb_adjoint_step")
+        return True
 
     @staticmethod
     def _table_grads_from_device(acc_dev: dict) -> dict:

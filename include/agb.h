@@ -272,9 +272,14 @@ int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
  * into g_xyz [N,3] and accumulates the coefficient gradient into g_table as
  * agb_multipole_table_vjp does.  Needs a regular column structure
  * (AGB_STRUCT_ALL/EVEN).  precision: AGB_PREC_FP64 or AGB_PREC_MIXED (FP32
- * walk and warp reductions, FP64 accumulation).  Same workspace rules and size
- * as agb_multipole_table_vjp.  No counterpart in the reference.
+ * walk and warp reductions, FP64 accumulation).  Same workspace rules as
+ * agb_multipole_table_vjp; with agb_multipole_adjoint_workspace_bytes() bytes
+ * (with_force 1 for agb_multipole_adjoint_force) the per-point results are
+ * written in sorted order and added back in input order by a second launch
+ * instead of scattered read-modify-writes.  No counterpart in the reference.
  */
+size_t agb_multipole_adjoint_workspace_bytes(const agb_component* comp, const agb_leaf* leaf,
+                                             int64_t n, int with_force);
 int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
                           const double* xyz, int64_t n, int precision,
                           const double* g_phi, const double* g_force, double* g_xyz,
@@ -291,6 +296,32 @@ int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
                                 const double* g_phi, const double* g_force,
                                 double* g_xyz, double* force, double* g_table,
                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * One backward step of the leapfrog adjoint for a tree of one Multipole leaf
+ * (mp_leaf, regular column structure) and analytic leaves, in two launches:
+ * the fused Multipole adjoint (coefficient gradient added into g_table, its
+ * per-point VJP and force kept in the workspace in sorted order), then per
+ * particle the analytic leaves' VJP and force at x, the Multipole part added,
+ *     lx += gx;  lv = fma(dt, lx, lv);  gF = c lv                    (the kick)
+ * and with flags & AGB_ADJ_DRIFT the time-reversed drift with the total force
+ *     vh = fma(-k, F, vh);  x = fma(-dt_drift, vh, x).
+ * gF is read as the cotangent of the force at x and overwritten with c lv.
+ * The same arithmetic, in the same order, as agb_eval_vjp_force (analytic
+ * leaves) + agb_multipole_adjoint_force + agb_adjoint_kick + agb_reverse_drift,
+ * with two launches fewer and no intermediate gx / F arrays.  The workspace
+ * (agb_adjoint_step_workspace_bytes, 256-byte aligned) is required.  No
+ * counterpart in the reference.
+ */
+#define AGB_ADJ_DRIFT 1
+size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, int n_comps,
+                                        const agb_leaf* leaves, int n_leaves, int mp_leaf,
+                                        int64_t n, int flags);
+int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
+                     int n_leaves, int mp_leaf, int precision, double* x, double* vh,
+                     double* lx, double* lv, double* gF, double* g_table, int64_t n,
+                     double dt, double c, double k, double dt_drift, int flags,
+                     void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Leapfrog adjoint, per-step vector updates on [N,3] device arrays (one launch each):

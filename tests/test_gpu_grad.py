@@ -644,3 +644,32 @@ def test_cylspline_set_node_tables_on_device():
     a, b = cs.node_gradients(g), ref.node_gradients(gr)
     for m in a:
         assert np.abs(a[m] - b[m]).max() <= 1e-8 * max(np.abs(b[m]).max(), 1e-300), m
+
+
+@pytest.mark.parametrize("reconstruct,k", [("reverse", 8), ("recompute", 8), ("recompute", 1)])
+def test_fused_adjoint_step_equals_separate_launches(reconstruct, k):
+    """agb_adjoint_step (VJP + kick + reverse drift in two launches) gives the same
+    adjoint as the separate VJP, kick and drift launches: dL/dx0 and dL/dv0 bit for
+    bit; the mixed-precision table gradients to the run-to-run spread of their FP32
+    partial sums over 32-point groups (the order of points within an interval bin is
+    not deterministic)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import hernquist_points, nfw_multipole
+    pot = agb.MultipolePotentialGPU(nfw_multipole(lmax=8, n_nodes=40, seed=3)) + \
+        agb.MiyamotoNagaiPotentialGPU(mass=5e10, scaleRadius=3.0, scaleHeight=0.3)
+    xyz = hernquist_points(40_000, 15.0, 9)
+    x0 = torch.from_numpy(xyz).cuda()
+    v0 = torch.from_numpy(np.random.default_rng(2).normal(0, 100.0, xyz.shape)).cuda()
+    lam = torch.from_numpy(np.random.default_rng(3).normal(size=xyz.shape)).cuda()
+    out = []
+    for fused in (True, False):
+        integ = Leapfrog(pot, 2e-3, precision="mixed")
+        integ.fused_adjoint = fused
+        _, _, ck = integ.run(x0, v0, 24, checkpoint_every=k)
+        out.append(integ.adjoint(ck, 24, lam, 0.5 * lam, table_grads=True, reconstruct=reconstruct))
+    (a1, b1, t1), (a2, b2, t2) = out
+    assert torch.equal(a1, a2) and torch.equal(b1, b2)
+    for c in t1:
+        assert float((t1[c] - t2[c]).abs().max()) <= 2e-6 * float(t2[c].abs().max())
