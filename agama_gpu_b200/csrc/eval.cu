@@ -86,10 +86,6 @@ __device__ __forceinline__ void eval_component(const DevComp& c, double x, doubl
 // workspace the kernel instead writes records in sorted order ("stage") and
 // unpermute_kernel gathers them back, reading one record per point and writing
 // every output array contiguously.
-// blocks per SM of the fused Multipole adjoint's grid (one resident at a time)
-#ifndef AGB_ADJ_WAVES
-#define AGB_ADJ_WAVES 2
-#endif
 // internal mode of agb_eval_vjp_force: the VJP plus the force of the same leaves
 // (written to the `hess` pointer as [N,3]) from the same per-point sums
 #define AGB_MODE_VJPF 5
@@ -1253,8 +1249,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
         // per warp: the (U, V) tile, plus the interval accumulator when 8 warps' fit
         // (256 threads at 255 registers; 384 threads at 168 registers spilled and
         // made the backward step 22 % slower)
-        const int grid = (int)std::min<long long>((long long)num_sms() * AGB_ADJ_WAVES,
-                                                  (n + 255) / 256);
+        const int grid = (int)std::min<long long>((long long)num_sms() * 2, (n + 255) / 256);
         const long long warps = (long long)grid * 8, groups = (n + 31) / 32;
         g.chunk = ((groups + warps - 1) / warps) * 32;
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();

@@ -698,19 +698,20 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
             w[0] = sr; w[1] = s2; w[2] = s3; w[3] = s4; w[4] = s4 * sr;
             w[5] = R(2) * sr; w[6] = R(3) * s2; w[7] = R(4) * s3; w[8] = R(5) * s4;
         }
-        MPSums t = {};
+        MPSums tw = {};
         // warp-uniform choice: tile emission (all 32 points in one interval) or atomics
         if (c.structure == AGB_STRUCT_EVEN) {
             if (T.on)
-                mp_adj_walk<R, 2, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+                mp_adj_walk<R, 2, 1>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, tw);
             else
-                mp_adj_walk<R, 2, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+                mp_adj_walk<R, 2, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, tw);
         } else {
             if (T.on)
-                mp_adj_walk<R, 1, 0>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+                mp_adj_walk<R, 1, 0>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, tw);
             else
-                mp_adj_walk<R, 1, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, t);
+                mp_adj_walk<R, 1, 2>(c, kw, (R)s, cth, sth, cph, sph, P1, P2, P3, P4, gbase, T, lane, inside, tw);
         }
+        const MPSums t = tw;
         // monopole column of the coefficient gradient
         {
             const double Bp = t.B * inv_dlogr;
