@@ -18,6 +18,8 @@ OUT_NEGATE = 1
 OUT_NO_BINNING = 2
 OUT_BIN_ALWAYS = 4
 OUT_GRID_SHIFT = 8
+OUT_BLOCK_SHIFT = 12
+OUT_PPT_SHIFT = 16
 BIN_MIN_POINTS = 16384
 
 KIND_MULTIPOLE = 1
@@ -183,6 +185,13 @@ def _load():
     lib.agb_batch_eval.argtypes = [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.agb_batch_eval_ws.restype = ctypes.c_int
+    lib.agb_batch_eval_ws.argtypes = [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+        ctypes.c_void_p]
+    lib.agb_batch_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_batch_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.agb_batch_points.restype = ctypes.c_int64
     lib.agb_batch_points.argtypes = [ctypes.c_void_p]
     lib.agb_batch_tiles.restype = ctypes.c_int
@@ -228,7 +237,8 @@ EXPORTED = [
     "agb_multipole_table_vjp", "agb_multipole_table_vjp_workspace_bytes",
     "agb_multipole_adjoint", "agb_multipole_adjoint_workspace_bytes", "agb_cylspline_table_vjp",
     "agb_adjoint_step", "agb_adjoint_step_workspace_bytes", "agb_adjoint_kick", "agb_reverse_drift",
-    "agb_batch_create", "agb_batch_eval", "agb_batch_points", "agb_batch_tiles",
+    "agb_batch_create", "agb_batch_eval", "agb_batch_eval_ws", "agb_batch_workspace_bytes",
+    "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy", "agb_time_plan_create", "agb_time_plan_destroy",
     "agb_time_plan_leaves_host", "agb_time_plan_leaves", "agb_eval_timed_workspace_bytes",
     "agb_eval_timed", "agb_leapfrog_kick_drift",

@@ -8,6 +8,11 @@ harmonics, how many components), the number of points and the mode:
   contiguous range of the interval-sorted points; more blocks balance the
   cost spread along r better, fewer keep each block's table records in L1
   longer.
+* points per thread (1, 4, 16, 64): instead of a grid, a fixed range of
+  threads x ppt points per block and as many blocks as the points need.
+* block size: 256, 128 or 512 threads (512 in the potential, force and
+  density modes); the resident-block bound scales so every size keeps the
+  same registers per thread.
 * binning: sort the points by radial interval first (default from
   AGB_BIN_MIN_POINTS points on), never, or always.  The sort costs three small
   launches and 32 B of scratch per point; it pays when the harmonic sums are
@@ -40,6 +45,8 @@ from .potentials import _PRECISIONS, prep_xyz
 MODES = {"potential": _lib.MODE_POT, "force": _lib.MODE_GRAD, "forceDeriv": _lib.MODE_HESS,
          "density": _lib.MODE_DENS}
 GRIDS = (1, 2, 4, 8)
+PPTS = (1, 4, 16, 64)                   # points per thread (powers of two)
+BLOCKS = {256: 0, 128: 1, 512: 2}       # threads per block -> AGB_OUT_BLOCK code
 
 _lock = threading.Lock()
 
@@ -98,13 +105,18 @@ def _time(fn, reps: int) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def _candidates(n: int):
-    """(name, extra out_flags) pairs for a call of n points."""
+def _candidates(n: int, mode: int = _lib.MODE_GRAD):
+    """(name, extra out_flags) pairs for a call of n points in this mode."""
     out = []
     bins = [("sort", _lib.OUT_BIN_ALWAYS), ("nosort", _lib.OUT_NO_BINNING)]
+    scheds = [(f"grid{g}", g << _lib.OUT_GRID_SHIFT) for g in GRIDS]
+    scheds += [(f"ppt{p}", (p.bit_length()) << _lib.OUT_PPT_SHIFT) for p in PPTS]
     for name, bf in bins:
-        for g in GRIDS:
-            out.append((f"{name}/grid{g}", bf | (g << _lib.OUT_GRID_SHIFT)))
+        for bs, code in BLOCKS.items():
+            if bs == 512 and mode == _lib.MODE_HESS:
+                continue                 # the Hessian kernel runs 256 threads at most
+            for sname, sf in scheds:
+                out.append((f"{name}/b{bs}/{sname}", bf | (code << _lib.OUT_BLOCK_SHIFT) | sf))
     return out
 
 
@@ -130,13 +142,13 @@ def autotune(pot, xyz, mode: str = "force", t: float = 0.0, precision: Optional[
     saved = dict(pot.__dict__.get("_tuned", {}))
     times = {}
     try:
-        for name, flags in _candidates(n):
+        for name, flags in _candidates(n, m):
             _set(pot, m, prec, n, flags)
             times[name] = _time(lambda: pot._launch(arr, t, m, True, precision=pname), reps)
     finally:
         pot.__dict__["_tuned"] = saved
     best = min(times, key=times.get)
-    flags = dict(_candidates(n))[best]
+    flags = dict(_candidates(n, m))[best]
     _set(pot, m, prec, n, flags)
     if persist:
         _store(signature(pot, m, prec, n, t), {"flags": flags, "best": best, "ms": times})

@@ -36,7 +36,7 @@ class BatchedPotentialGPU(_GPUPotBase):
     """
 
     def __init__(self, potentials: Sequence, counts: Sequence[int], tile_points: int = 4096,
-                 precision: Optional[str] = None) -> None:
+                 precision: Optional[str] = None, presort: bool = True) -> None:
         from .integrate import is_static
         pots = list(potentials)
         counts = np.asarray(counts, dtype=np.int64)
@@ -53,7 +53,12 @@ class BatchedPotentialGPU(_GPUPotBase):
         self.n_points = int(self.offsets[-1])
         self.tile_points = int(tile_points)
         self.precision = precision
+        # device-wide pre-sort of every unit's points by interval before the work-queue
+        # launch (agb_batch_eval_ws), in a workspace the object keeps per device,
+        # precision and stream
+        self.presort = bool(presort)
         self._plans = {}
+        self._ws = {}
 
     def __add__(self, other):
         raise TypeError("a batch of independent potentials cannot be summed")
@@ -126,9 +131,19 @@ class BatchedPotentialGPU(_GPUPotBase):
         plan = self._plan(dev, prec)
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         stream = torch.cuda.current_stream(dev).cuda_stream
-        rc = _lib.lib.agb_batch_eval(plan, arr.data_ptr(), mode, ptr(phi), ptr(grad), ptr(hess),
-                                     ptr(rho), _lib.OUT_NEGATE, ctypes.c_void_p(stream))
-        _lib.check(rc, "agb_batch_eval")
+        ws, nws = None, 0
+        if self.presort:
+            nws = int(_lib.lib.agb_batch_workspace_bytes(plan, mode))
+            if nws:
+                key = (dev.index, prec, stream)
+                ws = self._ws.get(key)
+                if ws is None or ws.numel() < nws:
+                    ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+                    self._ws[key] = ws
+        rc = _lib.lib.agb_batch_eval_ws(plan, arr.data_ptr(), mode, ptr(phi), ptr(grad), ptr(hess),
+                                        ptr(rho), _lib.OUT_NEGATE, ptr(ws), nws,
+                                        ctypes.c_void_p(stream))
+        _lib.check(rc, "agb_batch_eval_ws")
         return phi, grad, hess, rho
 
     def _vjp(self, *args, **kw):
@@ -148,6 +163,7 @@ class BatchedPotentialGPU(_GPUPotBase):
             except Exception:   # interpreter shutdown
                 pass
         self._plans = {}
+        self._ws = {}
         # CUDA graphs captured over the old plans must not replay them
         self.plan_generation = getattr(self, "plan_generation", 0) + 1
 

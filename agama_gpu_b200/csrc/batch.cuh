@@ -34,11 +34,13 @@ struct BatchArgs {
     int* counter;             // device, zero at launch
     int n_tiles;
     int out_flags;
-    const double* xyz;
+    const double* xyz;        // presorted: the sorted copy of the points
     double* phi;
     double* grad;
     double* hess;
     double* rho;
+    const int* perm;          // presorted: sorted position -> row of the caller's arrays
+    double* stage;            // presorted with room: per-position output records
 };
 
 template <int MODE, typename R>
@@ -58,7 +60,9 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         const int l0 = a.unit_leaf[T.unit], l1 = a.unit_leaf[T.unit + 1];
         const BinKey K = a.ukey[T.unit];
         const int nb = K.n_int + 2;
-        const bool sorted = K.n_int >= 0 && nb <= AGB_BATCH_MAX_BINS && T.count <= AGB_BATCH_SORT_MAX;
+        // points pre-sorted by agb_batch_eval_ws: a tile is a run of sorted positions
+        const bool sorted = !a.perm && K.n_int >= 0 && nb <= AGB_BATCH_MAX_BINS &&
+                            T.count <= AGB_BATCH_SORT_MAX;
         if (sorted) {
             for (int q = threadIdx.x; q < nb; q += blockDim.x) s_hist[q] = 0;
             __syncthreads();
@@ -92,8 +96,9 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
             __syncthreads();
         }
         for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
-            const long long i = T.start + (sorted ? (int)s_order[j] : j);
-            const double x = a.xyz[3 * i], y = a.xyz[3 * i + 1], z = a.xyz[3 * i + 2];
+            const long long pos = T.start + (sorted ? (int)s_order[j] : j);
+            const long long i = a.perm ? (long long)__ldg(a.perm + pos) : pos;
+            const double x = a.xyz[3 * pos], y = a.xyz[3 * pos + 1], z = a.xyz[3 * pos + 2];
             double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
             double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             for (int L = l0; L < l1; ++L) {
@@ -122,11 +127,23 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
                     }
                 }
             }
+            const double sg = (a.out_flags & AGB_OUT_NEGATE) ? -1.0 : 1.0;
+            if (a.stage) {               // sorted order: contiguous records, then a gather
+                constexpr int REC = stage_rec(MODE);
+                double* o = a.stage + REC * pos;
+                if (MODE == AGB_MODE_DENS) { o[0] = rho; continue; }
+                o[0] = phi;
+                if (MODE != AGB_MODE_POT) { o[1] = sg * g0; o[2] = sg * g1; o[3] = sg * g2; }
+                if (MODE == AGB_MODE_HESS) {
+                    #pragma unroll
+                    for (int q = 0; q < 6; ++q) o[4 + q] = sg * h[q];
+                }
+                continue;
+            }
             if (MODE == AGB_MODE_DENS) {
                 a.rho[i] = rho;
                 continue;
             }
-            const double sg = (a.out_flags & AGB_OUT_NEGATE) ? -1.0 : 1.0;
             if (a.phi) a.phi[i] = phi;
             if (MODE != AGB_MODE_POT && a.grad) {
                 a.grad[3 * i] = sg * g0; a.grad[3 * i + 1] = sg * g1; a.grad[3 * i + 2] = sg * g2;
@@ -136,6 +153,67 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
                 for (int q = 0; q < 6; ++q) a.hess[6 * i + q] = sg * h[q];
             }
         }
+    }
+}
+
+// Device-wide pre-sort of a batch (agb_batch_eval_ws): every unit's points by the
+// radial interval of its sort key, each unit within its own rows (unit u owns
+// global bins [ubin[u], ubin[u+1]) and the bins run unit by unit), so a tile --
+// a run of sorted positions -- spans a few intervals instead of all of them and
+// its blocks' table reads hit L1.  One block per tile; block-local histograms in
+// shared memory, one global atomic per (tile, bin).
+__global__ void __launch_bounds__(256)
+batch_bin_count(const BatchTile* __restrict__ tiles, const BinKey* __restrict__ ukey,
+                const int* __restrict__ ubin, const double* __restrict__ xyz,
+                int* __restrict__ keys, int* __restrict__ counts)
+{
+    extern __shared__ int hist[];
+    const BatchTile T = tiles[blockIdx.x];
+    const BinKey K = ukey[T.unit];
+    const int b0 = ubin[T.unit], nb = ubin[T.unit + 1] - b0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) hist[q] = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
+        const long long i = T.start + j;
+        const int k = nb > 1 ? bin_of(K, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]) : 0;
+        keys[i] = k;
+        atomicAdd(&hist[k], 1);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nb; q += blockDim.x)
+        if (hist[q]) atomicAdd(&counts[b0 + q], hist[q]);
+}
+
+// keys[i] becomes the sorted position of row i (the gather index of unpermute_kernel)
+__global__ void __launch_bounds__(256)
+batch_bin_scatter(const BatchTile* __restrict__ tiles, const int* __restrict__ ubin,
+                  const double* __restrict__ xyz, int* __restrict__ keys,
+                  int* __restrict__ cursor, int* __restrict__ perm, double* __restrict__ xs)
+{
+    extern __shared__ int sm[];
+    const BatchTile T = tiles[blockIdx.x];
+    const int b0 = ubin[T.unit], nb = ubin[T.unit + 1] - b0;
+    int* hist = sm;
+    int* base = sm + nb;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) hist[q] = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < T.count; j += blockDim.x) atomicAdd(&hist[keys[T.start + j]], 1);
+    __syncthreads();
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+        const int c = hist[q];
+        base[q] = c ? atomicAdd(&cursor[b0 + q], c) : 0;
+        hist[q] = 0;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
+        const long long i = T.start + j;
+        const int k = keys[i];
+        const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
+        perm[pos] = (int)i;
+        keys[i] = (int)pos;
+        xs[3 * pos] = xyz[3 * i];
+        xs[3 * pos + 1] = xyz[3 * i + 1];
+        xs[3 * pos + 2] = xyz[3 * i + 2];
     }
 }
 
@@ -152,6 +230,9 @@ struct agb_batch {
     const BatchTile* tiles;
     const BinKey* ukey;
     int* counter;
+    const int* ubin;          // device [n_units + 1]: first global bin of each unit
+    int n_bins;               // bins of the pre-sort over all units (0: not pre-sortable)
+    int max_unit_bins;        // largest unit's bin count (shared-memory histogram size)
 };
 
 // per-point flop estimate of a leaf (the roofline convention), for tile ordering
@@ -259,7 +340,23 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
     const size_t o_t = al256(o_u + sizeof(int) * (size_t)(n_units + 1));
     const size_t o_y = al256(o_t + sizeof(BatchTile) * (size_t)(n_tiles > 0 ? n_tiles : 1));
     const size_t o_k = al256(o_y + sizeof(BinKey) * (size_t)n_units);
-    const size_t bytes = o_k + 256;
+    const size_t o_b = o_k + 256;
+    const size_t bytes = al256(o_b + sizeof(int) * (size_t)(n_units + 1));
+    // global bins of the pre-sort: unit u owns n_int + 2 of them (1 without a key)
+    int* hb = rc ? nullptr : (int*)malloc(sizeof(int) * (size_t)(n_units + 1));
+    if (!rc && !hb) rc = set_err(AGB_ERR_DEVICE, "agb_batch_create: host allocation failed");
+    long long n_bins = 0;
+    int max_unit_bins = 1;
+    for (int u = 0; u < n_units && !rc; ++u) {
+        hb[u] = (int)std::min<long long>(n_bins, 0x7fffffffLL);
+        const int nb = hk[u].n_int >= 0 ? hk[u].n_int + 2 : 1;
+        n_bins += nb;
+        max_unit_bins = std::max(max_unit_bins, nb);
+    }
+    if (!rc) hb[n_units] = (int)std::min<long long>(n_bins, 0x7fffffffLL);
+    // (positions are 32-bit in the sort's keys and permutation)
+    const bool presortable = n_bins < (1LL << 30) && max_unit_bins <= AGB_MAX_BINS &&
+                             n_points < 0x7fffffffLL;
     agb_batch* p = nullptr;
     if (!rc) {
         p = (agb_batch*)calloc(1, sizeof(agb_batch));
@@ -284,6 +381,8 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
         ok = ok && cudaMemcpy(m + o_y, hk, sizeof(BinKey) * (size_t)n_units,
                               cudaMemcpyHostToDevice) == cudaSuccess;
         ok = ok && cudaMemset(m + o_k, 0, 256) == cudaSuccess;
+        ok = ok && cudaMemcpy(m + o_b, hb, sizeof(int) * (size_t)(n_units + 1),
+                              cudaMemcpyHostToDevice) == cudaSuccess;
         if (!ok) rc = set_err(AGB_ERR_DEVICE, "agb_batch_create: upload of the plan failed");
         p->precision = precision;
         p->n_units = n_units;
@@ -295,8 +394,11 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
         p->tiles = (const BatchTile*)(m + o_t);
         p->ukey = (const BinKey*)(m + o_y);
         p->counter = (int*)(m + o_k);
+        p->ubin = (const int*)(m + o_b);
+        p->n_bins = presortable ? (int)n_bins : 0;
+        p->max_unit_bins = max_unit_bins;
     }
-    free(hc); free(hl); free(ucost); free(hk); free(ht);
+    free(hc); free(hl); free(ucost); free(hk); free(ht); free(hb);
     if (rc) {
         if (p) {
             if (p->mem) cudaFree(p->mem);
@@ -324,6 +426,24 @@ extern "C" void agb_batch_destroy(agb_batch* plan)
     free(plan);
 }
 
+// Scratch of the pre-sort: keys and perm (4 B per point each), the sorted copy of
+// the points (24 B), the bin counters and cursors, then (optional) the sorted-order
+// output records.
+static size_t batch_ws_bytes(const agb_batch* p)
+{
+    const size_t n = (size_t)p->n_points;
+    return 2 * al256(4 * n) + al256(24 * n) + 2 * al256(4 * (size_t)p->n_bins);
+}
+
+extern "C" size_t agb_batch_workspace_bytes(const agb_batch* plan, int mode)
+{
+    if (!plan || plan->n_bins == 0 || plan->n_tiles == 0) return 0;
+    if (mode != AGB_MODE_POT && mode != AGB_MODE_GRAD && mode != AGB_MODE_HESS &&
+        mode != AGB_MODE_DENS)
+        return 0;
+    return batch_ws_bytes(plan) + al256(8 * (size_t)stage_rec(mode) * (size_t)plan->n_points);
+}
+
 template <int MODE, typename R>
 static int launch_batch(const BatchArgs& a, cudaStream_t st)
 {
@@ -334,8 +454,49 @@ static int launch_batch(const BatchArgs& a, cudaStream_t st)
     return check_launch("agb_batch_kernel");
 }
 
+static std::atomic<unsigned long long> g_batch_bin_attr{0};     // one bit per device
+
+static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchArgs& a,
+                         cudaStream_t st)
+{
+    const size_t n = (size_t)p->n_points;
+    int* keys = (int*)ws;
+    int* perm = (int*)(ws + al256(4 * n));
+    double* xs = (double*)(ws + 2 * al256(4 * n));
+    int* counts = (int*)(ws + 2 * al256(4 * n) + al256(24 * n));
+    int* cursor = (int*)((char*)counts + al256(4 * (size_t)p->n_bins));
+    const unsigned long long bit = 1ull << current_device();
+    if (!(g_batch_bin_attr.load(std::memory_order_acquire) & bit)) {
+        cudaFuncSetAttribute(batch_bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             4 * AGB_MAX_BINS);
+        cudaFuncSetAttribute(batch_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             8 * AGB_MAX_BINS);
+        g_batch_bin_attr.fetch_or(bit, std::memory_order_release);
+    }
+    if (cudaMemsetAsync(counts, 0, 4 * (size_t)p->n_bins, st) != cudaSuccess)
+        return set_err(AGB_ERR_DEVICE, "agb_batch_eval_ws: memset of the bin counts failed");
+    const size_t h = 4 * (size_t)p->max_unit_bins;
+    batch_bin_count<<<p->n_tiles, 256, h, st>>>(p->tiles, p->ukey, p->ubin, xyz, keys, counts);
+    int rc = check_launch("batch_bin_count");
+    if (rc) return rc;
+    bin_scan<<<1, 1024, 0, st>>>(counts, cursor, p->n_bins);
+    if ((rc = check_launch("bin_scan"))) return rc;
+    batch_bin_scatter<<<p->n_tiles, 256, 2 * h, st>>>(p->tiles, p->ubin, xyz, keys, cursor, perm, xs);
+    if ((rc = check_launch("batch_bin_scatter"))) return rc;
+    a.xyz = xs;
+    a.perm = perm;
+    return AGB_OK;
+}
+
 extern "C" int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode, double* phi,
                               double* grad, double* hess, double* rho, int out_flags, void* stream)
+{
+    return agb_batch_eval_ws(plan, xyz, mode, phi, grad, hess, rho, out_flags, nullptr, 0, stream);
+}
+
+extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int mode, double* phi,
+                                 double* grad, double* hess, double* rho, int out_flags,
+                                 void* workspace, size_t workspace_bytes, void* stream)
 {
     if (!plan) return set_err(AGB_ERR_ARG, "agb_batch_eval: plan is null");
     switch (mode) {
@@ -359,13 +520,37 @@ extern "C" int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode
     a.n_tiles = plan->n_tiles;
     a.out_flags = out_flags; a.xyz = xyz;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
+    a.perm = nullptr; a.stage = nullptr;
+    int rc = AGB_OK;
+    const int* dest = nullptr;
+    if (workspace && plan->n_bins > 0) {
+        const size_t need = batch_ws_bytes(plan);
+        if (((uintptr_t)workspace & 255u) || workspace_bytes < need)
+            return set_err(AGB_ERR_ARG, "agb_batch_eval_ws: workspace of %zu bytes (256-byte "
+                           "aligned) is smaller than the %zu bytes of the pre-sort",
+                           workspace_bytes, need);
+        if ((rc = batch_presort(plan, xyz, (char*)workspace, a, st))) return rc;
+        if (workspace_bytes >= agb_batch_workspace_bytes(plan, mode)) {
+            a.stage = (double*)((char*)workspace + need);
+            dest = (const int*)workspace;
+        }
+    }
     if (cudaMemsetAsync(plan->counter, 0, sizeof(int), st) != cudaSuccess)
         return set_err(AGB_ERR_DEVICE, "agb_batch_eval: reset of the work queue failed");
     const bool mixed = plan->precision == AGB_PREC_MIXED;
     switch (mode) {
-    case AGB_MODE_POT:  return mixed ? launch_batch<AGB_MODE_POT, float>(a, st)  : launch_batch<AGB_MODE_POT, double>(a, st);
-    case AGB_MODE_GRAD: return mixed ? launch_batch<AGB_MODE_GRAD, float>(a, st) : launch_batch<AGB_MODE_GRAD, double>(a, st);
-    case AGB_MODE_HESS: return mixed ? launch_batch<AGB_MODE_HESS, float>(a, st) : launch_batch<AGB_MODE_HESS, double>(a, st);
-    default:            return mixed ? launch_batch<AGB_MODE_DENS, float>(a, st) : launch_batch<AGB_MODE_DENS, double>(a, st);
+    case AGB_MODE_POT:  rc = mixed ? launch_batch<AGB_MODE_POT, float>(a, st)  : launch_batch<AGB_MODE_POT, double>(a, st); break;
+    case AGB_MODE_GRAD: rc = mixed ? launch_batch<AGB_MODE_GRAD, float>(a, st) : launch_batch<AGB_MODE_GRAD, double>(a, st); break;
+    case AGB_MODE_HESS: rc = mixed ? launch_batch<AGB_MODE_HESS, float>(a, st) : launch_batch<AGB_MODE_HESS, double>(a, st); break;
+    default:            rc = mixed ? launch_batch<AGB_MODE_DENS, float>(a, st) : launch_batch<AGB_MODE_DENS, double>(a, st); break;
     }
+    if (rc || !a.stage) return rc;
+    const long long n = plan->n_points;
+    switch (mode) {
+    case AGB_MODE_POT:  unpermute_kernel<AGB_MODE_POT><<<grid_for(n), 256, 0, st>>>(dest, a.stage, n, phi, grad, hess, rho); break;
+    case AGB_MODE_GRAD: unpermute_kernel<AGB_MODE_GRAD><<<grid_for(n), 256, 0, st>>>(dest, a.stage, n, phi, grad, hess, rho); break;
+    case AGB_MODE_HESS: unpermute_kernel<AGB_MODE_HESS><<<grid_for(n), 256, 0, st>>>(dest, a.stage, n, phi, grad, hess, rho); break;
+    default:            unpermute_kernel<AGB_MODE_DENS><<<grid_for(n), 256, 0, st>>>(dest, a.stage, n, phi, grad, hess, rho); break;
+    }
+    return check_launch("unpermute_kernel");
 }

@@ -132,9 +132,16 @@ unpermute_kernel(const int* __restrict__ dest, const double* __restrict__ stage,
 // DYN: the leaves come from device memory (agb_eval_timed: computed by
 // time_leaves_kernel from a device-resident time), copied to shared memory once
 // per block; otherwise they are kernel parameters.
-template <int MODE, typename R, bool AN = false, bool DYN = false>
-__global__ void __launch_bounds__(256, ((MODE == AGB_MODE_HESS || MODE == AGB_MODE_VJP ||
-                                       MODE == AGB_MODE_VJPF) && !AN) ? 1 : (AN ? 3 : 2))
+// BS: threads per block (AGB_OUT_BLOCK); the resident-block bound scales with it so
+// that every block size keeps the register budget of the 256-thread shape.
+__host__ __device__ constexpr int eval_min_blocks(int mode, bool an, int bs)
+{
+    return (((mode == AGB_MODE_HESS || mode == AGB_MODE_VJP || mode == AGB_MODE_VJPF) && !an)
+            ? 1 : (an ? 3 : 2)) * 256 / bs;
+}
+
+template <int MODE, typename R, bool AN = false, bool DYN = false, int BS = 256>
+__global__ void __launch_bounds__(BS, eval_min_blocks(MODE, AN, BS))
 agb_eval_kernel(const __grid_constant__ EvalArgs a)
 {
     // the VJP modes evaluate every component with its Hessian and contract at the end
@@ -321,11 +328,11 @@ static int grid_for(long long n)
 static int default_waves(long long n) { return n > (1LL << 21) ? 1 : 2; }
 
 // resident blocks per SM of one instantiation
-template <int MODE, typename R, bool AN, bool DYN = false>
+template <int MODE, typename R, bool AN, bool DYN = false, int BS = 256>
 static int eval_blocks_per_sm()
 {
     static std::atomic<int> per_sm[AGB_MAX_DEVICES];
-    return blocks_per_sm(per_sm, agb_eval_kernel<MODE, R, AN, DYN>, 256);
+    return blocks_per_sm(per_sm, agb_eval_kernel<MODE, R, AN, DYN, BS>, BS);
 }
 
 // points that one wave of resident threads holds (one point per thread)
@@ -335,16 +342,48 @@ static long long eval_wave_points()
     return (long long)num_sms() * eval_blocks_per_sm<MODE, R, AN>() * 256;
 }
 
+// The launch shape.  Each block takes one contiguous range of a.chunk points:
+// AGB_OUT_PPT(p) fixes the range at BS x 2^(p-1) points (points per thread) and
+// the grid grows with n; otherwise the grid is AGB_OUT_GRID's blocks per resident
+// slot (default_waves when unset) and the range is what the points need.
+template <int MODE, typename R, bool AN, bool DYN, int BS>
+static void launch_eval_bs(EvalArgs& a, cudaStream_t st)
+{
+    const int p = (a.out_flags >> AGB_OUT_PPT_SHIFT) & 15;
+    long long grid;
+    if (p) {
+        long long chunk = (long long)BS << (p - 1);
+        if ((a.n + chunk - 1) / chunk > 0x7fffffffLL)      // the grid's x limit
+            chunk = ((a.n + 0x7ffffffeLL) / 0x7fffffffLL + 31) / 32 * 32;
+        a.chunk = chunk;
+        grid = (a.n + chunk - 1) / chunk;
+        if (grid < 1) grid = 1;
+    } else {
+        const int per_sm = eval_blocks_per_sm<MODE, R, AN, DYN, BS>();
+        const long long want = (a.n + BS - 1) / BS;
+        const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
+        const long long slots = (long long)num_sms() * per_sm * (w ? w : default_waves(a.n));
+        grid = want < slots ? (want > 0 ? want : 1) : slots;
+        a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
+    }
+    agb_eval_kernel<MODE, R, AN, DYN, BS><<<(int)grid, BS, 0, st>>>(a);
+}
+
+// AGB_OUT_BLOCK picks 128 or 512 threads per block for the host-leaf kernels of
+// the four evaluation modes; 512 only where the 256-thread shape holds two blocks
+// per SM (the Hessian kernel's 255 registers a thread leave room for 256 threads).
+// Device-time leaves, the analytic-only and the VJP kernels run 256 threads.
 template <int MODE, typename R, bool AN = false, bool DYN = false>
 static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
-    const int per_sm = eval_blocks_per_sm<MODE, R, AN, DYN>();
-    const long long want = (a.n + 255) / 256;
-    const int w = (a.out_flags >> AGB_OUT_GRID_SHIFT) & 15;
-    const long long slots = (long long)num_sms() * per_sm * (w ? w : default_waves(a.n));
-    const long long grid = want < slots ? (want > 0 ? want : 1) : slots;
-    a.chunk = ((a.n + grid - 1) / grid + 31) / 32 * 32;
-    agb_eval_kernel<MODE, R, AN, DYN><<<(int)grid, 256, 0, st>>>(a);
+    constexpr bool SHAPES = !AN && !DYN && MODE != AGB_MODE_VJP && MODE != AGB_MODE_VJPF;
+    const int b = (a.out_flags >> AGB_OUT_BLOCK_SHIFT) & 3;
+    if constexpr (SHAPES) {
+        if (b == 1) return launch_eval_bs<MODE, R, AN, DYN, 128>(a, st);
+        if constexpr (eval_min_blocks(MODE, AN, 256) >= 2)
+            if (b == 2) return launch_eval_bs<MODE, R, AN, DYN, 512>(a, st);
+    }
+    launch_eval_bs<MODE, R, AN, DYN, 256>(a, st);
 }
 
 static bool analytic_only(const EvalArgs& a)
@@ -645,6 +684,8 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
 {
     int rc = validate(comps, n_comps, leaves, n_leaves, xyz, n, mode, precision, phi, grad, hess, rho);
     if (rc) return rc;
+    if (((out_flags >> AGB_OUT_BLOCK_SHIFT) & 3) == 3)
+        return set_err(AGB_ERR_ARG, "agb_eval: block-size code 3 in out_flags is not defined");
     if (n == 0) return AGB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     static thread_local EvalArgs a;

@@ -726,8 +726,8 @@ class _GPUPotBase:
         if wave and len(bounds) > 2 and all((hi - lo) % wave == 0 for lo, hi in bounds[:-1]):
             # chunks in whole waves: one resident block per slot, so every thread of
             # a launch takes the same number of passes (unless a tuned shape is set)
-            flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 else f | (1 << _lib.OUT_GRID_SHIFT)
-                     for m, f in flags.items()}
+            flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 or (f >> _lib.OUT_PPT_SHIFT) & 15
+                     else f | (1 << _lib.OUT_GRID_SHIFT) for m, f in flags.items()}
         nws = max((int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3],
                                                          m, flags[m])) for m in sizes), default=0)
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731

@@ -59,11 +59,23 @@ extern "C" {
 #define AGB_OUT_NEGATE     1   /* write -grad (force) and -Hessian (forceDeriv layout) */
 #define AGB_OUT_NO_BINNING 2   /* evaluate the points in input order (no scratch memory) */
 #define AGB_OUT_BIN_ALWAYS 4   /* sort by interval even below AGB_BIN_MIN_POINTS points */
-/* bits 8-11: blocks per resident slot of the evaluation kernel's grid, 1-15
-   (0: the default, 4).  Results do not depend on it: a launch-shape knob for
-   the autotuner (agama_gpu_b200/autotune.py).  No counterpart in the reference. */
-#define AGB_OUT_GRID_SHIFT 8
-#define AGB_OUT_GRID(w)    (((w) & 15) << AGB_OUT_GRID_SHIFT)
+/* Launch-shape knobs of the evaluation kernel.  Results do not depend on them;
+   the autotuner (agama_gpu_b200/autotune.py) times them.  No counterpart in the
+   reference, whose launch shape is fixed.
+   bits 8-11:  blocks per resident slot of the grid, 1-15 (0: the default, one
+               slot's worth above 2^21 points, two below).
+   bits 12-13: threads per block: 0 = 256, 1 = 128, 2 = 512 (512 in the potential,
+               force and density modes; the Hessian modes keep 256).  Host-leaf
+               calls of agb_eval / agb_eval_ws / agb_eval_static only.
+   bits 16-19: points per thread p, 1-15: each block takes a contiguous range of
+               threads x 2^(p-1) points and the grid grows with n (overrides
+               bits 8-11; 0: off). */
+#define AGB_OUT_GRID_SHIFT  8
+#define AGB_OUT_GRID(w)     (((w) & 15) << AGB_OUT_GRID_SHIFT)
+#define AGB_OUT_BLOCK_SHIFT 12
+#define AGB_OUT_BLOCK(b)    (((b) & 3) << AGB_OUT_BLOCK_SHIFT)
+#define AGB_OUT_PPT_SHIFT   16
+#define AGB_OUT_PPT(p)      (((p) & 15) << AGB_OUT_PPT_SHIFT)
 
 /* agb_eval sorts the points by the radial interval of its heaviest Multipole
    leaf (a counting sort in device scratch) when there are at least this many */
@@ -397,6 +409,26 @@ int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode,
 int64_t agb_batch_points(const agb_batch* plan);
 int     agb_batch_tiles(const agb_batch* plan);
 void    agb_batch_destroy(agb_batch* plan);
+
+/*
+ * agb_batch_eval with a caller-owned device workspace (256-byte aligned) that
+ * turns on a device-wide pre-sort: every unit's points are counting-sorted by
+ * the radial interval of the unit's heaviest Multipole, each unit within its own
+ * rows, so that a tile is a run of sorted points spanning a few intervals and
+ * the kernel's table reads hit L1 (the in-tile sort is then skipped).  Three
+ * small launches before the kernel.  agb_batch_workspace_bytes(plan, mode) is
+ * the size that also holds sorted-order output records (gathered back by one
+ * more launch, every output array written contiguously); a workspace of at
+ * least the pre-sort's own part (32 bytes per point plus the bin counters) but
+ * smaller makes the kernel write each point's outputs in place.  Returns 0 when
+ * the plan cannot be pre-sorted (a unit with more than 8190 intervals); a null
+ * workspace is agb_batch_eval.  Results equal agb_batch_eval's bit for bit.
+ */
+size_t  agb_batch_workspace_bytes(const agb_batch* plan, int mode);
+int     agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int mode,
+                          double* phi, double* grad, double* hess, double* rho,
+                          int out_flags, void* workspace, size_t workspace_bytes,
+                          void* stream);
 
 /*
  * Time-dependent leaves evaluated on the device.  The reference evaluates the

@@ -54,6 +54,10 @@ def test_argument_errors_need_no_gpu():
     assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, ctypes.c_void_p(16),
                              None, None, 0, None) == 0
     assert _lib.lib.agb_eval_workspace_bytes(comps, 1, leaves, 1, 10**6, 0) == 0   # no Multipole
+    # an undefined block-size code among the launch-shape bits
+    rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
+                           ctypes.c_void_p(16), None, None, 3 << _lib.OUT_BLOCK_SHIFT, None)
+    assert rc == -1 and "block-size code" in _lib.last_error()
     # the wave size: 0 for bad arguments, before any CUDA call
     assert _lib.lib.agb_eval_wave_points(None, 0, None, 0, 1, 0) == 0
     leaves[0].comp = 3

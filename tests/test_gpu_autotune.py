@@ -23,16 +23,23 @@ def test_launch_shapes_agree(n, tmp_path, monkeypatch):
     x = torch.from_numpy(hernquist_points(n, 10.0, 4)).cuda()
     ref = pot.force(x)
     for prec in ("fp64", "mixed"):
-        base = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
-        for name, flags in autotune._candidates(n):
-            autotune._set(pot, _lib.MODE_GRAD, _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED,
-                          n, flags)
-            got = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
-            for g, b in zip(got[:2], base[:2]):
-                assert float((g - b).abs().max()) <= 1e-14 * float(b.abs().max()), (prec, name)
-        pot.__dict__.pop("_tuned", None)
+        pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
+        for mode in (_lib.MODE_GRAD, _lib.MODE_POT, _lib.MODE_HESS, _lib.MODE_DENS):
+            base = pot._launch(x, 0.0, mode, True, precision=prec)
+            cands = autotune._candidates(n, mode)
+            if mode != _lib.MODE_GRAD:       # every block size and both schedule kinds
+                cands = [c for c in cands if c[0].endswith(("/grid2", "/ppt16"))]
+            for name, flags in cands:
+                autotune._set(pot, mode, pc, n, flags)
+                got = pot._launch(x, 0.0, mode, True, precision=prec)
+                for g, b in zip(got, base):
+                    if b is not None:
+                        assert float((g - b).abs().max()) <= 1e-14 * float(b.abs().max()), \
+                            (prec, mode, name)
+            pot.__dict__.pop("_tuned", None)
     res = autotune.autotune(pot, x, mode="force", precision="mixed", reps=2)
-    assert res["best"] in res["ms"] and len(res["ms"]) == 2 * len(autotune.GRIDS)
+    assert res["best"] in res["ms"]
+    assert len(res["ms"]) == len(autotune._candidates(n, _lib.MODE_GRAD)) == 48
     assert (_lib.MODE_GRAD, _lib.PREC_MIXED, n.bit_length()) in pot._tuned
     assert torch.equal(pot.force(x), ref)                 # fp64 calls keep their own shape
     rec = json.loads((tmp_path / "cache.json").read_text())

@@ -73,6 +73,49 @@ def test_batch_matches_per_unit_calls(prec, mode):
             assert err <= 1e-14, (u, err)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_presort_equals_in_tile_sort(prec):
+    """The device-wide pre-sort (agb_batch_eval_ws) changes only the order in which
+    points are visited: bit for bit the in-tile sort's results, with sorted-order
+    output records and with outputs written in place (a workspace without room for
+    the records)."""
+    import ctypes
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    units, counts = _units()
+    plain = agb.BatchedPotentialGPU(units, counts, tile_points=512, presort=False)
+    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512)
+    x = torch.from_numpy(_points(plain.n_points, 8)).cuda()
+    pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
+    plan = sorted_._plan(x.device, pc)
+    n = plain.n_points
+    for mode, rec in ((0, 1), (1, 4), (2, 10), (3, 1)):
+        want = plain._launch(x, 0.0, mode, True, precision=prec)
+        got = sorted_._launch(x, 0.0, mode, True, precision=prec)
+        for g, w in zip(got, want):
+            if w is not None:
+                assert torch.equal(g, w), (prec, mode)
+        full = int(_lib.lib.agb_batch_workspace_bytes(plan, mode))
+        part = full - (8 * rec * n + 255) // 256 * 256
+        assert part > 0
+        ws = torch.empty(part, dtype=torch.uint8, device=x.device)
+        outs = [None if w is None else torch.full_like(w, float("nan")) for w in want]
+        ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+        rc = _lib.lib.agb_batch_eval_ws(plan, x.data_ptr(), mode, *[ptr(o) for o in outs],
+                                        _lib.OUT_NEGATE, ws.data_ptr(), part,
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        _lib.check(rc, "agb_batch_eval_ws")
+        for g, w in zip(outs, want):
+            if w is not None:
+                assert torch.equal(g, w), (prec, mode, "in place")
+        small = ctypes.c_size_t(part // 2)
+        rc = _lib.lib.agb_batch_eval_ws(plan, x.data_ptr(), mode, *[ptr(o) for o in outs],
+                                        _lib.OUT_NEGATE, ws.data_ptr(), small,
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == -1 and "pre-sort" in _lib.last_error()
+
+
 def test_batch_many_small_units_and_two_calls():
     import torch
     import agama_gpu_b200 as agb
