@@ -20,6 +20,7 @@ OUT_BIN_ALWAYS = 4
 OUT_GRID_SHIFT = 8
 OUT_BLOCK_SHIFT = 12
 OUT_PPT_SHIFT = 16
+MP_NCONST = 8                # agb_component.p[3..9] + pad: invPhi0, inner s U W, outer s U W
 BIN_MIN_POINTS = 16384
 
 KIND_MULTIPOLE = 1
@@ -122,8 +123,8 @@ def _load():
     lib.agb_multipole_table_vjp.restype = ctypes.c_int
     lib.agb_multipole_table_vjp.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
-        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-        ctypes.c_void_p]
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_adjoint_workspace_bytes.restype = ctypes.c_size_t
     lib.agb_multipole_adjoint_workspace_bytes.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_int64, ctypes.c_int]
@@ -135,19 +136,19 @@ def _load():
     lib.agb_adjoint_step.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
-        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
-        ctypes.c_size_t, ctypes.c_void_p]
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_adjoint.restype = ctypes.c_int
     lib.agb_multipole_adjoint.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_adjoint_force.restype = ctypes.c_int
     lib.agb_multipole_adjoint_force.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_adjoint_kick.restype = ctypes.c_int
     lib.agb_adjoint_kick.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,

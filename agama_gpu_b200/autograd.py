@@ -49,7 +49,14 @@ class _PhiForce(torch.autograd.Function):
             for comp, sigma, gamma, ampl in pot._leaves(float(t)):
                 if id(comp) not in want:
                     continue
-                g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
+                kw = {}
+                if comp.kind == _lib.KIND_MULTIPOLE:     # and the builder's scalars
+                    key = ("const", comp)
+                    if key not in acc:
+                        acc[key] = torch.zeros(_lib.MP_NCONST, dtype=torch.float64,
+                                               device=arr.device)
+                    kw["const_grad"] = acc[key]
+                g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl), **kw)
                 acc[comp] = acc[comp] + g if comp in acc else g
             node_grads = pot._node_param_grads(acc, ctx.tracked)
         return (gx, None, None, None, None, *node_grads)

@@ -1171,8 +1171,8 @@ extern "C" size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* c
 
 extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
                                        const double* xyz, int64_t n, const double* g_phi,
-                                       const double* g_force, double* g_table, void* workspace,
-                                       size_t workspace_bytes, void* stream)
+                                       const double* g_force, double* g_table, double* g_const,
+                                       void* workspace, size_t workspace_bytes, void* stream)
 {
     if (!comp || !leaf || !g_table) return set_err(AGB_ERR_ARG, "agb_multipole_table_vjp: null argument");
     if (comp->kind != AGB_KIND_MULTIPOLE)
@@ -1189,6 +1189,7 @@ extern "C" int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf
     g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
     g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
     g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force; g.grad = g_table;
+    g.gconst = g_const;
     cudaStream_t st = (cudaStream_t)stream;
     agb_leaf l = *leaf;
     l.comp = 0;
@@ -1233,8 +1234,9 @@ struct AdjKeep {
 static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* leaf,
                                   const double* xyz, int64_t n, int precision,
                                   const double* g_phi, const double* g_force, double* g_xyz,
-                                  double* force, double* g_table, void* workspace,
-                                  size_t workspace_bytes, void* stream, AdjKeep* keep = nullptr)
+                                  double* force, double* g_table, double* g_const,
+                                  void* workspace, size_t workspace_bytes, void* stream,
+                                  AdjKeep* keep = nullptr)
 {
     const bool keep_on = keep && keep->on;
     if (!comp || !leaf || !g_table || (!g_xyz && !keep_on))
@@ -1255,7 +1257,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
     g.leaf.comp = 0; g.leaf.sigma = leaf->sigma; g.leaf.ampl = leaf->ampl;
     g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
     g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force;
-    g.gx = g_xyz; g.grad = g_table; g.force = force;
+    g.gx = g_xyz; g.grad = g_table; g.force = force; g.gconst = g_const;
     cudaStream_t st = (cudaStream_t)stream;
     agb_leaf l = *leaf;
     l.comp = 0;
@@ -1299,8 +1301,10 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
         if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                    current_device()) != cudaSuccess)
             optin = 48 * 1024;
-        g.staged = (size_t)8 * (tile + acc) <= (size_t)optin;
-        g.warp_smem = g.staged ? (int)(tile + acc) : tile;
+        // + 64 bytes per warp: its sums of the builder-scalar gradients (g_const)
+        const size_t cst = g_const ? 64 : 0;
+        g.staged = (size_t)8 * (tile + acc + cst) <= (size_t)optin;
+        g.warp_smem = (int)((g.staged ? tile + acc : tile) + cst);
         const size_t smem = (size_t)8 * g.warp_smem;
         const void* fn = precision == AGB_PREC_MIXED ? (const void*)mp_adjoint_kernel<float>
                                                      : (const void*)mp_adjoint_kernel<double>;
@@ -1442,9 +1446,10 @@ extern "C" size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, i
 
 extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                                 int n_leaves, int mp_leaf, int precision, double* x, double* vh,
-                                double* lx, double* lv, double* gF, double* g_table, int64_t n,
-                                double dt, double c, double k, double dt_drift, int flags,
-                                void* workspace, size_t workspace_bytes, void* stream)
+                                double* lx, double* lv, double* gF, double* g_table,
+                                double* g_const, int64_t n, double dt, double c, double k,
+                                double dt_drift, int flags, void* workspace,
+                                size_t workspace_bytes, void* stream)
 {
     int rc = adjoint_step_check(comps, n_comps, leaves, n_leaves, mp_leaf);
     if (rc) return rc;
@@ -1459,7 +1464,7 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
     keep.dest = nullptr;
     keep.stage = nullptr;
     rc = multipole_adjoint_impl(&comps[leaves[mp_leaf].comp], &leaves[mp_leaf], x, n, precision,
-                                nullptr, gF, nullptr, nullptr, g_table, workspace,
+                                nullptr, gF, nullptr, nullptr, g_table, g_const, workspace,
                                 workspace_bytes, stream, &keep);
     if (rc) return rc;
     static thread_local EvalArgs a;
@@ -1497,22 +1502,23 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
 extern "C" int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
                                      const double* xyz, int64_t n, int precision,
                                      const double* g_phi, const double* g_force, double* g_xyz,
-                                     double* g_table, void* workspace, size_t workspace_bytes,
-                                     void* stream)
+                                     double* g_table, double* g_const, void* workspace,
+                                     size_t workspace_bytes, void* stream)
 {
     return multipole_adjoint_impl(comp, leaf, xyz, n, precision, g_phi, g_force, g_xyz, nullptr,
-                                  g_table, workspace, workspace_bytes, stream);
+                                  g_table, g_const, workspace, workspace_bytes, stream);
 }
 
 extern "C" int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
                                            const double* xyz, int64_t n, int precision,
                                            const double* g_phi, const double* g_force,
                                            double* g_xyz, double* force, double* g_table,
-                                           void* workspace, size_t workspace_bytes, void* stream)
+                                           double* g_const, void* workspace,
+                                           size_t workspace_bytes, void* stream)
 {
     if (!force) return set_err(AGB_ERR_ARG, "agb_multipole_adjoint_force: force is null");
     return multipole_adjoint_impl(comp, leaf, xyz, n, precision, g_phi, g_force, g_xyz, force,
-                                  g_table, workspace, workspace_bytes, stream);
+                                  g_table, g_const, workspace, workspace_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------

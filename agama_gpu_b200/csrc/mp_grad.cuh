@@ -6,8 +6,7 @@
 // outputs, the loss depends on the leaf's Phi(x') and grad Phi(x') through
 //   alpha = gPhi A,   w = -A sigma gF,   beta_r,theta,phi = w . (u_r, u_theta, u_phi)
 // where grad Phi = Phi_r u_r + Phi_theta u_theta + Phi_os u_phi.  Inside the
-// radial grid (extrapolated points depend only on the extrapolation
-// constants, which are held fixed) and with the log-scaling factor F(log r):
+// radial grid and with the log-scaling factor F(log r):
 //   dL/da_{c,j} = s^j U_c + j s^(j-1) V_c                               (c >= 1)
 //   U_c = (alpha F + beta_r dF) W_c + beta_theta F dW_c + beta_phi F Q_c
 //   V_c = beta_r F inv_dlogr W_c
@@ -16,14 +15,107 @@
 // Each warp reduces its lanes' six values per harmonic with shuffles when all
 // of its points share one interval (the points are binned by interval), else
 // every lane adds its own; FP64 atomics accumulate into grad[k][c][j].
+//
+// The scalars the table builder derives from the nodes get their gradient too
+// (gconst, 8 doubles: invPhi0, inner s, U, W, outer eps, T, S (below), 0).  A point
+// inside the grid depends on invPhi0 through F = 1/(invPhi0 - e^c0):
+//   dL/dinvPhi0 = -F^2 QF - 2 F dF QdF,
+// QF and QdF the weights of F and dF in the point's loss (those of the monopole
+// column below).  A point beyond the grid has Phi = MP0 p0(log r) and
+// grad Phi = MP0 d1 x / r^2 with p0 = U e^(s dlr) + W (inside the first node) or
+// W e^(-dlr) + U e^(s dlr) (beyond the last) and d1 = dp0/dlog r, so
+//   dL/dc = MP0 (alpha dp0/dc + beta_r dd1/dc),  beta_r = w . x / r^2.
+// The outer fit is usually degenerate: its power s = -1 + eps with eps at the
+// rounding level and U ~ -W ~ 1e16 (the builder's two roots coincide), so its
+// gradient is taken in the well-conditioned variables eps = s + 1,
+// T = U eps, S = U + W:  p0 = e^(-dlr) (S + T phi),  phi = expm1(eps dlr) / eps,
+// d1 = e^(-dlr) (T e^(eps dlr) - S - T phi).
 #pragma once
 #include "multipole.cuh"
+
+#ifndef AGB_MP_NCONST
+#define AGB_MP_NCONST 8
+#endif
+
+// one point's contributions to the gradient of the builder's scalars (zeros for a
+// point inside the grid except v[0], which the caller sets)
+__device__ __forceinline__ void mp_const_extrap(const DevComp& c, double r, double alpha,
+                                                double br, double v[AGB_MP_NCONST])
+{
+    const double MP0 = AGB_MUL0 * AGB_PREFACT[0];
+    const double logr_min = c.p[0], dlogr = c.p[1];
+    if (!(r >= 1.0e-300)) {                 // the origin: Phi = MP0 W_in, no force
+        v[3] += MP0 * alpha;
+        return;
+    }
+    const double logr = log(r);
+    if (logr < logr_min) {
+        const double s = c.p[4], U = c.p[5];
+        const double dlr = logr - logr_min;
+        const double rs = (s != 0.0) ? exp(s * dlr) : 1.0;
+        // p0 = U rs + W, d1 = U s rs
+        v[1] += MP0 * (alpha * U * dlr * rs + br * U * rs * (1.0 + s * dlr));
+        v[2] += MP0 * (alpha * rs + br * s * rs);
+        v[3] += MP0 * alpha;
+        return;
+    }
+    const int k = (int)((logr - logr_min) * c.p[2]);
+    if (k < c.n_int) return;
+    const double eps = c.p[7] + 1.0, T = c.p[8] * eps, S = c.p[8] + c.p[9];
+    const double dlr = logr - (logr_min + c.n_int * dlogr);
+    const double en = exp(-dlr), x = eps * dlr, ex = exp(x);
+    double ph, dph;                         // phi and dphi/deps (series near eps = 0)
+    if (fabs(x) < 1.0e-4) {
+        ph = dlr * (1.0 + x * (0.5 + x * (1.0 / 6.0)));
+        dph = dlr * dlr * (0.5 + x * (1.0 / 3.0 + x * 0.125));
+    } else {
+        ph = expm1(x) / eps;
+        dph = (dlr * ex * eps - expm1(x)) / (eps * eps);
+    }
+    v[4] += MP0 * en * T * (alpha * dph + br * (dlr * ex - dph));     // d/deps
+    v[5] += MP0 * en * (alpha * ph + br * (ex - ph));                 // d/dT
+    v[6] += MP0 * en * (alpha - br);                                  // d/dS
+}
 
 __device__ __forceinline__ double warp_sum(double v)
 {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Warp reduce-scatter of eight values: lane L returns the warp sum of value
+// 4*b4 + 2*b3 + b2 (b = bits of L); 9 shuffles instead of 40 for eight
+// independent butterflies.
+template <typename T>
+__device__ __forceinline__ T warp_rs8(const T v[8], int lane)
+{
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    T w[4], u[2];
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const T keep = h16 ? v[q + 4] : v[q];
+        const T send = h16 ? v[q] : v[q + 4];
+        w[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    #pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const T keep = h8 ? w[q + 2] : w[q];
+        const T send = h8 ? w[q] : w[q + 2];
+        u[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    T z = (h4 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, h4 ? u[0] : u[1], 4);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    return z;
+}
+
+// add the warp's eight constant gradients (lane values v) into g: one atomic each
+__device__ __forceinline__ void mp_const_flush(double* g, const double v[AGB_MP_NCONST], int lane)
+{
+    const double z = warp_rs8<double>(v, lane);
+    const int idx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+    if ((lane & 3) == 0 && z != 0.0) atomicAdd(g + idx, z);
 }
 
 // add six per-lane values into gk[col][0..5]; gk is the interval's row of the
@@ -52,6 +144,7 @@ struct MPGradArgs {
     const double* gphi;       // [N] or null
     const double* gforce;     // [N,3] or null
     double* grad;             // [n_int][n_lm][6], accumulated
+    double* gconst;           // [AGB_MP_NCONST] or null, accumulated
     DevComp c;
     DevLeaf leaf;
 };
@@ -159,6 +252,18 @@ mp_grad_kernel(const __grid_constant__ MPGradArgs a)
             const int kk = uniform ? kmax : k;
             grad_add6((kk >= 0) ? a.grad + (long long)kk * c.n_lm * 6 : nullptr, 0, v, uniform,
                       lane, active);
+            if (a.gconst) {             // the builder's scalars (warp-uniform branch)
+                double cv[AGB_MP_NCONST] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (active && c.log_scaling) {
+                    const double QF = alpha * (MP0 + t.A) + br * Bp + bt * t.Th + bp * t.Pos;
+                    const double QdF = br * (MP0 + t.A);
+                    cv[0] = -F * F * QF - 2.0 * F * dF * QdF;
+                } else if (!active && pos < a.n) {
+                    const double brx = -As * (gf0 * px + gf1 * py + gf2 * pz) / r2;
+                    mp_const_extrap(c, r, gp * a.leaf.ampl, r2 > 0.0 ? brx : 0.0, cv);
+                }
+                mp_const_flush(a.gconst, cv, lane);
+            }
         }
 
         // harmonic columns: the same regular / list walk as the forward
@@ -262,32 +367,6 @@ mp_grad_kernel(const __grid_constant__ MPGradArgs a)
 // one walk over the harmonics (regular column structures).
 // ---------------------------------------------------------------------------
 
-// Warp reduce-scatter of eight values: lane L returns the warp sum of value
-// 4*b4 + 2*b3 + b2 (b = bits of L); 9 shuffles instead of 40 for eight
-// independent butterflies.
-template <typename T>
-__device__ __forceinline__ T warp_rs8(const T v[8], int lane)
-{
-    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
-    T w[4], u[2];
-    #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const T keep = h16 ? v[q + 4] : v[q];
-        const T send = h16 ? v[q] : v[q + 4];
-        w[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const T keep = h8 ? w[q + 2] : w[q];
-        const T send = h8 ? w[q] : w[q + 2];
-        u[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    T z = (h4 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, h4 ? u[0] : u[1], 4);
-    z += __shfl_xor_sync(0xffffffffu, z, 2);
-    z += __shfl_xor_sync(0xffffffffu, z, 1);
-    return z;
-}
-
 // add six per-lane gradient values of one column into gk[col][0..5]; when the
 // warp is uniform and sk (the warp's shared-memory accumulator for this
 // interval) is given, the reduced values go there instead of to global memory
@@ -326,6 +405,7 @@ struct MPAdjArgs {
     double* stage;            // binned calls: per sorted position the 3 (6 with force)
                               // values to add, gathered back by adj_unpermute_add
     int stage_rec;            // 3, or 6 with the force
+    double* gconst;           // [AGB_MP_NCONST] or null, accumulated
     DevComp c;
     DevLeaf leaf;
 };
@@ -594,6 +674,10 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
     const long long hi = lo + a.chunk < a.n ? lo + a.chunk : a.n;
     if (swarp)
         for (int q = lane; q < nval; q += 32) swarp[q] = 0.0;
+    // this warp's sums of the builder-scalar gradients (the last 64 bytes of its slice)
+    double* wc = a.gconst ? reinterpret_cast<double*>(wbase + a.warp_smem - 64) : nullptr;
+    if (wc && lane < AGB_MP_NCONST) wc[lane] = 0.0;
+    __syncwarp();
     int cur_k = -1;                      // interval held in swarp
     auto flush = [&]() {
         __syncwarp();
@@ -730,6 +814,24 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
                 for (int j = 0; j < 6; ++j) v[j] = alpha * MP0 * sp[j] + br * MP0 * inv_dlogr * dw[j];
             }
             grad_emit6<double>(gbase, sk, 0, v, uniform, lane, inside);
+            if (wc) {                   // the builder's scalars (warp-uniform branch)
+                double gi = 0.0;
+                if (inside && c.log_scaling) {
+                    const double QF = alpha * (MP0 + t.A) + br * Bp + bt * t.Th + bp * t.Pos;
+                    const double QdF = br * (MP0 + t.A);
+                    gi = -F * F * QF - 2.0 * F * dF * QdF;
+                }
+                gi = warp_sum(gi);
+                if (lane == 0) wc[0] += gi;
+                if (valid && !inside) {     // beyond the grid: few points, shared atomics
+                    double cv[AGB_MP_NCONST] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    const double brx = (w0 * px + w1 * py + w2 * pz) / r2;
+                    mp_const_extrap(c, r, gp * A, r2 > 0.0 ? brx : 0.0, cv);
+                    #pragma unroll
+                    for (int q = 1; q < 7; ++q)
+                        if (cv[q] != 0.0) atomicAdd(wc + q, cv[q]);
+                }
+            }
         }
         if (!valid) continue;
         // position VJP of this leaf: A sigma (gPhi grad - sigma H gF)
@@ -765,6 +867,10 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
         }
     }
     if (swarp) flush();
+    if (wc) {
+        __syncwarp();
+        if (lane < AGB_MP_NCONST && wc[lane] != 0.0) atomicAdd(a.gconst + lane, wc[lane]);
+    }
 }
 
 // the staged records of a binned adjoint added back in input order: point i's

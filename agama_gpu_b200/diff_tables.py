@@ -6,9 +6,14 @@ the six Horner coefficients per interval -- written with torch operations so
 that a gradient with respect to the coefficients (from the table-VJP kernel)
 can be carried back to the node tables Phi_lm(r_i) and dPhi_lm/dr(r_i).
 
-Held fixed (treated as constants of the tables): the radial grid, invPhi0,
-the inner/outer extrapolation constants, the harmonic set after pruning.
-A grid that had to be resampled to log-uniform is not supported here.
+The scalars the builder derives from the l=0 nodes -- invPhi0 and the inner
+and outer power-law extrapolation constants (s, U, W) -- are restated too
+(``multipole_consts_from_nodes``), so that with their explicit gradients (the
+kernels' g_const) a node gradient is the derivative of the whole builder;
+branch choices (which power law, the constant-density core, invPhi0 = 0) are
+taken at the current values.  Held fixed: the radial grid, the harmonic set
+after pruning, the log-scaling switch.  A grid that had to be resampled to
+log-uniform is not supported here.
 """
 from __future__ import annotations
 
@@ -54,9 +59,148 @@ def quintic_poly_torch(logr: torch.Tensor, f: torch.Tensor, df: torch.Tensor, h:
     return a.permute(1, 0, 2)
 
 
-def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) -> torch.Tensor:
+_EPS = float(np.finfo(np.float64).eps)
+
+
+def _f(q) -> float:
+    """Value of a (0-d) tensor or number, for the builder's branch decisions."""
+    return float(q.detach()) if torch.is_tensor(q) else float(q)
+
+
+class _LambertW(torch.autograd.Function):
+    """Real branch k (0 or -1) of the Lambert W function of a 0-d tensor;
+    dW/dx = W / (x (1 + W))."""
+
+    @staticmethod
+    def forward(ctx, x, k):
+        from scipy.special import lambertw
+        w = torch.tensor(float(np.real(lambertw(float(x), k=k))), dtype=x.dtype, device=x.device)
+        ctx.save_for_backward(x, w)
+        return w
+
+    @staticmethod
+    def backward(ctx, g):
+        x, w = ctx.saved_tensors
+        return g * w / (x * (1.0 + w)), None
+
+
+def inner_extrapolation_torch(phi0: torch.Tensor, dphi0_dr: torch.Tensor, r: np.ndarray):
+    """(invPhi0, s, U, W) as prep_multipole.inner_extrapolation computes them, as
+    differentiable functions of the l=0 node values phi0 (nR,) and dPhi0/dr (nR,)."""
+    zero = phi0.new_zeros(())
+    P1, P2, d1, d2 = phi0[0], phi0[1], dphi0_dr[0], dphi0_dr[1]
+    r1, r2 = float(r[0]), float(r[1])
+    lnr = float(np.log(r2 / r1))
+    g1 = r1 * d1
+    tiny = 100.0 * _EPS
+    if abs(_f(g1)) == 0.0 or abs(_f(P1 - P2)) < tiny * max(abs(_f(P1)), abs(_f(P2))):
+        return zero, zero, zero, P1
+    A = lnr * g1 / (P1 - P2)
+    a = _f(A)
+    if not np.isfinite(a) or a >= 0.0:
+        return zero, zero, zero, P1
+    if abs(a + 1.0) < np.sqrt(_EPS):
+        s = zero
+    else:
+        s = (A - _LambertW.apply(A * torch.exp(A), 0 if a > -1.0 else -1)) / lnr
+    if not np.isfinite(_f(s)):
+        s = zero + 2.0
+    if _f(s) != 0.0:
+        U = (r1 * d1) / s
+        W = (r1 * d1 - s * P1) / (-s)
+        pred_pow = U * s * torch.exp(s * lnr) / r2
+    else:
+        U = r1 * d1
+        W = P1
+        pred_pow = r1 * d1 / r2
+    pred_cub = (r2 / r1 * (6.0 * r1 * (P2 - P1) / (r2 - r1) - d1 * (2 * r1 + r2))) / (2 * r2 + r1)
+    if abs(_f(d2 - pred_cub)) < abs(_f(d2 - pred_pow)):
+        s = zero + 2.0
+        U = 0.5 * r1 * d1
+        W = P1 - U
+    if _f(s) <= 0.0:
+        return zero, s, U, W
+    inv = 1.0 / W
+    if bool((phi0.detach() * _f(inv) >= 1.0).any()):
+        inv = zero
+    return inv, s, U, W
+
+
+def outer_extrapolation_torch(phi0: torch.Tensor, dphi0_dr: torch.Tensor, r: np.ndarray):
+    """(s, U, W) as prep_multipole.outer_extrapolation computes them, differentiable
+    in the l=0 node values."""
+    zero = phi0.new_zeros(())
+    v = -1.0
+    P1, P2, d1 = phi0[-1], phi0[-2], dphi0_dr[-1]
+    r1, r2 = float(r[-1]), float(r[-2])
+    lnr = float(np.log(r2 / r1))
+    num1, num2 = r1 * d1, v * P1
+    den1, den2 = P1, P2 * float(np.exp(-v * lnr))
+    tiny = 100.0 * _EPS
+    f = _f
+    roundoff = (abs(f(num1 - num2)) < max(abs(f(num1)), abs(f(num2))) * tiny or
+                abs(f(den1 - den2)) < max(abs(f(den1)), abs(f(den2))) * tiny)
+    if not np.isfinite(f(P1)) or roundoff or f(den1) == f(den2):
+        return zero, zero, P1
+    A = lnr * (num1 - num2) / (den1 - den2)
+    a = f(A)
+    if not np.isfinite(a) or a >= 0:
+        return zero, zero, P1
+    if abs(a + 1) < np.sqrt(_EPS):
+        s = zero + v
+    else:
+        s = v + (A - _LambertW.apply(A * torch.exp(A), 0 if a > -1 else -1)) / lnr
+    if not np.isfinite(f(s)) or f(s) >= 0:
+        s = zero - 2.0
+    if f(s) != v:
+        U = (r1 * d1 - v * P1) / (s - v)
+        W = (r1 * d1 - s * P1) / (v - s)
+    else:
+        U = r1 * d1 - v * P1
+        W = P1
+    return s, U, W
+
+
+def outer_fit_variables(phi0: torch.Tensor, dphi0_dr: torch.Tensor, r: np.ndarray):
+    """(eps, T, S) = (s + 1, U (s + 1), U + W) of the outer fit, the variables of the
+    kernels' g_const[4..6].  The fit is usually degenerate (s = -1 up to rounding,
+    U ~ -W ~ 1e16); in these variables it is well-conditioned: where the builder
+    divides by s + 1, T = r1 dPhi/dr(r1) + Phi(r1) and S = Phi(r1) exactly."""
+    s, U, W = outer_extrapolation_torch(phi0, dphi0_dr, r)
+    eps = s + 1.0
+    if _f(eps) != 0.0 and _f(W) != _f(phi0[-1]):
+        r1 = float(r[-1])
+        P1 = phi0[-1]
+        T = r1 * dphi0_dr[-1] + P1            # = (r1 d1 - v P1), v = -1
+        S = P1                                # U + W = P1 when U = T / eps
+        return eps, T, S
+    return eps, U * eps, U + W
+
+
+def multipole_consts_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) -> torch.Tensor:
+    """(8,) [invPhi0, inner s, U, W, outer eps, T, S, 0] -- the order of the kernels'
+    g_const -- from node tables (nR, n_lm) in the builder's harmonic order,
+    differentiable (computed on the host: a few scalars)."""
+    if int(np.asarray(tables.node_cols)[0]) != 0:
+        raise ValueError("the builder's l=0 column must be the coefficient file's first column")
+    r = np.asarray(tables.r_grid, dtype=np.float64)
+    p0 = phi[:, 0].to("cpu", torch.float64)
+    d0 = dphi_dr[:, 0].to("cpu", torch.float64)
+    zero = p0.new_zeros(())
+    out_e, out_T, out_S = outer_fit_variables(p0, d0, r)
+    if tables.log_scaling:
+        inv, in_s, in_U, in_W = inner_extrapolation_torch(p0, d0, r)
+    else:
+        inv, in_s, in_U, in_W = zero, zero, zero, p0[0]
+    parts = [inv, in_s, in_U, in_W, out_e, out_T, out_S, zero]
+    return torch.stack([q if torch.is_tensor(q) else zero + q for q in parts]).to(phi.device)
+
+
+def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor,
+                              inv=None) -> torch.Tensor:
     """Quintic coefficients (n_lm, n_int, 6) from node tables (nR, n_lm) in the
-    builder's harmonic order (``tables.node_phi`` layout); differentiable."""
+    builder's harmonic order (``tables.node_phi`` layout); differentiable.  inv: the
+    log-scaling constant invPhi0 (a float or a 0-d tensor; default: the builder's)."""
     if tables.resampled:
         raise ValueError("node gradients need a log-uniform input grid (this one was resampled)")
     dev = phi.device
@@ -65,7 +209,8 @@ def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) 
     dphi_dlogr = dphi_dr * r[:, None]
     if tables.log_scaling:
         p0 = phi[:, 0]
-        inv = float(tables.invPhi0)
+        if inv is None:
+            inv = float(tables.invPhi0)
         f0 = torch.log(inv - 1.0 / p0)
         df0 = dphi_dlogr[:, 0] / (p0 * (inv * p0 - 1.0))
         ratio = phi[:, 1:] / p0[:, None]
@@ -78,7 +223,8 @@ def multipole_poly_from_nodes(tables, phi: torch.Tensor, dphi_dr: torch.Tensor) 
 
 
 def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: Optional[int],
-             nodes=None) -> Tuple[torch.Tensor, torch.Tensor]:
+             nodes=None, grad_const: Optional[torch.Tensor] = None
+             ) -> Tuple[torch.Tensor, torch.Tensor]:
     """Carry dL/dpoly back to the node tables in the coefficient file's column order.
 
     Returns (dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_cols); columns
@@ -87,7 +233,10 @@ def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: Optional[int],
     builder's harmonic order instead, (nR, n_lm) like ``tables.node_phi``.
     ``nodes`` = (phi, dphi_dr) in the builder's order when the tables were
     replaced on the device (set_node_tables), else the builder's own node values
-    are used.
+    are used.  grad_const (8,): the explicit gradient with respect to invPhi0 and
+    the extrapolation constants (the kernels' g_const); with it the builder's
+    scalars are functions of the nodes (the derivative of the whole builder, as
+    set_node_tables rebuilds them), without it they are held fixed.
     """
     dev = grad_poly.device
     if nodes is None:
@@ -98,9 +247,20 @@ def node_vjp(tables, grad_poly: torch.Tensor, n_file_cols: Optional[int],
         dphi = nodes[1].detach().to(dev, torch.float64).requires_grad_(True)
     # also called from the backward of an autograd.Function, where grad mode is off
     with torch.enable_grad():
-        poly = multipole_poly_from_nodes(tables, phi, dphi)
-        gphi, gdphi = torch.autograd.grad(poly, (phi, dphi),
-                                          grad_outputs=grad_poly.to(torch.float64))
+        if grad_const is None:
+            poly = multipole_poly_from_nodes(tables, phi, dphi)
+            gphi, gdphi = torch.autograd.grad(poly, (phi, dphi),
+                                              grad_outputs=grad_poly.to(torch.float64))
+        else:
+            k = multipole_consts_from_nodes(tables, phi, dphi)
+            poly = multipole_poly_from_nodes(tables, phi, dphi, inv=k[0])
+            gphi, gdphi = torch.autograd.grad(
+                (poly, k), (phi, dphi),
+                grad_outputs=(grad_poly.to(torch.float64),
+                              grad_const.to(device=dev, dtype=torch.float64)),
+                allow_unused=True)
+            gphi = torch.zeros_like(phi) if gphi is None else gphi
+            gdphi = torch.zeros_like(dphi) if gdphi is None else gdphi
     if n_file_cols is None:
         return gphi, gdphi
     cols = torch.as_tensor(np.asarray(tables.node_cols), dtype=torch.long, device=dev)

@@ -37,6 +37,15 @@ from . import _lib
 GYR_PER_TIME_UNIT = 0.977792221          # 1 kpc / (km/s) in Gyr
 
 
+def _consts_epoch(pot) -> int:
+    """The components' builder-scalar generation (captured graphs bake the descriptors)."""
+    from .potentials import consts_epoch
+    try:
+        return consts_epoch(pot._all_components())
+    except (AttributeError, TypeError):
+        return 0
+
+
 def gyr_to_time(dt_gyr: float) -> float:
     return float(dt_gyr) / GYR_PER_TIME_UNIT
 
@@ -86,7 +95,9 @@ def allreduce_table_grads(tg: dict, group=None) -> dict:
     import torch.distributed as dist
     if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) < 2:
         return tg
-    for key in sorted(tg, key=lambda c: c._sync_order):
+    def order(key):             # a component, or ("const", component) after it
+        return (key[1]._sync_order, 1) if isinstance(key, tuple) else (key._sync_order, 0)
+    for key in sorted(tg, key=order):
         dist.all_reduce(tg[key], op=dist.ReduceOp.SUM, group=group)
     return tg
 
@@ -249,7 +260,7 @@ class Leapfrog:
                 self._step(x, v, F, n0 + k)
             return
         key = (x.data_ptr(), v.data_ptr(), F.data_ptr(), x.shape[0],
-               getattr(self.pot, "plan_generation", 0))
+               getattr(self.pot, "plan_generation", 0), _consts_epoch(self.pot))
         if self._graph is None or self._graph_key != key:
             self._capture(x, v, F, n0)
             self._graph_key = key

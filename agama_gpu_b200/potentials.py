@@ -115,10 +115,11 @@ class _TimePlan:
         self._arrays = {}
 
     def component_array(self, dev):
-        a = self._arrays.get(dev)
+        key = (dev, consts_epoch(self.comps))
+        a = self._arrays.get(key)
         if a is None:
             a = (_lib.AgbComponent * len(self.comps))(*[c._device_component(dev) for c in self.comps])
-            self._arrays[dev] = a
+            self._arrays = {key: a}
         return a
 
     def __del__(self):
@@ -129,6 +130,22 @@ class _TimePlan:
             except Exception:       # interpreter shutdown
                 pass
             self.handle = None
+
+
+def consts_epoch(comps) -> int:
+    """Changes whenever set_node_tables() changed the builder scalars of one of the
+    components (their descriptors, which launches pass by value, changed with them)."""
+    return sum(c.__dict__.get("_consts_gen", 0) for c in comps)
+
+
+def _const_buffer(acc: dict, comp, dev) -> torch.Tensor:
+    """The (8,) accumulator of dL/d(builder scalars) of Multipole comp in acc."""
+    key = ("const", comp)
+    buf = acc.get(key)
+    if buf is None:
+        buf = torch.zeros(_lib.MP_NCONST, dtype=torch.float64, device=dev)
+        acc[key] = buf
+    return buf
 
 
 class _GPUPotBase:
@@ -371,6 +388,8 @@ class _GPUPotBase:
             g = table_grads.get(comp)
             if g is None:
                 out.extend(torch.zeros_like(q) for q in params)
+            elif comp.kind == _lib.KIND_MULTIPOLE:
+                out.extend(comp._grads_of_nodes(g, table_grads.get(("const", comp))))
             else:
                 out.extend(comp._grads_of_nodes(g))
         return out
@@ -499,7 +518,10 @@ class _GPUPotBase:
                       force_out=force_out)
             for comp, sigma, gamma, ampl in rest:
                 if comp.kind in (_lib.KIND_MULTIPOLE, _lib.KIND_CYLSPLINE):
-                    g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
+                    kw = {}
+                    if comp.kind == _lib.KIND_MULTIPOLE:
+                        kw["const_grad"] = _const_buffer(acc_dev, comp, dev)
+                    g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl), **kw)
                     key = ("poly", comp)
                     if key in acc_dev:
                         acc_dev[key].add_(g)
@@ -528,17 +550,19 @@ class _GPUPotBase:
             nws = int(_lib.lib.agb_multipole_adjoint_workspace_bytes(
                 ctypes.byref(c), ctypes.byref(lf), n, 0 if force_out is None else 1))
             ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
+            cg = _const_buffer(acc_dev, comp, dev)
             if force_out is None:
                 rc = _lib.lib.agb_multipole_adjoint(ctypes.byref(c), ctypes.byref(lf),
                                                     arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
-                                                    gx.data_ptr(), buf.data_ptr(), ptr(ws), nws,
-                                                    stream)
+                                                    gx.data_ptr(), buf.data_ptr(), cg.data_ptr(),
+                                                    ptr(ws), nws, stream)
                 _lib.check(rc, "agb_multipole_adjoint")
             else:
                 rc = _lib.lib.agb_multipole_adjoint_force(ctypes.byref(c), ctypes.byref(lf),
                                                           arr.data_ptr(), n, prec, ptr(gp), ptr(gf),
                                                           gx.data_ptr(), force_out.data_ptr(),
-                                                          buf.data_ptr(), ptr(ws), nws, stream)
+                                                          buf.data_ptr(), cg.data_ptr(), ptr(ws),
+                                                          nws, stream)
                 _lib.check(rc, "agb_multipole_adjoint_force")
         return gx
 
@@ -573,19 +597,24 @@ class _GPUPotBase:
                               device=dev)
             acc_dev[comp] = buf
         ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        cg = _const_buffer(acc_dev, comp, dev)
         rc = _lib.lib.agb_adjoint_step(
             *cargs, mp[0], prec, arr.data_ptr(), None if vh is None else vh.data_ptr(),
-            lx.data_ptr(), lv.data_ptr(), gF.data_ptr(), buf.data_ptr(), n, float(dt), float(c),
-            float(k), float(dt_drift), flags, ws.data_ptr(), nws,
+            lx.data_ptr(), lv.data_ptr(), gF.data_ptr(), buf.data_ptr(), cg.data_ptr(), n,
+            float(dt), float(c), float(k), float(dt_drift), flags, ws.data_ptr(), nws,
             ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
         _lib.check(rc, "agb_adjoint_step")
         return True
 
     @staticmethod
     def _table_grads_from_device(acc_dev: dict) -> dict:
-        """{component: dL/dpoly in the layout of component.tables.poly}."""
+        """{component: dL/dpoly in the layout of component.tables.poly} and, for each
+        Multipole, {("const", component): dL/d(builder scalars) (8,)}."""
         out = {}
         for key, g in acc_dev.items():
+            if isinstance(key, tuple) and key[0] == "const":
+                out[key] = g
+                continue
             if isinstance(key, tuple):              # already in poly layout
                 comp = key[1]
                 out[comp] = out[comp] + g if comp in out else g
@@ -602,13 +631,17 @@ class _GPUPotBase:
     def _table_vjp(self, arr: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
                    g_force: Optional[torch.Tensor], acc: Optional[dict] = None) -> dict:
         """Table gradients of every Multipole and CylSpline in the tree: {component:
-        dL/dpoly (n_lm, n_int, 6) | dL/d(node table) (n_harm, nR, nz, 4)}, summed over
+        dL/dpoly (n_lm, n_int, 6) | dL/d(node table) (n_harm, nR, nz, 4)} and, per
+        Multipole, {("const", component): dL/d(builder scalars) (8,)}, summed over
         the leaves that use it and added into ``acc`` when given."""
         acc = {} if acc is None else acc
         for comp, sigma, gamma, ampl in self._leaves(float(t)):
             if comp.kind not in (_lib.KIND_MULTIPOLE, _lib.KIND_CYLSPLINE):
                 continue
-            g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl))
+            kw = {}
+            if comp.kind == _lib.KIND_MULTIPOLE:
+                kw["const_grad"] = _const_buffer(acc, comp, arr.device)
+            g = comp.table_vjp(arr, t, g_phi, g_force, leaf=(sigma, gamma, ampl), **kw)
             if comp in acc:
                 acc[comp].add_(g)
             else:
@@ -1011,14 +1044,18 @@ class MultipolePotentialGPU(_Component):
                 pass
 
     def table_vjp(self, xyz: torch.Tensor, t: float, g_phi: Optional[torch.Tensor],
-                  g_force: Optional[torch.Tensor], leaf=None) -> torch.Tensor:
+                  g_force: Optional[torch.Tensor], leaf=None,
+                  const_grad: Optional[torch.Tensor] = None) -> torch.Tensor:
         """dL/dpoly (n_lm, n_int, 6) of this Multipole, in the layout of ``tables.poly``.
 
         g_phi (N,) and g_force (N,3) are cotangents of the potential and force of
         the tree this component belongs to; ``leaf`` = (sigma, gamma, ampl) of the
         component in that tree (default: the component on its own).  FP64.
-        Points outside the radial grid contribute nothing: the extrapolation
-        constants (and invPhi0) are held fixed.
+        const_grad: an (8,) FP64 device tensor that receives (adds) the gradient
+        with respect to the builder's scalars -- invPhi0 from the points inside
+        the grid, the inner and outer l=0 extrapolation from the points beyond it
+        (see diff_tables.multipole_consts_from_nodes); pass it on to
+        node_gradients() for the derivative of the whole builder.
         """
         dev = xyz.device
         comp = self._device_component(dev)
@@ -1038,23 +1075,30 @@ class MultipolePotentialGPU(_Component):
                                                                        ctypes.byref(lf), n))
             ws = torch.empty(nws, dtype=torch.uint8, device=dev) if nws else None
             ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
+            if const_grad is not None and (const_grad.dtype != torch.float64 or
+                                           const_grad.numel() != _lib.MP_NCONST or
+                                           const_grad.device != dev):
+                raise ValueError("const_grad must be an (8,) float64 tensor on the points' device")
             rc = _lib.lib.agb_multipole_table_vjp(
                 ctypes.byref(comp), ctypes.byref(lf), arr.data_ptr(), n, ptr(gp), ptr(gf),
-                g.data_ptr(), ptr(ws), nws,
+                g.data_ptr(), ptr(const_grad), ptr(ws), nws,
                 ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
             _lib.check(rc, "agb_multipole_table_vjp")
         cols = torch.from_numpy(self._col_of).to(dev)
         return g.index_select(1, cols).permute(1, 0, 2).contiguous()
 
-    def node_gradients(self, grad_poly: torch.Tensor):
+    def node_gradients(self, grad_poly: torch.Tensor, grad_const: Optional[torch.Tensor] = None):
         """(dL/dPhi_nodes, dL/d(dPhi/dr)_nodes), each (nR, n_file_columns), from dL/dpoly.
 
         Chains through a differentiable restatement of the table construction
-        (diff_tables); invPhi0 and the extrapolation constants are held fixed.
+        (diff_tables).  With grad_const (table_vjp's const_grad, or the adjoint's
+        table gradients) also through invPhi0 and the l=0 extrapolation constants,
+        as functions of the nodes: the derivative of the whole builder, which is
+        what set_node_tables() rebuilds; without it they are held fixed.
         """
         from .diff_tables import node_vjp
         n_file = int(max(self.tables.node_cols)) + 1 if self._n_file_cols is None else self._n_file_cols
-        return node_vjp(self.tables, grad_poly, n_file, nodes=self._nodes)
+        return node_vjp(self.tables, grad_poly, n_file, nodes=self._nodes, grad_const=grad_const)
 
     _n_file_cols = None
 
@@ -1079,21 +1123,24 @@ class MultipolePotentialGPU(_Component):
     def _apply_nodes(self, p) -> None:
         self._set_nodes(p[0], p[1])
 
-    def _grads_of_nodes(self, grad_poly: torch.Tensor) -> List[torch.Tensor]:
+    def _grads_of_nodes(self, grad_poly: torch.Tensor,
+                        grad_const: Optional[torch.Tensor] = None) -> List[torch.Tensor]:
         """[dL/dPhi nodes, dL/d(dPhi/dr) nodes] in the layout of node_parameters()."""
         from .diff_tables import node_vjp
-        g0, g1 = node_vjp(self.tables, grad_poly, None, nodes=self._nodes)
+        g0, g1 = node_vjp(self.tables, grad_poly, None, nodes=self._nodes, grad_const=grad_const)
         dev = self._node_params[0].device
         return [g0.to(dev), g1.to(dev)]
 
-    def _device_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor):
+    def _device_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor, inv=None):
         """(FP64 interval-major, FP32) device tables of this object's layout from node
         tables (nR, n_lm) in the builder's harmonic order, computed with torch on
-        their device (differentiable restatement of the builder: diff_tables)."""
+        their device (differentiable restatement of the builder: diff_tables); inv:
+        invPhi0 (default: the builder's)."""
         from .diff_tables import multipole_poly_from_nodes
         t = self.tables
         dev = phi.device
-        pb = multipole_poly_from_nodes(t, phi.to(torch.float64), dphi_dr.to(torch.float64))
+        pb = multipole_poly_from_nodes(t, phi.to(torch.float64), dphi_dr.to(torch.float64),
+                                       inv=inv)
         full = torch.zeros((self._n_cols, t.n_int, 6), dtype=torch.float64, device=dev)
         full[torch.from_numpy(self._col_of).to(dev)] = pb
         full = full * torch.from_numpy(self._col_scale).to(dev)[:, None, None]
@@ -1104,30 +1151,66 @@ class MultipolePotentialGPU(_Component):
                                                                            device=dev))
         return im, p32.to(torch.float32).reshape(t.n_int, self._n_cols, 8).contiguous()
 
-    def set_node_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor) -> None:
+    def set_node_tables(self, phi: torch.Tensor, dphi_dr: torch.Tensor,
+                        rebuild_constants: bool = True) -> None:
         """Replace the expansion's node values Phi_lm(r_i) and dPhi_lm/dr(r_i) -- (nR,
         n_lm) tensors in the builder's harmonic order (the layout of tables.node_phi) --
-        rebuilding the quintic tables on the GPU, in place: nothing goes through the
-        host, and CUDA graphs captured over this potential (leapfrog) stay valid and
-        see the new tables.  The radial grid, the harmonic set, invPhi0 and the l=0
-        extrapolation constants are kept from construction (the same constants that
-        node_gradients() holds fixed).  Not differentiable itself: use
-        node_gradients() on the adjoint's table gradient."""
-        self._set_nodes(phi, dphi_dr)
+        rebuilding the quintic tables on the GPU, in place (a CUDA graph captured over
+        this potential sees the new tables).  The scalars the builder derives from the
+        l=0 nodes -- invPhi0 and the inner and outer power-law constants -- are
+        recomputed as the builder does (one small device-to-host copy of the l=0
+        column); graphs captured before a change of them are captured again by the
+        integrators.  rebuild_constants=False keeps those of construction (and of
+        node_gradients() without grad_const).  The radial grid, the harmonic set and
+        the log-scaling switch stay those of construction.  Not differentiable
+        itself: use node_gradients() on the adjoint's table gradient."""
+        self._set_nodes(phi, dphi_dr, rebuild_constants)
         self._refresh_tracked([phi.detach(), dphi_dr.detach()])
 
-    def _set_nodes(self, phi: torch.Tensor, dphi_dr: torch.Tensor) -> None:
+    def _builder_scalars(self, phi: torch.Tensor, dphi_dr: torch.Tensor) -> List[float]:
+        """[invPhi0, inner s, U, W, outer s, U, W] of the builder for these nodes."""
+        from .prep_multipole import inner_extrapolation, outer_extrapolation
+        t = self.tables
+        p0 = phi[:, 0].detach().to("cpu", torch.float64).numpy()
+        d0 = dphi_dr[:, 0].detach().to("cpu", torch.float64).numpy()
+        if np.array_equal(p0, t.node_phi[:, 0]) and np.array_equal(d0, t.node_dphi_dr[:, 0]):
+            # the construction's l=0 nodes: its scalars (the builder took dPhi/dr from
+            # the file, which the node table holds rounded through d/dlog r)
+            return [t.invPhi0, t.inner_s, t.inner_U, t.inner_W, t.outer_s, t.outer_U,
+                    t.outer_W]
+        r = np.asarray(t.r_grid, dtype=np.float64)
+        if bool(t.log_scaling) != bool(np.all(p0 < 0.0)):
+            raise ValueError("the new l=0 nodes change the sign condition of the log-scaling "
+                             "the tables were built with")
+        out = list(outer_extrapolation(p0, d0, r))
+        if t.log_scaling:
+            inner = list(inner_extrapolation(p0, d0, r))
+        else:
+            inner = [0.0, 0.0, 0.0, float(p0[0])]
+        return [float(v) for v in inner + out]
+
+    def _set_nodes(self, phi: torch.Tensor, dphi_dr: torch.Tensor,
+                   rebuild_constants: bool = True) -> None:
         if phi.shape != self.tables.node_phi.shape or dphi_dr.shape != phi.shape:
             raise ValueError(f"node tables must have shape {self.tables.node_phi.shape}")
         dev = phi.device if phi.device.type == "cuda" else _cuda_device()
         phi = phi.detach().to(dev, torch.float64).clone()
         dphi_dr = dphi_dr.detach().to(dev, torch.float64).clone()
-        im, p32 = self._device_tables(phi, dphi_dr)
+        t = self.tables
+        built = [t.invPhi0, t.inner_s, t.inner_U, t.inner_W, t.outer_s, t.outer_U, t.outer_W]
+        consts = self._builder_scalars(phi, dphi_dr) if rebuild_constants else built
+        im, p32 = self._device_tables(phi, dphi_dr, inv=consts[0])
         self._nodes = (phi, dphi_dr)
         self._node_tables = (im, p32)
         for cdev, (_, keep) in self.__dict__.get("_dev_cache", {}).items():
             keep[0].copy_(im.to(cdev), non_blocking=True)
             keep[1].copy_(p32.to(cdev), non_blocking=True)
+        if consts != self.__dict__.get("_consts", built):
+            self._consts = consts
+            for c, _ in self.__dict__.get("_dev_cache", {}).values():
+                for i, v in enumerate(consts):
+                    c.p[3 + i] = v
+            self._consts_gen = self.__dict__.get("_consts_gen", 0) + 1
 
     def _upload(self, dev):
         t = self.tables
@@ -1151,6 +1234,8 @@ class MultipolePotentialGPU(_Component):
         c.lm = lm.data_ptr()
         for i, v in enumerate(t.scalars()):
             c.p[i] = v
+        for i, v in enumerate(self.__dict__.get("_consts") or []):     # set_node_tables
+            c.p[3 + i] = v
         return c, (poly, poly32, lm)
 
 

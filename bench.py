@@ -243,7 +243,7 @@ def adjoint_ratio(dev, n_streams: int, per_stream: int, n_steps: int, precision:
     e1.record()
     lx, lv, tg = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT),
                                table_grads=True, reconstruct=reconstruct)
-    gnodes = mp.node_gradients(tg[mp])
+    gnodes = mp.node_gradients(tg[mp], tg.get(("const", mp)))
     e2.record()
     lx2, _ = integ.adjoint(ck, n_steps, 2 * (xT - target), torch.zeros_like(vT),
                            reconstruct=reconstruct)

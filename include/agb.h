@@ -265,17 +265,23 @@ int agb_eval_vjp_force(const agb_component* comps, int n_comps,
  * component's interval-major FP64 table [n_int][n_lm][6], the sum over points
  * of dL/da_{c,k,j} for cotangents g_phi [N] (dL/dPhi) and g_force [N,3]
  * (dL/dF) of the composite's outputs; leaf gives the component's transform.
- * Points outside the radial grid contribute nothing (the extrapolation
- * constants are held fixed).  FP64; points are sorted by interval in scratch
+ * g_const (NULL, or AGB_MP_NCONST = 8 doubles, accumulated): the gradient with
+ * respect to the scalars the table builder derives from the nodes -- invPhi0
+ * (p[3]; from the points inside the grid), the inner s, U, W (p[4..6]; points
+ * inside the first node) and, for the points beyond the last node, the outer
+ * fit in the well-conditioned variables eps = s + 1, T = U eps, S = U + W of
+ * (s, U, W) = p[7..9] (the fit is usually degenerate: s = -1 to rounding,
+ * U ~ -W ~ 1e16) -- and 0.  FP64; points are sorted by interval in scratch
  * (workspace as for agb_eval_ws, NULL: allocated stream-ordered inside) and
  * each warp reduces its lanes before one atomic add per coefficient.
  * No counterpart in the reference.
  */
+#define AGB_MP_NCONST 8
 size_t agb_multipole_table_vjp_workspace_bytes(const agb_component* comp,
                                                const agb_leaf* leaf, int64_t n);
 int agb_multipole_table_vjp(const agb_component* comp, const agb_leaf* leaf,
                             const double* xyz, int64_t n, const double* g_phi,
-                            const double* g_force, double* g_table,
+                            const double* g_force, double* g_table, double* g_const,
                             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
@@ -295,8 +301,8 @@ size_t agb_multipole_adjoint_workspace_bytes(const agb_component* comp, const ag
 int agb_multipole_adjoint(const agb_component* comp, const agb_leaf* leaf,
                           const double* xyz, int64_t n, int precision,
                           const double* g_phi, const double* g_force, double* g_xyz,
-                          double* g_table, void* workspace, size_t workspace_bytes,
-                          void* stream);
+                          double* g_table, double* g_const, void* workspace,
+                          size_t workspace_bytes, void* stream);
 
 /*
  * agb_multipole_adjoint that also ADDS this leaf's force, -A sigma grad Phi,
@@ -307,7 +313,8 @@ int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
                                 const double* xyz, int64_t n, int precision,
                                 const double* g_phi, const double* g_force,
                                 double* g_xyz, double* force, double* g_table,
-                                void* workspace, size_t workspace_bytes, void* stream);
+                                double* g_const, void* workspace, size_t workspace_bytes,
+                                void* stream);
 
 /*
  * One backward step of the leapfrog adjoint for a tree of one Multipole leaf
@@ -331,8 +338,8 @@ size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, int n_comps,
                                         int64_t n, int flags);
 int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                      int n_leaves, int mp_leaf, int precision, double* x, double* vh,
-                     double* lx, double* lv, double* gF, double* g_table, int64_t n,
-                     double dt, double c, double k, double dt_drift, int flags,
+                     double* lx, double* lv, double* gF, double* g_table, double* g_const,
+                     int64_t n, double dt, double c, double k, double dt_drift, int flags,
                      void* workspace, size_t workspace_bytes, void* stream);
 
 /*

@@ -142,7 +142,7 @@ def test_leapfrog_backward_fills_node_grads():
 def test_potential_and_force_node_grads_and_in_place_updates():
     import torch
     from agama_gpu_b200 import autograd
-    from agama_gpu_b200.diff_tables import multipole_poly_from_nodes
+    from agama_gpu_b200.diff_tables import multipole_consts_from_nodes, multipole_poly_from_nodes
     from oracle.torch_mp import multipole_phi
     mp, _, pot = _pot(lmax=6)
     phi, dphi = mp.node_parameters()
@@ -161,13 +161,19 @@ def test_potential_and_force_node_grads_and_in_place_updates():
     p2, f2 = pot2.eval(x, pot=True, acc=True)
     assert torch.equal(p1, p2) and torch.equal(f1, f2)
     ((p1 * gp).sum() + (f1 * gf).sum()).backward()
-    # torch autograd of the same loss through the restatement
+    # torch autograd of the same loss through the restatement, invPhi0 a function of
+    # the nodes as the builder makes it (the points stay inside the radial grid)
     t = mp.tables
     pt = phi.detach().cpu().clone().requires_grad_(True)
     dt_ = dphi.detach().cpu().clone().requires_grad_(True)
-    poly = multipole_poly_from_nodes(t, pt, dt_)
+    k = multipole_consts_from_nodes(t, pt, dt_)
+    poly = multipole_poly_from_nodes(t, pt, dt_, inv=k[0])
     xr = x.cpu().clone().requires_grad_(True)
-    ph = multipole_phi(poly, t.lm_l, t.lm_m, t.scalars(), t.log_scaling, xr)
+    r = xr.detach().norm(dim=1)
+    assert float(r.min()) > t.r_grid[0] and float(r.max()) < t.r_grid[-1]
+    sc = list(t.scalars())
+    sc[3] = k[0]
+    ph = multipole_phi(poly, t.lm_l, t.lm_m, sc, t.log_scaling, xr)
     (g,) = torch.autograd.grad(ph.sum(), xr, create_graph=True)
     ((ph * gp.cpu()).sum() - (g * gf.cpu()).sum()).backward()
     for got, want in ((phi.grad.cpu(), pt.grad), (dphi.grad.cpu(), dt_.grad)):
