@@ -66,15 +66,20 @@ def _torch_leapfrog_loss(mp, phi, dphi, x0, v0, target):
     """The same leapfrog in FP64 torch with the Multipole force from the node tables
     (builder restatement -> oracle/torch_mp.py) plus Miyamoto-Nagai; autograd-able."""
     import torch
-    from agama_gpu_b200.diff_tables import multipole_poly_from_nodes
+    from agama_gpu_b200.diff_tables import multipole_consts_from_nodes, multipole_poly_from_nodes
     from oracle.torch_mp import multipole_phi
     t = mp.tables
-    poly = multipole_poly_from_nodes(t, phi, dphi)
+    # invPhi0 a function of the nodes, as the builder makes it (the orbits stay inside
+    # the radial grid, where it is the only one of the builder's scalars in use)
+    k = multipole_consts_from_nodes(t, phi, dphi)
+    poly = multipole_poly_from_nodes(t, phi, dphi, inv=k[0])
+    sc = list(t.scalars())
+    sc[3] = k[0]
 
     def force(x):
         with torch.enable_grad():
             xr = x if x.requires_grad else x.detach().requires_grad_(True)
-            p = multipole_phi(poly, t.lm_l, t.lm_m, t.scalars(), t.log_scaling, xr)
+            p = multipole_phi(poly, t.lm_l, t.lm_m, sc, t.log_scaling, xr)
             (g,) = torch.autograd.grad(p.sum(), xr, create_graph=True)
         return -g + _mn_force_torch(x)
 
