@@ -193,6 +193,11 @@ def _load():
         ctypes.c_void_p]
     lib.agb_batch_workspace_bytes.restype = ctypes.c_size_t
     lib.agb_batch_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.agb_batch_sort_workspace_bytes.restype = ctypes.c_size_t
+    lib.agb_batch_sort_workspace_bytes.argtypes = [ctypes.c_void_p]
+    lib.agb_batch_sort.restype = ctypes.c_int
+    lib.agb_batch_sort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_batch_points.restype = ctypes.c_int64
     lib.agb_batch_points.argtypes = [ctypes.c_void_p]
     lib.agb_batch_tiles.restype = ctypes.c_int
@@ -239,6 +244,7 @@ EXPORTED = [
     "agb_multipole_adjoint", "agb_multipole_adjoint_workspace_bytes", "agb_cylspline_table_vjp",
     "agb_adjoint_step", "agb_adjoint_step_workspace_bytes", "agb_adjoint_kick", "agb_reverse_drift",
     "agb_batch_create", "agb_batch_eval", "agb_batch_eval_ws", "agb_batch_workspace_bytes",
+    "agb_batch_sort", "agb_batch_sort_workspace_bytes",
     "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy", "agb_time_plan_create", "agb_time_plan_destroy",
     "agb_time_plan_leaves_host", "agb_time_plan_leaves", "agb_eval_timed_workspace_bytes",

@@ -57,6 +57,9 @@ class BatchedPotentialGPU(_GPUPotBase):
         # launch (agb_batch_eval_ws), in a workspace the object keeps per device,
         # precision and stream
         self.presort = bool(presort)
+        # set by the integrators while they keep the particles in sort_order(): the
+        # rows are then evaluated in order (no pre-sort, no in-tile sort)
+        self._rows_in_order = False
         self._plans = {}
         self._ws = {}
 
@@ -132,7 +135,8 @@ class BatchedPotentialGPU(_GPUPotBase):
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         stream = torch.cuda.current_stream(dev).cuda_stream
         ws, nws = None, 0
-        if self.presort:
+        flags = _lib.OUT_NEGATE | (_lib.OUT_NO_BINNING if self._rows_in_order else 0)
+        if self.presort and not self._rows_in_order:
             nws = int(_lib.lib.agb_batch_workspace_bytes(plan, mode))
             if nws:
                 key = (dev.index, prec, stream)
@@ -141,10 +145,32 @@ class BatchedPotentialGPU(_GPUPotBase):
                     ws = torch.empty(nws, dtype=torch.uint8, device=dev)
                     self._ws[key] = ws
         rc = _lib.lib.agb_batch_eval_ws(plan, arr.data_ptr(), mode, ptr(phi), ptr(grad), ptr(hess),
-                                        ptr(rho), _lib.OUT_NEGATE, ptr(ws), nws,
+                                        ptr(rho), flags, ptr(ws), nws,
                                         ctypes.c_void_p(stream))
         _lib.check(rc, "agb_batch_eval_ws")
         return phi, grad, hess, rho
+
+    def sort_order(self, xyz: torch.Tensor, precision: Optional[str] = None) -> Optional[torch.Tensor]:
+        """(N,) int64 device permutation: rows in the order the batch evaluates best --
+        each unit's particles by the radial interval of its Multipole, inside the unit's
+        own rows (xyz[order] keeps unit u in unit_rows(u)); None when the units cannot
+        be sorted.  The leapfrog integrator keeps the particles in this order during a
+        run and evaluates them without sorting."""
+        arr = xyz.to(torch.float64).contiguous()
+        if arr.shape[0] != self.n_points:
+            raise ValueError(f"the batch holds {self.n_points} particles, got {arr.shape[0]}")
+        dev = arr.device
+        prec = _PRECISIONS[precision or self.precision or _default()]
+        plan = self._plan(dev, prec)
+        nws = int(_lib.lib.agb_batch_sort_workspace_bytes(plan))
+        if nws == 0:
+            return None
+        ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        perm = torch.empty(self.n_points, dtype=torch.int32, device=dev)
+        rc = _lib.lib.agb_batch_sort(plan, arr.data_ptr(), perm.data_ptr(), ws.data_ptr(), nws,
+                                     ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        _lib.check(rc, "agb_batch_sort")
+        return perm.long()
 
     def _vjp(self, *args, **kw):
         raise NotImplementedError("position derivatives are not batched")

@@ -61,8 +61,9 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         const BinKey K = a.ukey[T.unit];
         const int nb = K.n_int + 2;
         // points pre-sorted by agb_batch_eval_ws: a tile is a run of sorted positions
-        const bool sorted = !a.perm && K.n_int >= 0 && nb <= AGB_BATCH_MAX_BINS &&
-                            T.count <= AGB_BATCH_SORT_MAX;
+        // (AGB_OUT_NO_BINNING: the caller keeps the rows in interval order itself)
+        const bool sorted = !a.perm && !(a.out_flags & AGB_OUT_NO_BINNING) && K.n_int >= 0 &&
+                            nb <= AGB_BATCH_MAX_BINS && T.count <= AGB_BATCH_SORT_MAX;
         if (sorted) {
             for (int q = threadIdx.x; q < nb; q += blockDim.x) s_hist[q] = 0;
             __syncthreads();
@@ -211,9 +212,11 @@ batch_bin_scatter(const BatchTile* __restrict__ tiles, const int* __restrict__ u
         const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
         perm[pos] = (int)i;
         keys[i] = (int)pos;
-        xs[3 * pos] = xyz[3 * i];
-        xs[3 * pos + 1] = xyz[3 * i + 1];
-        xs[3 * pos + 2] = xyz[3 * i + 2];
+        if (xs) {
+            xs[3 * pos] = xyz[3 * i];
+            xs[3 * pos + 1] = xyz[3 * i + 1];
+            xs[3 * pos + 2] = xyz[3 * i + 2];
+        }
     }
 }
 
@@ -456,15 +459,12 @@ static int launch_batch(const BatchArgs& a, cudaStream_t st)
 
 static std::atomic<unsigned long long> g_batch_bin_attr{0};     // one bit per device
 
-static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchArgs& a,
-                         cudaStream_t st)
+// the counting sort of the pre-sort: perm (sorted position -> row), keys (row -> sorted
+// position), xs (the sorted copy of the points, when given)
+static int batch_sort(const agb_batch* p, const double* xyz, int* keys, int* perm, double* xs,
+                      int* counts, cudaStream_t st)
 {
-    const size_t n = (size_t)p->n_points;
-    int* keys = (int*)ws;
-    int* perm = (int*)(ws + al256(4 * n));
-    double* xs = (double*)(ws + 2 * al256(4 * n));
-    int* counts = (int*)(ws + 2 * al256(4 * n) + al256(24 * n));
-    int* cursor = (int*)((char*)counts + al256(4 * (size_t)p->n_bins));
+    int* cursor = counts + p->n_bins;
     const unsigned long long bit = 1ull << current_device();
     if (!(g_batch_bin_attr.load(std::memory_order_acquire) & bit)) {
         cudaFuncSetAttribute(batch_bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -482,10 +482,51 @@ static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchA
     bin_scan<<<1, 1024, 0, st>>>(counts, cursor, p->n_bins);
     if ((rc = check_launch("bin_scan"))) return rc;
     batch_bin_scatter<<<p->n_tiles, 256, 2 * h, st>>>(p->tiles, p->ubin, xyz, keys, cursor, perm, xs);
-    if ((rc = check_launch("batch_bin_scatter"))) return rc;
+    return check_launch("batch_bin_scatter");
+}
+
+static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchArgs& a,
+                         cudaStream_t st)
+{
+    const size_t n = (size_t)p->n_points;
+    int* keys = (int*)ws;
+    int* perm = (int*)(ws + al256(4 * n));
+    double* xs = (double*)(ws + 2 * al256(4 * n));
+    int* counts = (int*)(ws + 2 * al256(4 * n) + al256(24 * n));
+    const int rc = batch_sort(p, xyz, keys, perm, xs, counts, st);
+    if (rc) return rc;
     a.xyz = xs;
     a.perm = perm;
     return AGB_OK;
+}
+
+extern "C" size_t agb_batch_sort_workspace_bytes(const agb_batch* plan)
+{
+    if (!plan || plan->n_bins == 0 || plan->n_tiles == 0) return 0;
+    return al256(4 * (size_t)plan->n_points) + al256(8 * (size_t)plan->n_bins);
+}
+
+extern "C" int agb_batch_sort(const agb_batch* plan, const double* xyz, int32_t* perm,
+                              void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (!plan) return set_err(AGB_ERR_ARG, "agb_batch_sort: plan is null");
+    if (plan->n_tiles == 0) return AGB_OK;
+    if (plan->n_bins == 0)
+        return set_err(AGB_ERR_UNSUPPORTED, "agb_batch_sort: the plan's units cannot be sorted "
+                       "(more than %d intervals or 2^31 points)", AGB_MAX_BINS - 2);
+    if (!xyz || !perm) return set_err(AGB_ERR_ARG, "agb_batch_sort: null array");
+    const size_t need = agb_batch_sort_workspace_bytes(plan);
+    if (!workspace || ((uintptr_t)workspace & 255u) || workspace_bytes < need)
+        return set_err(AGB_ERR_ARG, "agb_batch_sort: a 256-byte aligned workspace of %zu bytes "
+                       "is required", need);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != plan->device)
+        return set_err(AGB_ERR_ARG, "agb_batch_sort: plan lives on device %d, current is %d",
+                       plan->device, cur);
+    char* ws = (char*)workspace;
+    return batch_sort(plan, xyz, (int*)ws, (int*)perm, nullptr,
+                      (int*)(ws + al256(4 * (size_t)plan->n_points)), (cudaStream_t)stream);
 }
 
 extern "C" int agb_batch_eval(const agb_batch* plan, const double* xyz, int mode, double* phi,
@@ -523,7 +564,7 @@ extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int m
     a.perm = nullptr; a.stage = nullptr;
     int rc = AGB_OK;
     const int* dest = nullptr;
-    if (workspace && plan->n_bins > 0) {
+    if (workspace && plan->n_bins > 0 && !(out_flags & AGB_OUT_NO_BINNING)) {
         const size_t need = batch_ws_bytes(plan);
         if (((uintptr_t)workspace & 255u) || workspace_bytes < need)
             return set_err(AGB_ERR_ARG, "agb_batch_eval_ws: workspace of %zu bytes (256-byte "

@@ -297,7 +297,40 @@ class Leapfrog:
         (substep = step * S) and at the end.  k = 1 keeps the positions at every substep
         (v is None except at the end) and the adjoint then re-computes nothing;
         checkpoint_every=None picks k with ``auto_checkpoint_every`` (1 whenever the
-        trajectory fits in 60% of the free device memory)."""
+        trajectory fits in 60% of the free device memory).
+
+        A batch of potentials (BatchedPotentialGPU with its pre-sort on) is integrated
+        with its particles in the batch's sort_order() of x0: every force of the run
+        then visits the rows in order without sorting them again (results are per
+        particle and do not depend on the order); x_T, v_T and the checkpoints come
+        back in the caller's order."""
+        order = self._sort_order(x0)
+        if order is None:
+            return self._run(x0, v0, n_steps, checkpoint_every)
+        self.pot._rows_in_order = True
+        try:
+            xT, vT, ck = self._run(x0.detach()[order], v0.detach()[order], n_steps,
+                                   checkpoint_every)
+        finally:
+            self.pot._rows_in_order = False
+
+        def back(a):
+            if a is None:
+                return None
+            out = torch.empty_like(a)
+            out[order] = a
+            return out
+        return back(xT), back(vT), [(g, back(xs), back(vs)) for g, xs, vs in ck]
+
+    def _sort_order(self, x0: torch.Tensor):
+        """The batch's evaluation order of x0's rows (None: keep the caller's order)."""
+        pot = self.pot
+        if not (x0.is_cuda and getattr(pot, "presort", False) and hasattr(pot, "sort_order")):
+            return None
+        return pot.sort_order(x0.detach(), precision=self.precision)
+
+    def _run(self, x0: torch.Tensor, v0: torch.Tensor, n_steps: int,
+             checkpoint_every: Optional[int] = 64) -> Tuple[torch.Tensor, torch.Tensor, List]:
         x, v, F = self._buffers(x0)
         x.copy_(x0.detach())
         v.copy_(v0.detach())

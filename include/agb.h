@@ -432,6 +432,18 @@ void    agb_batch_destroy(agb_batch* plan);
  * workspace is agb_batch_eval.  Results equal agb_batch_eval's bit for bit.
  */
 size_t  agb_batch_workspace_bytes(const agb_batch* plan, int mode);
+/*
+ * The pre-sort's permutation alone: perm[pos] = the row at sorted position pos
+ * (each unit's rows ordered by the radial interval of its sort key, inside the
+ * unit's own rows).  A caller that keeps its particle arrays in this order (an
+ * integrator between re-sorts) evaluates them with AGB_OUT_NO_BINNING in out_flags:
+ * the rows are then visited in order, with no pre-sort, no in-tile sort and no
+ * workspace.  Workspace: agb_batch_sort_workspace_bytes(plan) bytes, 256-byte
+ * aligned.  Results do not depend on the order.
+ */
+size_t  agb_batch_sort_workspace_bytes(const agb_batch* plan);
+int     agb_batch_sort(const agb_batch* plan, const double* xyz, int32_t* perm,
+                       void* workspace, size_t workspace_bytes, void* stream);
 int     agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int mode,
                           double* phi, double* grad, double* hess, double* rho,
                           int out_flags, void* workspace, size_t workspace_bytes,

@@ -159,6 +159,36 @@ def test_batch_leapfrog_graph_matches_per_unit():
         assert float((vT[rows] - vu).abs().max()) <= 1e-10 * float(vu.abs().max())
 
 
+def test_batch_leapfrog_in_sort_order_is_bit_equal():
+    """The integrator keeps a batch's particles in the batch's sort order (each unit's
+    rows sorted by interval, inside the unit) and evaluates them without sorting:
+    positions, velocities and checkpoints equal those of the run in the caller's order
+    with the in-tile sort, bit for bit."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    units, counts = _units()
+    rng = np.random.default_rng(14)
+    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512)
+    plain = agb.BatchedPotentialGPU(units, counts, tile_points=512, presort=False)
+    n = sorted_.n_points
+    x0 = torch.from_numpy(_points(n, 15)).cuda()
+    v0 = torch.from_numpy(rng.normal(0, 50.0, (n, 3))).cuda()
+    order = sorted_.sort_order(x0)
+    assert sorted(order.tolist()) == list(range(n))
+    for u in range(len(units)):
+        rows = sorted_.unit_rows(u)
+        got = order[rows]
+        assert bool(((got >= rows.start) & (got < rows.stop)).all())
+    for graph in (True, False):
+        a = Leapfrog(sorted_, 0.002, use_graph=graph, graph_steps=4).run(x0, v0, 9, checkpoint_every=4)
+        b = Leapfrog(plain, 0.002, use_graph=graph, graph_steps=4).run(x0, v0, 9, checkpoint_every=4)
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]), graph
+        for (ga, xa, va), (gb, xb, vb) in zip(a[2], b[2]):
+            assert ga == gb and torch.equal(xa, xb) and torch.equal(va, vb)
+        assert not sorted_._rows_in_order
+
+
 def test_batch_rejects_wrong_size():
     import torch
     import agama_gpu_b200 as agb
