@@ -54,6 +54,14 @@ def test_argument_errors_need_no_gpu():
     assert _lib.lib.agb_eval(comps, 1, leaves, 1, None, 0, 1, 0, None, ctypes.c_void_p(16),
                              None, None, 0, None) == 0
     assert _lib.lib.agb_eval_workspace_bytes(comps, 1, leaves, 1, 10**6, 0) == 0   # no Multipole
+    # batch entries without a plan: errors and zero sizes before any CUDA call
+    assert _lib.lib.agb_batch_workspace_bytes(None, 1) == 0
+    assert _lib.lib.agb_batch_sort_workspace_bytes(None) == 0
+    rc = _lib.lib.agb_batch_sort(None, ctypes.c_void_p(16), ctypes.c_void_p(16), None, 0, None)
+    assert rc == -1 and "plan is null" in _lib.last_error()
+    rc = _lib.lib.agb_batch_eval_ws(None, ctypes.c_void_p(16), 1, None, ctypes.c_void_p(16),
+                                    None, None, 0, None, 0, None)
+    assert rc == -1 and "plan is null" in _lib.last_error()
     # an undefined block-size code among the launch-shape bits
     rc = _lib.lib.agb_eval(comps, 1, leaves, 1, ctypes.c_void_p(16), 10, 1, 0, None,
                            ctypes.c_void_p(16), None, None, 3 << _lib.OUT_BLOCK_SHIFT, None)
