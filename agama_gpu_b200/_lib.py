@@ -17,6 +17,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 OUT_NEGATE = 1
 OUT_NO_BINNING = 2
 OUT_BIN_ALWAYS = 4
+OUT_STAGE = 32
 OUT_GRID_SHIFT = 8
 OUT_BLOCK_SHIFT = 12
 OUT_PPT_SHIFT = 16
@@ -195,6 +196,8 @@ def _load():
     lib.agb_batch_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.agb_batch_sort_workspace_bytes.restype = ctypes.c_size_t
     lib.agb_batch_sort_workspace_bytes.argtypes = [ctypes.c_void_p]
+    lib.agb_batch_stage_errors.restype = ctypes.c_int
+    lib.agb_batch_stage_errors.argtypes = [ctypes.c_void_p]
     lib.agb_batch_sort.restype = ctypes.c_int
     lib.agb_batch_sort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
@@ -244,7 +247,7 @@ EXPORTED = [
     "agb_multipole_adjoint", "agb_multipole_adjoint_workspace_bytes", "agb_cylspline_table_vjp",
     "agb_adjoint_step", "agb_adjoint_step_workspace_bytes", "agb_adjoint_kick", "agb_reverse_drift",
     "agb_batch_create", "agb_batch_eval", "agb_batch_eval_ws", "agb_batch_workspace_bytes",
-    "agb_batch_sort", "agb_batch_sort_workspace_bytes",
+    "agb_batch_sort", "agb_batch_sort_workspace_bytes", "agb_batch_stage_errors",
     "agb_batch_points", "agb_batch_tiles",
     "agb_batch_destroy", "agb_time_plan_create", "agb_time_plan_destroy",
     "agb_time_plan_leaves_host", "agb_time_plan_leaves", "agb_eval_timed_workspace_bytes",

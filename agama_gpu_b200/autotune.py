@@ -17,7 +17,9 @@ harmonics, how many components), the number of points and the mode:
   AGB_BIN_MIN_POINTS points on), never, or always.  The sort costs three small
   launches and 32 B of scratch per point; it pays when the harmonic sums are
   long.
-* tile_points (batches): points per work-queue tile of a BatchedPotentialGPU.
+* tile_points and stage (batches): points per work-queue tile of a
+  BatchedPotentialGPU, and whether each tile's table rows are bulk-copied (TMA)
+  into shared memory or read through L1/L2.
 
 ``autotune(pot, xyz)`` times every candidate on the caller's own points with
 CUDA events, keeps the fastest for that (mode, precision, size class) on the
@@ -171,17 +173,21 @@ def apply_cached(pot, n: int, mode: str = "force", t: float = 0.0,
 
 def tune_batch(batch, xyz, tiles=(1024, 2048, 4096, 8192), precision: Optional[str] = None,
                reps: int = 3) -> Dict:
-    """Pick the work-queue tile size of a BatchedPotentialGPU on its own points."""
+    """Pick the work-queue tile size of a BatchedPotentialGPU, and whether its tiles'
+    table rows are staged in shared memory by bulk copy (``stage``), on its own points.
+    Returns {"best": (tile_points, stage), "ms": {(tile_points, stage): ms}}."""
     arr, _ = prep_xyz(xyz)
     F = torch.empty_like(arr)
     times = {}
     for tp in tiles:
         batch.tile_points = int(tp)
         batch._release_plans()
-        times[int(tp)] = _time(lambda: batch._launch(arr, 0.0, _lib.MODE_GRAD, False,
-                                                     precision=precision,
-                                                     out=(None, F, None, None)), reps)
+        for st in (False, True):
+            batch.stage = st
+            times[(int(tp), st)] = _time(lambda: batch._launch(arr, 0.0, _lib.MODE_GRAD, False,
+                                                               precision=precision,
+                                                               out=(None, F, None, None)), reps)
     best = min(times, key=times.get)
-    batch.tile_points = best
+    batch.tile_points, batch.stage = best
     batch._release_plans()
     return {"best": best, "ms": times}

@@ -19,6 +19,17 @@
 #define AGB_BATCH_SORT_MAX 8192        // largest tile that is sorted (34 KB of shared memory)
 #define AGB_BATCH_MAX_BINS 256         // most intervals (+2) of a sorted unit
 
+// Staging (AGB_OUT_STAGE, mixed precision, points pre-sorted): a tile of sorted
+// points spans a run of intervals k0..k1 of its unit's keyed Multipole; one thread
+// bulk-copies those rows of the FP32 table (contiguous in the interval-major layout,
+// as many as fit in AGB_BATCH_STAGE_BYTES) into shared memory while the others wait
+// on an mbarrier, and the walk of that component reads them there instead of
+// through L1/L2.  A wait that gives up (bounded) records an error and the block reads
+// global memory from then on.
+#define AGB_BATCH_STAGE_BYTES (64 * 1024)
+#define AGB_BATCH_STAGE_TRIES (1 << 22)
+#include "bulk.cuh"
+
 struct BatchTile {
     long long start;          // first point (row of xyz)
     int unit;
@@ -41,21 +52,84 @@ struct BatchArgs {
     double* rho;
     const int* perm;          // presorted: sorted position -> row of the caller's arrays
     double* stage;            // presorted with room: per-position output records
+    int* err;                 // ST: set to 1 when a staging wait gave up (sticky)
 };
 
-template <int MODE, typename R>
+// ST: stage the keyed Multipole's interval rows of each tile (see above; FP32 only)
+template <int MODE, typename R, bool ST = false>
 __global__ void __launch_bounds__(256, (MODE == AGB_MODE_HESS) ? 1 : 2)
 agb_batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ int s_tile;
     __shared__ int s_hist[AGB_BATCH_MAX_BINS], s_cur[AGB_BATCH_MAX_BINS];
     __shared__ unsigned short s_key[AGB_BATCH_SORT_MAX], s_order[AGB_BATCH_SORT_MAX];
+    extern __shared__ __align__(128) float agb_batch_slab[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_k0, s_k1, s_dead;
+    unsigned phase = 0;
+    if (ST) {
+        if (threadIdx.x == 0) {
+            mbar_init(&s_bar, 1);
+            s_dead = 0;
+        }
+        __syncthreads();
+    }
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(a.counter, 1);
+        if (ST) __syncthreads();          // the previous tile's reads of the slab are done
+        if (threadIdx.x == 0) {
+            s_tile = atomicAdd(a.counter, 1);
+            if (ST) {
+                // the tile's in-grid interval run from its first and last (sorted) point
+                int k0 = 0, k1 = -1;
+                const int tt = s_tile;
+                if (tt < a.n_tiles && !s_dead) {
+                    const BatchTile T = a.tiles[tt];
+                    const BinKey K = a.ukey[T.unit];
+                    const DevComp* kc = K.comp >= 0 ? &a.comps[K.comp] : nullptr;
+                    if (kc && K.n_int > 0 && kc->kind == AGB_KIND_MULTIPOLE && kc->table32 &&
+                        kc->structure != AGB_STRUCT_LIST && T.count > 0) {
+                        const long long p0 = T.start, p1 = T.start + T.count - 1;
+                        const int b0 = bin_of(K, a.xyz[3 * p0], a.xyz[3 * p0 + 1], a.xyz[3 * p0 + 2]);
+                        const int b1 = bin_of(K, a.xyz[3 * p1], a.xyz[3 * p1 + 1], a.xyz[3 * p1 + 2]);
+                        const long long row = 32LL * kc->n_lm;          // bytes per interval
+                        if (b0 < K.n_int && row <= AGB_BATCH_STAGE_BYTES) {
+                            k0 = b0;
+                            k1 = b1 < K.n_int ? b1 : K.n_int - 1;
+                            if (k1 < k0) k1 = k0;
+                            const int fit = (int)(AGB_BATCH_STAGE_BYTES / row);
+                            if (k1 - k0 + 1 > fit) k1 = k0 + fit - 1;
+                            const unsigned bytes = (unsigned)((k1 - k0 + 1) * row);
+                            // the previous tile's generic reads of the slab come first
+                            fence_proxy_async_smem();
+                            mbar_arrive_expect_tx(&s_bar, bytes);
+                            bulk_copy_g2s(agb_batch_slab, kc->table32 + (long long)k0 * kc->n_lm * 8,
+                                          bytes, &s_bar);
+                        }
+                    }
+                }
+                s_k0 = k0;
+                s_k1 = k1;
+            }
+        }
         __syncthreads();
         const int t = s_tile;
+        int k0 = 0, k1 = -1;
+        if (ST) { k0 = s_k0; k1 = s_k1; }
         __syncthreads();                  // every thread has read s_tile before it changes
-        if (t >= a.n_tiles) return;
+        if (t >= a.n_tiles) return;       // (no copy is issued for t >= n_tiles)
+        if (ST && k1 >= k0) {
+            const bool ok = mbar_wait_bounded(&s_bar, phase, AGB_BATCH_STAGE_TRIES);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) {  // gave up: read global memory from here on
+                k1 = k0 - 1;
+                if (threadIdx.x == 0) {
+                    s_dead = 1;
+                    if (a.err) atomicExch(a.err, 1);
+                    // the copy in flight must land before the block can exit
+                    mbar_wait_bounded(&s_bar, phase ^ 1u, AGB_BATCH_STAGE_TRIES);
+                }
+            }
+        }
         const BatchTile T = a.tiles[t];
         const int l0 = a.unit_leaf[T.unit], l1 = a.unit_leaf[T.unit + 1];
         const BinKey K = a.ukey[T.unit];
@@ -110,8 +184,12 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
                 o.g[0] = o.g[1] = o.g[2] = 0.0;
                 #pragma unroll
                 for (int q = 0; q < 6; ++q) o.h[q] = 0.0;
-                eval_component<MODE, R, false>(c, lf.sigma * x - lf.g0, lf.sigma * y - lf.g1,
-                                               lf.sigma * z - lf.g2, o);
+                if (ST && k1 >= k0 && lf.comp == K.comp)     // the staged component
+                    multipole_point<MODE, R, true>(c, lf.sigma * x - lf.g0, lf.sigma * y - lf.g1,
+                                                   lf.sigma * z - lf.g2, o, agb_batch_slab, k0, k1);
+                else
+                    eval_component<MODE, R, false>(c, lf.sigma * x - lf.g0, lf.sigma * y - lf.g1,
+                                                   lf.sigma * z - lf.g2, o);
                 const double A = lf.ampl;
                 if (MODE == AGB_MODE_DENS) {
                     rho += (A * lf.sigma * lf.sigma) * o.rho;
@@ -306,8 +384,10 @@ extern "C" int agb_batch_create(const agb_component* comps, int n_comps, const a
                 best = L;
         }
         hk[u].n_int = -1;
+        hk[u].comp = -1;
         if (best >= 0) {
             const agb_component& c = comps[leaves[best].comp];
+            hk[u].comp = leaves[best].comp;
             hk[u].sigma = leaves[best].sigma;
             hk[u].g0 = leaves[best].gamma[0]; hk[u].g1 = leaves[best].gamma[1];
             hk[u].g2 = leaves[best].gamma[2];
@@ -450,11 +530,45 @@ extern "C" size_t agb_batch_workspace_bytes(const agb_batch* plan, int mode)
 template <int MODE, typename R>
 static int launch_batch(const BatchArgs& a, cudaStream_t st)
 {
+    // staging: FP32 tables, points pre-sorted by this call.  (Rows an integrator keeps
+    // in the order of its run's start drift apart along r: a tile's first and last
+    // points then bound its intervals less well, and 100 config-4 leapfrog steps took
+    // 1363 ms staged against 1307 ms unstaged.)
+    const bool stage = std::is_same<R, float>::value && (a.out_flags & AGB_OUT_STAGE) && a.perm;
+    if (stage) {
+        static std::atomic<int> cache_st[AGB_MAX_DEVICES];
+        const int dev = current_device();
+        int per_sm = cache_st[dev].load(std::memory_order_relaxed);
+        if (per_sm == 0) {
+            cudaFuncSetAttribute(agb_batch_kernel<MODE, R, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, AGB_BATCH_STAGE_BYTES);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, agb_batch_kernel<MODE, R, true>,
+                                                              256, AGB_BATCH_STAGE_BYTES) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            cache_st[dev].store(per_sm, std::memory_order_relaxed);
+        }
+        const long long grid = std::min<long long>((long long)num_sms() * per_sm, a.n_tiles);
+        agb_batch_kernel<MODE, R, true><<<(int)std::max<long long>(grid, 1), 256,
+                                          AGB_BATCH_STAGE_BYTES, st>>>(a);
+        return check_launch("agb_batch_kernel");
+    }
     static std::atomic<int> cache[AGB_MAX_DEVICES];   // resident blocks per SM, per device
     const int per_sm = blocks_per_sm(cache, agb_batch_kernel<MODE, R>, 256);
     const long long grid = std::min<long long>((long long)num_sms() * per_sm, a.n_tiles);
     agb_batch_kernel<MODE, R><<<(int)std::max<long long>(grid, 1), 256, 0, st>>>(a);
     return check_launch("agb_batch_kernel");
+}
+
+// 1 when a staged batch kernel of this plan gave up waiting for a bulk copy (its
+// blocks then read global memory; results are unaffected), else 0; -1 on error
+extern "C" int agb_batch_stage_errors(const agb_batch* plan)
+{
+    if (!plan) return set_err(AGB_ERR_ARG, "agb_batch_stage_errors: plan is null");
+    int v = 0;
+    if (cudaMemcpy(&v, plan->counter + 1, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return set_err(AGB_ERR_DEVICE, "agb_batch_stage_errors: read failed");
+    return v;
 }
 
 static std::atomic<unsigned long long> g_batch_bin_attr{0};     // one bit per device
@@ -562,6 +676,7 @@ extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int m
     a.out_flags = out_flags; a.xyz = xyz;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
     a.perm = nullptr; a.stage = nullptr;
+    a.err = plan->counter + 1;            // the word after the queue counter (sticky)
     int rc = AGB_OK;
     const int* dest = nullptr;
     if (workspace && plan->n_bins > 0 && !(out_flags & AGB_OUT_NO_BINNING)) {

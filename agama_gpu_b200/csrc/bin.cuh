@@ -34,6 +34,7 @@ struct BinKey {
     // one block-sized window at a time, which L2 holds and merges, instead of
     // scattering partial-sector writes over the whole output array.
     int log_block;
+    int comp;                     // batches: the keyed leaf's component (-1: none)
 };
 
 // in-grid interval k in [0, n_int), n_int for the inner region (and the

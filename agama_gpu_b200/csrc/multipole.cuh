@@ -231,17 +231,20 @@ template <> struct MPPtr<double> {
     {
         return c.table + (long long)k * c.n_lm * 6;
     }
+    template <bool GEN = false>
     static __device__ __forceinline__ void load(const double* p, double a[6])
     {
         const double2* q = reinterpret_cast<const double2*>(p);
-        const double2 v0 = __ldg(q), v1 = __ldg(q + 1), v2 = __ldg(q + 2);
+        const double2 v0 = GEN ? q[0] : __ldg(q), v1 = GEN ? q[1] : __ldg(q + 1),
+                      v2 = GEN ? q[2] : __ldg(q + 2);
         a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y; a[4] = v2.x; a[5] = v2.y;
     }
     // the cos and sin records of an m>0 harmonic (consecutive columns)
+    template <bool GEN = false>
     static __device__ __forceinline__ void load_cs(const double* p, double c[6], double s[6])
     {
-        load(p, c);
-        load(p + REC, s);
+        load<GEN>(p, c);
+        load<GEN>(p + REC, s);
     }
 };
 template <> struct MPPtr<float> {
@@ -250,18 +253,23 @@ template <> struct MPPtr<float> {
     {
         return c.table32 + (long long)k * c.n_lm * 8;
     }
+    // GEN: p may point to shared memory (a staged slab): generic loads, not __ldg
+    template <bool GEN = false>
+    static __device__ __forceinline__ float4 ld4(const float4* q) { return GEN ? *q : __ldg(q); }
+    template <bool GEN = false>
     static __device__ __forceinline__ void load(const float* p, float a[6])
     {
         const float4* q = reinterpret_cast<const float4*>(p);
-        const float4 v0 = __ldg(q), v1 = __ldg(q + 1);
+        const float4 v0 = ld4<GEN>(q), v1 = ld4<GEN>(q + 1);
         a[0] = v0.x; a[1] = v0.y; a[2] = v0.z; a[3] = v0.w; a[4] = v1.x; a[5] = v1.y;
     }
     // an m>0 harmonic's cos and sin records, stored interleaved in the FP32
     // table of a regular structure: c0 s0 c1 s1 ... c5 s5 (+4 pads)
+    template <bool GEN = false>
     static __device__ __forceinline__ void load_cs(const float* p, float c[6], float s[6])
     {
         const float4* q = reinterpret_cast<const float4*>(p);
-        const float4 v0 = __ldg(q), v1 = __ldg(q + 1), v2 = __ldg(q + 2);
+        const float4 v0 = ld4<GEN>(q), v1 = ld4<GEN>(q + 1), v2 = ld4<GEN>(q + 2);
         c[0] = v0.x; s[0] = v0.y; c[1] = v0.z; s[1] = v0.w;
         c[2] = v1.x; s[2] = v1.y; c[3] = v1.z; s[3] = v1.w;
         c[4] = v2.x; s[4] = v2.y; c[5] = v2.z; s[5] = v2.w;
@@ -329,10 +337,13 @@ __device__ __forceinline__ void mp_col_finish(MPCol<R>& g, R inv_sth, R q1, R np
         g.VRR *= R(2);                                          // the FP32 walk sums C''/2
 }
 
-template <int MODE, typename R, int PAR>
+// GEN: the interval's records come from `slab` (this interval's row of a staged
+// copy of the FP32 table, possibly in shared memory) instead of the table itself
+template <int MODE, typename R, int PAR, bool GEN = false>
 __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double s_d,
                                                  double cth_d, double sth_d,
-                                                 double cph, double sph, MPSums& tot)
+                                                 double cph, double sph, MPSums& tot,
+                                                 const R* slab = nullptr)
 {
     constexpr bool NEED_ANG = MODE == AGB_MODE_GRAD || MODE == AGB_MODE_HESS;
     constexpr bool NEED_ANG2 = MODE == AGB_MODE_HESS;
@@ -348,7 +359,8 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
     const R cot = near_pole ? R(0) : (R)(cth_d / sth_d);
     const R np1 = near_pole ? R(0) : R(1);
     const int lmax = c.lmax;
-    const R* rec = MPPtr<R>::base(c, k) + MPPtr<R>::REC;       // column 1 (column 0 = monopole)
+    // column 1 (column 0 = monopole)
+    const R* rec = (GEN ? slab : MPPtr<R>::base(c, k)) + MPPtr<R>::REC;
 
     double cm = 1.0, sm = 0.0, sinpow = 1.0, sinpow_m1 = 0.0;
     for (int m = 0; m <= lmax; ++m) {
@@ -389,8 +401,8 @@ __device__ __forceinline__ void mp_harmonics_reg(const DevComp& c, int k, double
         // the loads of a loop body issue together (no branch inside the body)
         auto acc = [&](int L, auto has_sin) {
             R ac[6], as[6];
-            if (has_sin) MPPtr<R>::load_cs(rec, ac, as);
-            else MPPtr<R>::load(rec, ac);
+            if (has_sin) MPPtr<R>::template load_cs<GEN>(rec, ac, as);
+            else MPPtr<R>::template load<GEN>(rec, ac);
             rec += has_sin ? 2 * MPPtr<R>::REC : MPPtr<R>::REC;
             const R ll1 = R(L * (L + 1));
             mp_col_acc<MODE, R>(gc, ac, sp, dw, ew, Pc, dPc, ll1);
@@ -714,9 +726,14 @@ __device__ __forceinline__ void mp_finish(const MPSums& t, double inv_dlogr, dou
     }
 }
 
-template <int MODE, typename R>
+// STAGED: the records of intervals [k0, k1] are also in `slab` (a staged copy of
+// those rows of the FP32 table, in shared memory): a point in that range reads them
+// there (FP32 walks of regular structures; other points read the table)
+template <int MODE, typename R, bool STAGED = false>
 __device__ __forceinline__ void multipole_point(const DevComp& c, double px, double py,
-                                                double pz, PointOut& o)
+                                                double pz, PointOut& o,
+                                                const float* slab = nullptr, int k0 = 0,
+                                                int k1 = -1)
 {
     const double logr_min = c.p[0], dlogr = c.p[1], inv_dlogr = c.p[2], invPhi0 = c.p[3];
     const double in_s = c.p[4], in_U = c.p[5], in_W = c.p[6];
@@ -772,12 +789,25 @@ __device__ __forceinline__ void multipole_point(const DevComp& c, double px, dou
     const double sph = (Rc > 1.0e-300) ? py / Rc : 0.0;
 
     MPSums t = {};
-    if (c.structure == AGB_STRUCT_EVEN)
-        mp_harmonics_reg<MODE, R, 2>(c, k, s, cth, sth, cph, sph, t);
-    else if (c.structure == AGB_STRUCT_ALL)
-        mp_harmonics_reg<MODE, R, 1>(c, k, s, cth, sth, cph, sph, t);
-    else
-        mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
+    bool staged = false;
+    if constexpr (STAGED && std::is_same<R, float>::value) {
+        if (k >= k0 && k <= k1 && c.structure != AGB_STRUCT_LIST) {
+            const float* row = slab + (long long)(k - k0) * c.n_lm * 8;
+            if (c.structure == AGB_STRUCT_EVEN)
+                mp_harmonics_reg<MODE, R, 2, true>(c, k, s, cth, sth, cph, sph, t, row);
+            else
+                mp_harmonics_reg<MODE, R, 1, true>(c, k, s, cth, sth, cph, sph, t, row);
+            staged = true;
+        }
+    }
+    if (!staged) {
+        if (c.structure == AGB_STRUCT_EVEN)
+            mp_harmonics_reg<MODE, R, 2>(c, k, s, cth, sth, cph, sph, t);
+        else if (c.structure == AGB_STRUCT_ALL)
+            mp_harmonics_reg<MODE, R, 1>(c, k, s, cth, sth, cph, sph, t);
+        else
+            mp_harmonics<MODE, R>(c, k, s, cth, sth, cph, sph, t);
+    }
 
     // monopole (FP64) and the log-scaling factor F(log r) with derivatives, after the
     // walk so that its values are not live across it (FP64 kernel 7.22 -> 6.96 ms)

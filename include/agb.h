@@ -59,6 +59,10 @@ extern "C" {
 #define AGB_OUT_NEGATE     1   /* write -grad (force) and -Hessian (forceDeriv layout) */
 #define AGB_OUT_NO_BINNING 2   /* evaluate the points in input order (no scratch memory) */
 #define AGB_OUT_BIN_ALWAYS 4   /* sort by interval even below AGB_BIN_MIN_POINTS points */
+#define AGB_OUT_STAGE      32  /* batches (mixed precision, pre-sorted points): each
+                                  tile's interval rows of the unit's keyed Multipole are
+                                  bulk-copied (TMA, cp.async.bulk) into shared memory and
+                                  read there */
 /* Launch-shape knobs of the evaluation kernel.  Results do not depend on them;
    the autotuner (agama_gpu_b200/autotune.py) times them.  No counterpart in the
    reference, whose launch shape is fixed.
@@ -442,6 +446,10 @@ size_t  agb_batch_workspace_bytes(const agb_batch* plan, int mode);
  * aligned.  Results do not depend on the order.
  */
 size_t  agb_batch_sort_workspace_bytes(const agb_batch* plan);
+/* 1 when a staged launch (AGB_OUT_STAGE) of this plan gave up waiting for one of its
+   bulk copies and read global memory instead (results are unaffected); 0 otherwise;
+   -1 on error.  Synchronous. */
+int     agb_batch_stage_errors(const agb_batch* plan);
 int     agb_batch_sort(const agb_batch* plan, const double* xyz, int32_t* perm,
                        void* workspace, size_t workspace_bytes, void* stream);
 int     agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int mode,

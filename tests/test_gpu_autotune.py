@@ -60,6 +60,6 @@ def test_tune_batch_keeps_results():
     x = torch.from_numpy(hernquist_points(batch.n_points, 8.0, 5)).cuda()
     f0 = batch.force(x)
     res = autotune.tune_batch(batch, x, tiles=(256, 2048, 8192))
-    assert batch.tile_points == res["best"]
+    assert (batch.tile_points, batch.stage) == res["best"] and len(res["ms"]) == 6
     f1 = batch.force(x)
     assert float((f1 - f0).abs().max()) <= 1e-14 * float(f0.abs().max())

@@ -85,7 +85,7 @@ def test_batch_presort_equals_in_tile_sort(prec):
     from agama_gpu_b200 import _lib
     units, counts = _units()
     plain = agb.BatchedPotentialGPU(units, counts, tile_points=512, presort=False)
-    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512)
+    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512, stage=False)
     x = torch.from_numpy(_points(plain.n_points, 8)).cuda()
     pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
     plan = sorted_._plan(x.device, pc)
@@ -114,6 +114,41 @@ def test_batch_presort_equals_in_tile_sort(prec):
                                         _lib.OUT_NEGATE, ws.data_ptr(), small,
                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
         assert rc == -1 and "pre-sort" in _lib.last_error()
+
+
+@pytest.mark.parametrize("tile", [512, 4096])
+def test_batch_staged_slabs_equal_unstaged(tile):
+    """AGB_OUT_STAGE (each tile's interval rows of its unit's Multipole bulk-copied into
+    shared memory, mixed precision, pre-sorted points): the unstaged results to
+    rounding (the staged walk is its own instantiation, whose FP64 group sums may
+    contract differently); no wait gave up; an integrator's run (rows kept in order:
+    not staged) is unchanged.  Includes an lmax = 32 unit (18 KB per interval: the
+    slab is cut to what fits)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    units, counts = _units()
+    units = units + [agb.MultipolePotentialGPU(nfw_multipole(lmax=32, n_nodes=80, seed=3, amp=0.2))]
+    counts = np.concatenate([counts, [20000]])
+    plain = agb.BatchedPotentialGPU(units, counts, tile_points=tile, precision="mixed",
+                                    stage=False)
+    staged = agb.BatchedPotentialGPU(units, counts, tile_points=tile, precision="mixed", stage=True)
+    x = torch.from_numpy(_points(plain.n_points, 16)).cuda()
+    for mode in (0, 1, 2, 3):
+        want = plain._launch(x, 0.0, mode, True)
+        got = staged._launch(x, 0.0, mode, True)
+        for g, w in zip(got, want):
+            if w is not None:
+                err = float((g - w).abs().max()) / max(float(w.abs().max()), 1e-300)
+                assert err <= 1e-13, (tile, mode, err)
+    assert staged.stage_errors() == 0
+    v0 = torch.from_numpy(np.random.default_rng(17).normal(0, 50.0, (plain.n_points, 3))).cuda()
+    a = Leapfrog(staged, 0.002, graph_steps=4).run(x, v0, 8, checkpoint_every=8)
+    b = Leapfrog(plain, 0.002, graph_steps=4).run(x, v0, 8, checkpoint_every=8)
+    for p_, q_ in ((a[0], b[0]), (a[1], b[1])):
+        assert float((p_ - q_).abs().max()) <= 1e-11 * float(q_.abs().max())
+    assert staged.stage_errors() == 0
 
 
 def test_batch_many_small_units_and_two_calls():
@@ -169,7 +204,7 @@ def test_batch_leapfrog_in_sort_order_is_bit_equal():
     from agama_gpu_b200.integrate import Leapfrog
     units, counts = _units()
     rng = np.random.default_rng(14)
-    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512)
+    sorted_ = agb.BatchedPotentialGPU(units, counts, tile_points=512, stage=False)
     plain = agb.BatchedPotentialGPU(units, counts, tile_points=512, presort=False)
     n = sorted_.n_points
     x0 = torch.from_numpy(_points(n, 15)).cuda()
