@@ -507,6 +507,47 @@ def test_set_node_tables_on_device():
     assert float((gp - gp_ref).abs().max()) <= 1e-9 * float(gp_ref.abs().max())
 
 
+def test_set_node_tables_rebuilds_builder_scalars_and_recaptures_graphs():
+    """New l = 0 nodes change invPhi0 and the extrapolation fits: set_node_tables
+    recomputes them as the builder does (equal to a host-built object from the same
+    coefficients, inside and beyond the grid), and a leapfrog whose graph was captured
+    before the change captures it again (the kernels take the scalars by value)."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200.coefs import MultipoleCoefs
+    from agama_gpu_b200.integrate import Leapfrog
+    from agama_gpu_b200.synthetic import nfw_multipole
+    coefs = nfw_multipole(lmax=6, n_nodes=40, rmin=0.05, rmax=200.0, seed=31, amp=0.3)
+    mp = agb.MultipolePotentialGPU(coefs)
+    x0, v0 = _disk_ics(200, 32)
+    integ = Leapfrog(mp, 0.002, graph_steps=5)
+    xa, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)          # captures the graph
+    # scale the l = 0 column near the centre: the inner fit and invPhi0 move
+    phi2, dphi2 = np.array(coefs.phi), np.array(coefs.dphi_dr)
+    r = np.asarray(coefs.R_grid)
+    w = 1.0 + 0.05 * np.exp(-r / 2.0)
+    phi2[:, 0] *= w
+    dphi2[:, 0] = dphi2[:, 0] * w - coefs.phi[:, 0] * 0.05 * np.exp(-r / 2.0) / 2.0
+    ref = agb.MultipolePotentialGPU(MultipoleCoefs(coefs.R_grid, phi2, dphi2, coefs.lm_labels))
+    assert ref.tables.invPhi0 != mp.tables.invPhi0
+    mp.set_node_tables(torch.from_numpy(ref.tables.node_phi).cuda(),
+                       torch.from_numpy(ref.tables.node_dphi_dr).cuda())
+    # inside the grid and inside its first node (beyond the last one the builder's outer
+    # fit is degenerate -- s = -1 to rounding -- and amplifies the rounding of dPhi/dr
+    # through d/dlog r in the node table by ~1e16: the far fields of the two objects
+    # differ at the percent level, as two host builds from inputs one rounding apart do)
+    xyz = torch.from_numpy(_pts(4000, 33, 0.01, 150.0)).cuda()
+    for prec, tol in (("fp64", 1e-11), ("mixed", 2e-6)):
+        fm = mp._launch(xyz, 0.0, 1, True, precision=prec)
+        fr = ref._launch(xyz, 0.0, 1, True, precision=prec)
+        for a, b in zip(fm[:2], fr[:2]):
+            assert float((a - b).abs().max()) <= tol * float(b.abs().max()), prec
+    xb, _, _ = integ.run(x0, v0, 10, checkpoint_every=64)
+    xc, _, _ = Leapfrog(ref, 0.002, use_graph=False).run(x0, v0, 10, checkpoint_every=64)
+    assert not torch.equal(xa, xb)
+    assert float((xb - xc).abs().max()) <= 1e-11 * float(xc.abs().max())
+
+
 def test_yoshida4_order_in_composite():
     """Global position error in a Multipole + Miyamoto-Nagai composite falls as
     dt^4 for the 4th-order composition (and as dt^2 for leapfrog).  (A CylSpline
