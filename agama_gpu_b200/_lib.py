@@ -80,6 +80,7 @@ class AgbLeaf(ctypes.Structure):
 MAX_LEAF_OPS = 6
 OP_SHIFT, OP_SCALE, OP_EVOLVE = 1, 2, 3
 ADJ_DRIFT = 1
+ADJ_LV_COT = 2
 
 
 class AgbLeafProg(ctypes.Structure):
@@ -138,8 +139,8 @@ def _load():
         ctypes.POINTER(AgbComponent), ctypes.c_int, ctypes.POINTER(AgbLeaf), ctypes.c_int,
         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
-        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
-        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     lib.agb_multipole_adjoint.restype = ctypes.c_int
     lib.agb_multipole_adjoint.argtypes = [
         ctypes.POINTER(AgbComponent), ctypes.POINTER(AgbLeaf), ctypes.c_void_p, ctypes.c_int64,

@@ -1236,7 +1236,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
                                   const double* g_phi, const double* g_force, double* g_xyz,
                                   double* force, double* g_table, double* g_const,
                                   void* workspace, size_t workspace_bytes, void* stream,
-                                  AdjKeep* keep = nullptr)
+                                  AdjKeep* keep = nullptr, double g_force_scale = 1.0)
 {
     const bool keep_on = keep && keep->on;
     if (!comp || !leaf || !g_table || (!g_xyz && !keep_on))
@@ -1258,6 +1258,7 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
     g.leaf.g0 = leaf->gamma[0]; g.leaf.g1 = leaf->gamma[1]; g.leaf.g2 = leaf->gamma[2];
     g.n = n; g.xyz = xyz; g.perm = nullptr; g.gphi = g_phi; g.gforce = g_force;
     g.gx = g_xyz; g.grad = g_table; g.force = force; g.gconst = g_const;
+    g.gforce_scale = g_force_scale;
     cudaStream_t st = (cudaStream_t)stream;
     agb_leaf l = *leaf;
     l.comp = 0;
@@ -1347,22 +1348,42 @@ struct AdjStepPtrs {
     double* vh;          // [N,3] half-step velocities (DRIFT)
     double* lx;          // [N,3] adjoint of x
     double* lv;          // [N,3] adjoint of v
-    double* gF;          // [N,3] in: cotangent of F at x; out: c lv
+    double* gF;          // [N,3] in: cotangent of F at x; out: c lv (unless lv_cot)
     const int* dest;     // sorted position of point i
     const double* stage; // [pos][stage_rec] Multipole VJP (and force)
     long long n;
     int stage_rec;
     int drift;
-    double dt, c, k, dt_drift;
+    int lv_cot;          // the cotangent of F is c_in lv (lv on entry); gF unused
+    double dt, c, c_in, k, dt_drift;
 };
 
+// One thread per particle.  The staged record (read through its sorted
+// position) and lv are loaded before the analytic leaves' arithmetic, so the
+// latency of that gather overlaps the FP64 Hessian instead of following it.
 __global__ void __launch_bounds__(256, 2)
 adjoint_step_kernel(const __grid_constant__ EvalArgs a, const __grid_constant__ AdjStepPtrs p)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) {
+        const double* t = p.stage + (long long)p.stage_rec * __ldg(p.dest + i);
         const double x = p.x[3 * i], y = p.x[3 * i + 1], z = p.x[3 * i + 2];
-        const double f0 = p.gF[3 * i], f1 = p.gF[3 * i + 1], f2 = p.gF[3 * i + 2];
+        double lv0[3], tv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        #pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            lv0[q] = p.lv[3 * i + q];
+            tv[q] = __ldg(t + q);
+        }
+        if (p.drift) {
+            #pragma unroll
+            for (int q = 0; q < 3; ++q) tv[3 + q] = __ldg(t + 3 + q);
+        }
+        double f0, f1, f2;
+        if (p.lv_cot) {
+            f0 = p.c_in * lv0[0]; f1 = p.c_in * lv0[1]; f2 = p.c_in * lv0[2];
+        } else {
+            f0 = p.gF[3 * i]; f1 = p.gF[3 * i + 1]; f2 = p.gF[3 * i + 2];
+        }
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
         double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int L = 0; L < a.n_leaves; ++L) {
@@ -1382,27 +1403,27 @@ adjoint_step_kernel(const __grid_constant__ EvalArgs a, const __grid_constant__ 
         }
         // the analytic leaves' VJP (no potential cotangent) and force, as the VJP-force
         // mode of agb_eval_kernel writes them, then the Multipole part added
-        const double* t = p.stage + (long long)p.stage_rec * __ldg(p.dest + i);
         double gx[3], F[3];
         gx[0] = 0.0 * g0 - (h[0] * f0 + h[3] * f1 + h[5] * f2);
         gx[1] = 0.0 * g1 - (h[3] * f0 + h[1] * f1 + h[4] * f2);
         gx[2] = 0.0 * g2 - (h[5] * f0 + h[4] * f1 + h[2] * f2);
-        gx[0] += t[0]; gx[1] += t[1]; gx[2] += t[2];
+        gx[0] += tv[0]; gx[1] += tv[1]; gx[2] += tv[2];
         if (p.drift) {
-            F[0] = -g0 + t[3]; F[1] = -g1 + t[4]; F[2] = -g2 + t[5];
+            F[0] = -g0 + tv[3]; F[1] = -g1 + tv[4]; F[2] = -g2 + tv[5];
         }
+        const double pos[3] = {x, y, z};
         #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const long long j = 3 * i + q;
             const double lxq = p.lx[j] + gx[q];
-            const double lvq = fma(p.dt, lxq, p.lv[j]);
+            const double lvq = fma(p.dt, lxq, lv0[q]);
             p.lx[j] = lxq;
             p.lv[j] = lvq;
-            p.gF[j] = p.c * lvq;
+            if (!p.lv_cot) p.gF[j] = p.c * lvq;
             if (p.drift) {
                 const double v = fma(-p.k, F[q], p.vh[j]);
                 p.vh[j] = v;
-                p.x[j] = fma(-p.dt_drift, v, p.x[j]);
+                p.x[j] = fma(-p.dt_drift, v, pos[q]);
             }
         }
     }
@@ -1447,8 +1468,8 @@ extern "C" size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, i
 extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                                 int n_leaves, int mp_leaf, int precision, double* x, double* vh,
                                 double* lx, double* lv, double* gF, double* g_table,
-                                double* g_const, int64_t n, double dt, double c, double k,
-                                double dt_drift, int flags, void* workspace,
+                                double* g_const, int64_t n, double dt, double c, double c_in,
+                                double k, double dt_drift, int flags, void* workspace,
                                 size_t workspace_bytes, void* stream)
 {
     int rc = adjoint_step_check(comps, n_comps, leaves, n_leaves, mp_leaf);
@@ -1456,7 +1477,8 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
     if (n < 0) return set_err(AGB_ERR_ARG, "agb_adjoint_step: negative count");
     if (n == 0) return AGB_OK;
     const bool drift = (flags & AGB_ADJ_DRIFT) != 0;
-    if (!x || !lx || !lv || !gF || !g_table || (drift && !vh))
+    const bool lv_cot = (flags & AGB_ADJ_LV_COT) != 0;
+    if (!x || !lx || !lv || (!gF && !lv_cot) || !g_table || (drift && !vh))
         return set_err(AGB_ERR_ARG, "agb_adjoint_step: null array");
     AdjKeep keep;
     keep.on = true;
@@ -1464,8 +1486,9 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
     keep.dest = nullptr;
     keep.stage = nullptr;
     rc = multipole_adjoint_impl(&comps[leaves[mp_leaf].comp], &leaves[mp_leaf], x, n, precision,
-                                nullptr, gF, nullptr, nullptr, g_table, g_const, workspace,
-                                workspace_bytes, stream, &keep);
+                                nullptr, lv_cot ? lv : gF, nullptr, nullptr, g_table, g_const,
+                                workspace, workspace_bytes, stream, &keep,
+                                lv_cot ? c_in : 1.0);
     if (rc) return rc;
     static thread_local EvalArgs a;
     memset(&a, 0, sizeof(a));
@@ -1493,8 +1516,8 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
     AdjStepPtrs q;
     q.x = x; q.vh = vh; q.lx = lx; q.lv = lv; q.gF = gF;
     q.dest = keep.dest; q.stage = keep.stage;
-    q.n = n; q.stage_rec = drift ? 6 : 3; q.drift = drift ? 1 : 0;
-    q.dt = dt; q.c = c; q.k = k; q.dt_drift = dt_drift;
+    q.n = n; q.stage_rec = drift ? 6 : 3; q.drift = drift ? 1 : 0; q.lv_cot = lv_cot ? 1 : 0;
+    q.dt = dt; q.c = c; q.c_in = c_in; q.k = k; q.dt_drift = dt_drift;
     adjoint_step_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(a, q);
     return check_launch("adjoint_step_kernel");
 }

@@ -406,6 +406,7 @@ struct MPAdjArgs {
                               // values to add, gathered back by adj_unpermute_add
     int stage_rec;            // 3, or 6 with the force
     double* gconst;           // [AGB_MP_NCONST] or null, accumulated
+    double gforce_scale;      // the force cotangent is gforce_scale * gforce
     DevComp c;
     DevLeaf leaf;
 };
@@ -706,7 +707,10 @@ mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
             py = sg * a.xyz[3 * pos + 1] - a.leaf.g1;
             pz = sg * a.xyz[3 * pos + 2] - a.leaf.g2;
             gp = a.gphi ? a.gphi[i] : 0.0;
-            if (a.gforce) { gf0 = a.gforce[3 * i]; gf1 = a.gforce[3 * i + 1]; gf2 = a.gforce[3 * i + 2]; }
+            if (a.gforce) {
+                const double sc = a.gforce_scale;
+                gf0 = sc * a.gforce[3 * i]; gf1 = sc * a.gforce[3 * i + 1]; gf2 = sc * a.gforce[3 * i + 2];
+            }
         }
         const double r2 = px * px + py * py + pz * pz;
         const double r = sqrt(r2);

@@ -424,10 +424,20 @@ class Leapfrog:
         starts = sorted(c[0] for c in ckpts if c[0] < G)
         bounds = starts + [G]
         # gF: cotangent of F(x_{g+1}) -- h_g lv from substep g's second half-kick plus
-        # h_{g+1} lv from substep g+1's first one, both with the same lv
+        # h_{g+1} lv from substep g+1's first one, both with the same lv.  The fused
+        # steps take it as cot[0] lv without reading or writing gF (cot[1]: gF is
+        # behind), and gF is formed from lv only where an unfused launch reads it
         gF = lv * self._sub[(G - 1) % S][1] if G > 0 else None
+        cot = [self._sub[(G - 1) % S][1] if G > 0 else 0.0, False]
+
+        def gF_now():
+            if cot[1]:
+                torch.mul(lv, cot[0], out=gF)
+                cot[1] = False
+            return gF
 
         def vjp(xg, t, g_force, force=None):
+            g_force = gF_now()
             kw = {} if force is None else {"force_out": force}
             if tg is None:
                 self.pot._vjp(xg, t, None, g_force, precision=self.precision, out=gx, **kw)
@@ -441,6 +451,7 @@ class Leapfrog:
             """lx += gx; lv += dt_g lx; gF = (h_g + h_{g-1}) lv (h_0 lv after substep 0)."""
             dtg, hg, _ = self._sub[g % S]
             c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
+            cot[0] = c
             if on_gpu:          # one launch (agb_adjoint_kick)
                 rc = _lib.lib.agb_adjoint_kick(lx.data_ptr(), lv.data_ptr(), gx.data_ptr(),
                                                gF.data_ptr(), lx.shape[0], dtg, c,
@@ -472,8 +483,13 @@ class Leapfrog:
                 return False
             dtg, hg, _ = self._sub[g % S]
             c = hg + (self._sub[(g - 1) % S][1] if g > 0 else 0.0)
-            return self.pot._adjoint_step(xg, self._t(g + 1), gF, tg, lx, lv, dtg, c, vh=vh_,
-                                          k=k_, dt_drift=dtg, precision=self.precision)
+            if not self.pot._adjoint_step(xg, self._t(g + 1), None, tg, lx, lv, dtg, c, vh=vh_,
+                                          k=k_, dt_drift=dtg, precision=self.precision,
+                                          c_in=cot[0]):
+                return False
+            cot[0] = c
+            cot[1] = True
+            return True
 
         for seg in range(len(starts) - 1, -1, -1):
             s, e = bounds[seg], bounds[seg + 1]
@@ -530,7 +546,7 @@ class Leapfrog:
                 kick(g)
         if G > 0:
             _, x0, _ = at[0]
-            vjp(x0, self.t0, gF)
+            vjp(x0, self.t0, None)
             lx.add_(gx)
         if tg is not None:
             return lx, lv, allreduce_table_grads(self.pot._table_grads_from_device(tg), group)

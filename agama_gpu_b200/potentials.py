@@ -566,16 +566,18 @@ class _GPUPotBase:
                 _lib.check(rc, "agb_multipole_adjoint_force")
         return gx
 
-    def _adjoint_step(self, arr: torch.Tensor, t: float, gF: torch.Tensor, acc_dev: dict,
-                      lx: torch.Tensor, lv: torch.Tensor, dt: float, c: float,
+    def _adjoint_step(self, arr: torch.Tensor, t: float, gF: Optional[torch.Tensor],
+                      acc_dev: dict, lx: torch.Tensor, lv: torch.Tensor, dt: float, c: float,
                       vh: Optional[torch.Tensor] = None, k: float = 0.0, dt_drift: float = 0.0,
-                      precision: Optional[str] = None) -> bool:
+                      precision: Optional[str] = None, c_in: Optional[float] = None) -> bool:
         """One backward leapfrog step in two launches (agb_adjoint_step): the VJP of the
         tree at arr with cotangent gF of the force, the coefficient gradient of its
         Multipole added into ``acc_dev`` (device layout, as ``_adjoint_vjp``), the kick
         lx += gx, lv = fma(dt, lx, lv), gF = c lv, and with ``vh`` the reverse drift
-        vh -= k F(arr), arr -= dt_drift vh, in place.  Returns False (nothing done) when
-        the tree at t is not one regular-structure Multipole plus analytic leaves."""
+        vh -= k F(arr), arr -= dt_drift vh, in place.  With ``c_in`` the cotangent of the
+        force is c_in lv (lv on entry) and gF is neither read nor written.  Returns False
+        (nothing done) when the tree at t is not one regular-structure Multipole plus
+        analytic leaves."""
         leaves = self._leaves(float(t))
         mp = [i for i, lf in enumerate(leaves) if lf[0].kind == _lib.KIND_MULTIPOLE]
         if len(mp) != 1 or any(lf[0].kind == _lib.KIND_CYLSPLINE for lf in leaves):
@@ -587,7 +589,8 @@ class _GPUPotBase:
         dev = arr.device
         prec = _PRECISIONS[precision or self.precision or _default_precision]
         cargs = self._c_args(t, dev, leaves)
-        flags = _lib.ADJ_DRIFT if vh is not None else 0
+        flags = (_lib.ADJ_DRIFT if vh is not None else 0) | \
+            (_lib.ADJ_LV_COT if c_in is not None else 0)
         nws = int(_lib.lib.agb_adjoint_step_workspace_bytes(*cargs, mp[0], n, flags))
         if nws == 0:
             return False
@@ -600,8 +603,10 @@ class _GPUPotBase:
         cg = _const_buffer(acc_dev, comp, dev)
         rc = _lib.lib.agb_adjoint_step(
             *cargs, mp[0], prec, arr.data_ptr(), None if vh is None else vh.data_ptr(),
-            lx.data_ptr(), lv.data_ptr(), gF.data_ptr(), buf.data_ptr(), cg.data_ptr(), n,
-            float(dt), float(c), float(k), float(dt_drift), flags, ws.data_ptr(), nws,
+            lx.data_ptr(), lv.data_ptr(), None if c_in is not None else gF.data_ptr(),
+            buf.data_ptr(), cg.data_ptr(), n, float(dt), float(c),
+            float(c_in) if c_in is not None else 0.0, float(k), float(dt_drift), flags,
+            ws.data_ptr(), nws,
             ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
         _lib.check(rc, "agb_adjoint_step")
         return True

@@ -329,7 +329,10 @@ int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
  *     lx += gx;  lv = fma(dt, lx, lv);  gF = c lv                    (the kick)
  * and with flags & AGB_ADJ_DRIFT the time-reversed drift with the total force
  *     vh = fma(-k, F, vh);  x = fma(-dt_drift, vh, x).
- * gF is read as the cotangent of the force at x and overwritten with c lv.
+ * gF is read as the cotangent of the force at x and overwritten with c lv;
+ * with flags & AGB_ADJ_LV_COT the cotangent is c_in lv (lv as it is on entry:
+ * the c lv of the previous step) and gF is neither read nor written (it may
+ * be null), which saves one [N,3] array's read and write per step.
  * The same arithmetic, in the same order, as agb_eval_vjp_force (analytic
  * leaves) + agb_multipole_adjoint_force + agb_adjoint_kick + agb_reverse_drift,
  * with two launches fewer and no intermediate gx / F arrays.  The workspace
@@ -337,14 +340,15 @@ int agb_multipole_adjoint_force(const agb_component* comp, const agb_leaf* leaf,
  * counterpart in the reference.
  */
 #define AGB_ADJ_DRIFT 1
+#define AGB_ADJ_LV_COT 2
 size_t agb_adjoint_step_workspace_bytes(const agb_component* comps, int n_comps,
                                         const agb_leaf* leaves, int n_leaves, int mp_leaf,
                                         int64_t n, int flags);
 int agb_adjoint_step(const agb_component* comps, int n_comps, const agb_leaf* leaves,
                      int n_leaves, int mp_leaf, int precision, double* x, double* vh,
                      double* lx, double* lv, double* gF, double* g_table, double* g_const,
-                     int64_t n, double dt, double c, double k, double dt_drift, int flags,
-                     void* workspace, size_t workspace_bytes, void* stream);
+                     int64_t n, double dt, double c, double c_in, double k, double dt_drift,
+                     int flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Leapfrog adjoint, per-step vector updates on [N,3] device arrays (one launch each):

@@ -71,6 +71,23 @@ def test_argument_errors_need_no_gpu():
     leaves[0].comp = 3
     assert _lib.lib.agb_eval_wave_points(comps, 1, leaves, 1, 1, 0) == 0
     leaves[0].comp = 0
+    # the backward leapfrog step: gF may be null only when the force cotangent comes
+    # from lv (AGB_ADJ_LV_COT); both checks happen before any CUDA call
+    mp2 = (_lib.AgbComponent * 2)()
+    mp2[0].kind = _lib.KIND_MULTIPOLE
+    mp2[1].kind = _lib.KIND_NFW
+    lv2 = (_lib.AgbLeaf * 2)()
+    lv2[1].comp = 1
+    P = ctypes.c_void_p(16)
+    rc = _lib.lib.agb_adjoint_step(mp2, 2, lv2, 2, 0, 1, P, None, P, P, None, P, None, 10,
+                                   0.1, 0.2, 0.2, 0.0, 0.0, 0, None, 0, None)
+    assert rc == -1 and "null array" in _lib.last_error()
+    rc = _lib.lib.agb_adjoint_step(mp2, 2, lv2, 2, 0, 1, P, None, P, P, None, None, None, 10,
+                                   0.1, 0.2, 0.2, 0.0, 0.0, _lib.ADJ_LV_COT, None, 0, None)
+    assert rc == -1 and "null array" in _lib.last_error()          # g_table is null
+    rc = _lib.lib.agb_adjoint_step(mp2, 2, lv2, 2, 1, 1, P, None, P, P, None, P, None, 10,
+                                   0.1, 0.2, 0.2, 0.0, 0.0, _lib.ADJ_LV_COT, None, 0, None)
+    assert rc == -3 and "must be analytic" in _lib.last_error()
     # lmax beyond the kernel's limit
     comps[0].kind = _lib.KIND_MULTIPOLE
     comps[0].lmax = 40
