@@ -750,50 +750,71 @@ class _GPUPotBase:
             return self._eval_host_run(src, host, want, n, chunk, t, mode, pot, dev, pipe)
 
     def _eval_host_run(self, src, host, want, n, chunk, t, mode, pot, dev, pipe):
-        # everything the launches need is prepared before the first copy is queued (the
-        # tree's arguments at t once, one workspace for the largest chunk), so each chunk
-        # costs the host one C call and the first kernel follows its copy directly
+        # The chunk layout, launch flags and workspace size depend only on the call's
+        # shape, so they are kept per shape on the object; the first chunk's copy-in is
+        # queued before the tree's arguments at t are formed (the host's remaining work
+        # before the first launch), so that copy overlaps it.  Each chunk then costs the
+        # host one C call and the first kernel follows its copy directly.
         prec = _PRECISIONS[self.precision or _default_precision]
-        cargs = self._c_args(t, dev)
-        wave = int(_lib.lib.agb_eval_wave_points(cargs[0], cargs[1], cargs[2], cargs[3], mode,
-                                                 prec))
-        bounds = _chunk_bounds(n, chunk, wave)
-        sizes = sorted({hi - lo for lo, hi in bounds})
-        chunk = max(sizes)                 # the device buffers hold the largest chunk
-        flags = {m: self._flags(mode, prec, m) for m in sizes}
-        if wave and len(bounds) > 2 and all((hi - lo) % wave == 0 for lo, hi in bounds[:-1]):
-            # chunks in whole waves: one resident block per slot, so every thread of
-            # a launch takes the same number of passes (unless a tuned shape is set)
-            flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 or (f >> _lib.OUT_PPT_SHIFT) & 15
-                     else f | (1 << _lib.OUT_GRID_SHIFT) for m, f in flags.items()}
-        nws = max((int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2], cargs[3],
-                                                         m, flags[m])) for m in sizes), default=0)
+        tuned = self.__dict__.get("_tuned") or {}
+        key = (dev.index, mode, prec, n, chunk, self.binning, tuple(sorted(tuned.items())))
+        plans = self.__dict__.setdefault("_host_plans", {})
+        plan = plans.get(key)
+        cargs = None
+        if plan is None:
+            cargs = self._c_args(t, dev)
+            wave = int(_lib.lib.agb_eval_wave_points(cargs[0], cargs[1], cargs[2], cargs[3],
+                                                     mode, prec))
+            bounds = _chunk_bounds(n, chunk, wave)
+            sizes = sorted({hi - lo for lo, hi in bounds})
+            flags = {m: self._flags(mode, prec, m) for m in sizes}
+            if wave and len(bounds) > 2 and all((hi - lo) % wave == 0 for lo, hi in bounds[:-1]):
+                # chunks in whole waves: one resident block per slot, so every thread of
+                # a launch takes the same number of passes (unless a tuned shape is set)
+                flags = {m: f if (f >> _lib.OUT_GRID_SHIFT) & 15 or (f >> _lib.OUT_PPT_SHIFT) & 15
+                         else f | (1 << _lib.OUT_GRID_SHIFT) for m, f in flags.items()}
+            nws = max((int(_lib.lib.agb_eval_workspace_bytes(cargs[0], cargs[1], cargs[2],
+                                                             cargs[3], m, flags[m]))
+                       for m in sizes), default=0)
+            # the device buffers hold the largest chunk
+            plan = (bounds, max(sizes), flags, nws)
+            if len(plans) >= 64:
+                plans.clear()
+            plans[key] = plan
+        bounds, chunk, flags, nws = plan
         ptr = lambda a: None if a is None else a.data_ptr()  # noqa: E731
         cur = torch.cuda.current_stream(dev)
         s_in, s_cmp, s_out = pipe["streams"]
+        for s in (s_in, s_cmp, s_out):
+            s.wait_stream(cur)
+        xb = pipe_buffers(pipe, dev, ("x", chunk), (chunk, 3))
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        lo0, hi0 = bounds[0]
+        with torch.cuda.stream(s_in):
+            xb[0][:hi0 - lo0].copy_(src[lo0:hi0], non_blocking=True)
+            ev_in[0].record(s_in)
+        if cargs is None:
+            cargs = self._c_args(t, dev)
         ws = pipe["bufs"].get("ws")
         if nws and (ws is None or ws.numel() < nws):
             # allocated on the compute stream, the only one that uses it
             with torch.cuda.device(dev), torch.cuda.stream(s_cmp):
                 ws = torch.empty(nws, dtype=torch.uint8, device=dev)
             pipe["bufs"]["ws"] = ws
-        for s in (s_in, s_cmp, s_out):
-            s.wait_stream(cur)
-        xb = pipe_buffers(pipe, dev, ("x", chunk), (chunk, 3))
         ob = [[pipe_buffers(pipe, dev, (k, chunk), (chunk,) + shape[1:])[j] if w else None
                for w, shape, k in want] for j in range(2)]
-        ev_in = [torch.cuda.Event() for _ in range(2)]
         ev_cmp = [torch.cuda.Event() for _ in range(2)]
         ev_out = [torch.cuda.Event() for _ in range(2)]
         started = [False, False]
         for i, (lo, hi) in enumerate(bounds):
             b = i & 1
             m = hi - lo
-            with torch.cuda.stream(s_in):
-                if started[b]:
-                    s_in.wait_event(ev_cmp[b])          # the kernel is done with xb[b]
-                xb[b][:m].copy_(src[lo:hi], non_blocking=True)
-                ev_in[b].record(s_in)
+            if i > 0:                                   # chunk 0 is on its way already
+                with torch.cuda.stream(s_in):
+                    if started[b]:
+                        s_in.wait_event(ev_cmp[b])      # the kernel is done with xb[b]
+                    xb[b][:m].copy_(src[lo:hi], non_blocking=True)
+                    ev_in[b].record(s_in)
             with torch.cuda.stream(s_cmp):
                 s_cmp.wait_event(ev_in[b])
                 if started[b]:
