@@ -18,6 +18,7 @@ OUT_NEGATE = 1
 OUT_NO_BINNING = 2
 OUT_BIN_ALWAYS = 4
 OUT_STAGE = 32
+OUT_STAGE_GIVE_UP = 1 << 24
 OUT_GRID_SHIFT = 8
 OUT_BLOCK_SHIFT = 12
 OUT_PPT_SHIFT = 16

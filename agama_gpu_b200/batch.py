@@ -65,6 +65,8 @@ class BatchedPotentialGPU(_GPUPotBase):
         # set by the integrators while they keep the particles in sort_order(): the
         # rows are then evaluated in order (no pre-sort, no in-tile sort)
         self._rows_in_order = False
+        # AGB_OUT_STAGE_GIVE_UP in tests of the bounded waits' failure path (else 0)
+        self._stage_test_flags = 0
         self._plans = {}
         self._ws = {}
 
@@ -142,7 +144,7 @@ class BatchedPotentialGPU(_GPUPotBase):
         ws, nws = None, 0
         flags = _lib.OUT_NEGATE | (_lib.OUT_NO_BINNING if self._rows_in_order else 0)
         if self.stage:
-            flags |= _lib.OUT_STAGE
+            flags |= _lib.OUT_STAGE | self._stage_test_flags
         if self.presort and not self._rows_in_order:
             nws = int(_lib.lib.agb_batch_workspace_bytes(plan, mode))
             if nws:

@@ -118,7 +118,10 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         __syncthreads();                  // every thread has read s_tile before it changes
         if (t >= a.n_tiles) return;       // (no copy is issued for t >= n_tiles)
         if (ST && k1 >= k0) {
-            const bool ok = mbar_wait_bounded(&s_bar, phase, AGB_BATCH_STAGE_TRIES);
+            // AGB_OUT_STAGE_GIVE_UP (tests of this path): give up at the first poll
+            const bool ok = mbar_wait_bounded(&s_bar, phase,
+                                              (a.out_flags & AGB_OUT_STAGE_GIVE_UP)
+                                                  ? 0 : AGB_BATCH_STAGE_TRIES);
             phase ^= 1u;
             if (__syncthreads_or(!ok)) {  // gave up: read global memory from here on
                 k1 = k0 - 1;

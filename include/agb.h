@@ -63,6 +63,12 @@ extern "C" {
                                   tile's interval rows of the unit's keyed Multipole are
                                   bulk-copied (TMA, cp.async.bulk) into shared memory and
                                   read there */
+/* batches with AGB_OUT_STAGE, for tests of the failure path of the bounded
+   waits: every block gives up its first wait for a bulk copy at once, records the
+   error (agb_batch_stage_errors then returns 1), waits for that copy to land
+   (bounded) and reads global memory from then on: the results are those of the
+   unstaged kernel */
+#define AGB_OUT_STAGE_GIVE_UP (1 << 24)
 /* Launch-shape knobs of the evaluation kernel.  Results do not depend on them;
    the autotuner (agama_gpu_b200/autotune.py) times them.  No counterpart in the
    reference, whose launch shape is fixed.

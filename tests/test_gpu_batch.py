@@ -151,6 +151,37 @@ def test_batch_staged_slabs_equal_unstaged(tile):
     assert staged.stage_errors() == 0
 
 
+def test_batch_staging_wait_that_gives_up_is_reported():
+    """The failure path of the bounded bulk-copy waits, without a fault: with
+    AGB_OUT_STAGE_GIVE_UP every block gives up its first wait at once, waits (bounded)
+    for that copy to land and reads global memory from then on.  The results are the
+    unstaged kernel's, agb_batch_stage_errors reports the give-up (sticky), and the
+    context stays usable for the next launches."""
+    import torch
+    import agama_gpu_b200 as agb
+    from agama_gpu_b200 import _lib
+    units, counts = _units()
+    plain = agb.BatchedPotentialGPU(units, counts, precision="mixed", stage=False)
+    staged = agb.BatchedPotentialGPU(units, counts, precision="mixed", stage=True)
+    x = torch.from_numpy(_points(plain.n_points, 21)).cuda()
+    want = plain._launch(x, 0.0, 1, True)
+    got = staged._launch(x, 0.0, 1, True)
+    assert staged.stage_errors() == 0
+    staged._stage_test_flags = _lib.OUT_STAGE_GIVE_UP
+    gave_up = staged._launch(x, 0.0, 1, True)
+    torch.cuda.synchronize()
+    assert staged.stage_errors() == 1
+    staged._stage_test_flags = 0
+    again = staged._launch(x, 0.0, 1, True)
+    for g in (got, gave_up, again):
+        for a, w in zip(g, want):
+            if w is not None:
+                err = float((a - w).abs().max()) / max(float(w.abs().max()), 1e-300)
+                assert err <= 1e-13, err
+    assert staged.stage_errors() == 1          # sticky until the plan is rebuilt
+    assert plain.stage_errors() == 0
+
+
 def test_batch_many_small_units_and_two_calls():
     import torch
     import agama_gpu_b200 as agb
