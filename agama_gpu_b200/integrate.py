@@ -436,7 +436,8 @@ class Leapfrog:
                 cot[1] = False
             return gF
 
-        def vjp(xg, t, g_force, force=None):
+        def vjp(xg, t, force=None):
+            """gx = (dF/dx)^T gF at xg (and the table gradients), gF formed if behind."""
             g_force = gF_now()
             kw = {} if force is None else {"force_out": force}
             if tg is None:
@@ -513,7 +514,7 @@ class Leapfrog:
                             continue
                     elif fused(xc, g):
                         continue
-                    vjp(xc, self._t(g + 1), gF, Fg if need else None)
+                    vjp(xc, self._t(g + 1), Fg if need else None)
                     kick(g)
                     if need:
                         if vh is None:
@@ -542,11 +543,11 @@ class Leapfrog:
             for g in range(e - 1, s - 1, -1):
                 if fused(pos[g + 1], g):
                     continue
-                vjp(pos[g + 1], self._t(g + 1), gF)
+                vjp(pos[g + 1], self._t(g + 1))
                 kick(g)
         if G > 0:
             _, x0, _ = at[0]
-            vjp(x0, self.t0, None)
+            vjp(x0, self.t0)
             lx.add_(gx)
         if tg is not None:
             return lx, lv, allreduce_table_grads(self.pot._table_grads_from_device(tg), group)
