@@ -46,6 +46,7 @@ struct BatchArgs {
     int n_tiles;
     int out_flags;
     const double* xyz;        // presorted: the sorted copy of the points
+    int xstride;              // doubles per point in xyz: 3 (the caller's), 4 (sorted copy)
     double* phi;
     double* grad;
     double* hess;
@@ -89,8 +90,10 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
                     if (kc && K.n_int > 0 && kc->kind == AGB_KIND_MULTIPOLE && kc->table32 &&
                         kc->structure != AGB_STRUCT_LIST && T.count > 0) {
                         const long long p0 = T.start, p1 = T.start + T.count - 1;
-                        const int b0 = bin_of(K, a.xyz[3 * p0], a.xyz[3 * p0 + 1], a.xyz[3 * p0 + 2]);
-                        const int b1 = bin_of(K, a.xyz[3 * p1], a.xyz[3 * p1 + 1], a.xyz[3 * p1 + 2]);
+                        const int b0 = bin_of(K, a.xyz[a.xstride * p0], a.xyz[a.xstride * p0 + 1],
+                                             a.xyz[a.xstride * p0 + 2]);
+                        const int b1 = bin_of(K, a.xyz[a.xstride * p1], a.xyz[a.xstride * p1 + 1],
+                                             a.xyz[a.xstride * p1 + 2]);
                         const long long row = 32LL * kc->n_lm;          // bytes per interval
                         if (b0 < K.n_int && row <= AGB_BATCH_STAGE_BYTES) {
                             k0 = b0;
@@ -146,7 +149,8 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
             __syncthreads();
             for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
                 const long long i = T.start + j;
-                const int k = bin_of(K, a.xyz[3 * i], a.xyz[3 * i + 1], a.xyz[3 * i + 2]);
+                const int k = bin_of(K, a.xyz[a.xstride * i], a.xyz[a.xstride * i + 1],
+                                    a.xyz[a.xstride * i + 2]);
                 s_key[j] = (unsigned short)k;
                 atomicAdd(&s_hist[k], 1);
             }
@@ -176,7 +180,13 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         for (int j = threadIdx.x; j < T.count; j += blockDim.x) {
             const long long pos = T.start + (sorted ? (int)s_order[j] : j);
             const long long i = a.perm ? (long long)__ldg(a.perm + pos) : pos;
-            const double x = a.xyz[3 * pos], y = a.xyz[3 * pos + 1], z = a.xyz[3 * pos + 2];
+            double x, y, z;
+            if (a.xstride == 4) {           // the sorted copy: one aligned 32-byte record
+                const double2 v = __ldg(reinterpret_cast<const double2*>(a.xyz + 4 * pos));
+                x = v.x; y = v.y; z = __ldg(a.xyz + 4 * pos + 2);
+            } else {
+                x = a.xyz[3 * pos]; y = a.xyz[3 * pos + 1]; z = a.xyz[3 * pos + 2];
+            }
             double phi = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, rho = 0.0;
             double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             for (int L = l0; L < l1; ++L) {
@@ -293,10 +303,10 @@ batch_bin_scatter(const BatchTile* __restrict__ tiles, const int* __restrict__ u
         const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
         perm[pos] = (int)i;
         keys[i] = (int)pos;
-        if (xs) {
-            xs[3 * pos] = xyz[3 * i];
-            xs[3 * pos + 1] = xyz[3 * i + 1];
-            xs[3 * pos + 2] = xyz[3 * i + 2];
+        if (xs) {          // 32-byte records: each write fills one whole sector
+            double2* o = reinterpret_cast<double2*>(xs + 4 * pos);
+            o[0] = make_double2(xyz[3 * i], xyz[3 * i + 1]);
+            o[1] = make_double2(xyz[3 * i + 2], 0.0);
         }
     }
 }
@@ -513,12 +523,12 @@ extern "C" void agb_batch_destroy(agb_batch* plan)
 }
 
 // Scratch of the pre-sort: keys and perm (4 B per point each), the sorted copy of
-// the points (24 B), the bin counters and cursors, then (optional) the sorted-order
-// output records.
+// the points (32-byte records: x, y, z, pad), the bin counters and cursors, then
+// (optional) the sorted-order output records.
 static size_t batch_ws_bytes(const agb_batch* p)
 {
     const size_t n = (size_t)p->n_points;
-    return 2 * al256(4 * n) + al256(24 * n) + 2 * al256(4 * (size_t)p->n_bins);
+    return 2 * al256(4 * n) + al256(32 * n) + 2 * al256(4 * (size_t)p->n_bins);
 }
 
 extern "C" size_t agb_batch_workspace_bytes(const agb_batch* plan, int mode)
@@ -609,10 +619,11 @@ static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchA
     int* keys = (int*)ws;
     int* perm = (int*)(ws + al256(4 * n));
     double* xs = (double*)(ws + 2 * al256(4 * n));
-    int* counts = (int*)(ws + 2 * al256(4 * n) + al256(24 * n));
+    int* counts = (int*)(ws + 2 * al256(4 * n) + al256(32 * n));
     const int rc = batch_sort(p, xyz, keys, perm, xs, counts, st);
     if (rc) return rc;
     a.xyz = xs;
+    a.xstride = 4;
     a.perm = perm;
     return AGB_OK;
 }
@@ -676,7 +687,7 @@ extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int m
     a.comps = plan->comps; a.leaves = plan->leaves; a.unit_leaf = plan->unit_leaf;
     a.tiles = plan->tiles; a.ukey = plan->ukey; a.counter = plan->counter;
     a.n_tiles = plan->n_tiles;
-    a.out_flags = out_flags; a.xyz = xyz;
+    a.out_flags = out_flags; a.xyz = xyz; a.xstride = 3;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
     a.perm = nullptr; a.stage = nullptr;
     a.err = plan->counter + 1;            // the word after the queue counter (sticky)
