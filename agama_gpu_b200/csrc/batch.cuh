@@ -47,6 +47,7 @@ struct BatchArgs {
     int out_flags;
     const double* xyz;        // presorted: the sorted copy of the points
     int xstride;              // doubles per point in xyz: 3 (the caller's), 4 (sorted copy)
+    int presorted;            // xyz is the sorted copy made by this call's pre-sort
     double* phi;
     double* grad;
     double* hess;
@@ -142,7 +143,7 @@ agb_batch_kernel(const __grid_constant__ BatchArgs a)
         const int nb = K.n_int + 2;
         // points pre-sorted by agb_batch_eval_ws: a tile is a run of sorted positions
         // (AGB_OUT_NO_BINNING: the caller keeps the rows in interval order itself)
-        const bool sorted = !a.perm && !(a.out_flags & AGB_OUT_NO_BINNING) && K.n_int >= 0 &&
+        const bool sorted = !a.presorted && !(a.out_flags & AGB_OUT_NO_BINNING) && K.n_int >= 0 &&
                             nb <= AGB_BATCH_MAX_BINS && T.count <= AGB_BATCH_SORT_MAX;
         if (sorted) {
             for (int q = threadIdx.x; q < nb; q += blockDim.x) s_hist[q] = 0;
@@ -301,7 +302,7 @@ batch_bin_scatter(const BatchTile* __restrict__ tiles, const int* __restrict__ u
         const long long i = T.start + j;
         const int k = keys[i];
         const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
-        perm[pos] = (int)i;
+        if (perm) perm[pos] = (int)i;
         keys[i] = (int)pos;
         if (xs) {          // 32-byte records: each write fills one whole sector
             double2* o = reinterpret_cast<double2*>(xs + 4 * pos);
@@ -547,7 +548,7 @@ static int launch_batch(const BatchArgs& a, cudaStream_t st)
     // in the order of its run's start drift apart along r: a tile's first and last
     // points then bound its intervals less well, and 100 config-4 leapfrog steps took
     // 1363 ms staged against 1307 ms unstaged.)
-    const bool stage = std::is_same<R, float>::value && (a.out_flags & AGB_OUT_STAGE) && a.perm;
+    const bool stage = std::is_same<R, float>::value && (a.out_flags & AGB_OUT_STAGE) && a.presorted;
     if (stage) {
         static std::atomic<int> cache_st[AGB_MAX_DEVICES];
         const int dev = current_device();
@@ -612,12 +613,14 @@ static int batch_sort(const agb_batch* p, const double* xyz, int* keys, int* per
     return check_launch("batch_bin_scatter");
 }
 
+// with_perm false: the outputs go through sorted-order records and keys (row ->
+// sorted position), so the permutation is not written
 static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchArgs& a,
-                         cudaStream_t st)
+                         bool with_perm, cudaStream_t st)
 {
     const size_t n = (size_t)p->n_points;
     int* keys = (int*)ws;
-    int* perm = (int*)(ws + al256(4 * n));
+    int* perm = with_perm ? (int*)(ws + al256(4 * n)) : nullptr;
     double* xs = (double*)(ws + 2 * al256(4 * n));
     int* counts = (int*)(ws + 2 * al256(4 * n) + al256(32 * n));
     const int rc = batch_sort(p, xyz, keys, perm, xs, counts, st);
@@ -625,6 +628,7 @@ static int batch_presort(const agb_batch* p, const double* xyz, char* ws, BatchA
     a.xyz = xs;
     a.xstride = 4;
     a.perm = perm;
+    a.presorted = 1;
     return AGB_OK;
 }
 
@@ -687,7 +691,7 @@ extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int m
     a.comps = plan->comps; a.leaves = plan->leaves; a.unit_leaf = plan->unit_leaf;
     a.tiles = plan->tiles; a.ukey = plan->ukey; a.counter = plan->counter;
     a.n_tiles = plan->n_tiles;
-    a.out_flags = out_flags; a.xyz = xyz; a.xstride = 3;
+    a.out_flags = out_flags; a.xyz = xyz; a.xstride = 3; a.presorted = 0;
     a.phi = phi; a.grad = grad; a.hess = hess; a.rho = rho;
     a.perm = nullptr; a.stage = nullptr;
     a.err = plan->counter + 1;            // the word after the queue counter (sticky)
@@ -699,8 +703,9 @@ extern "C" int agb_batch_eval_ws(const agb_batch* plan, const double* xyz, int m
             return set_err(AGB_ERR_ARG, "agb_batch_eval_ws: workspace of %zu bytes (256-byte "
                            "aligned) is smaller than the %zu bytes of the pre-sort",
                            workspace_bytes, need);
-        if ((rc = batch_presort(plan, xyz, (char*)workspace, a, st))) return rc;
-        if (workspace_bytes >= agb_batch_workspace_bytes(plan, mode)) {
+        const bool room = workspace_bytes >= agb_batch_workspace_bytes(plan, mode);
+        if ((rc = batch_presort(plan, xyz, (char*)workspace, a, !room, st))) return rc;
+        if (room) {
             a.stage = (double*)((char*)workspace + need);
             dest = (const int*)workspace;
         }
