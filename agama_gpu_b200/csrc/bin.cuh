@@ -121,7 +121,7 @@ bin_scatter(const double* __restrict__ xyz, long long n, int tile, int n_bins,
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const int k = keys[i];
         const long long pos = (long long)base[k] + atomicAdd(&hist[k], 1);
-        perm[pos] = (int)i;
+        if (perm) perm[pos] = (int)i;
         keys[i] = (int)pos;          // from here on: where point i went (the inverse of perm)
         xyz_sorted[3 * pos] = xyz[3 * i];
         xyz_sorted[3 * pos + 1] = xyz[3 * i + 1];

@@ -637,8 +637,11 @@ static int pack_args(EvalArgs& a, const agb_component* comps, int n_comps, const
 static std::atomic<unsigned long long> g_bin_attr_set{0};     // one bit per device
 
 // Sort the points by interval into the workspace; sets a.xyz / a.perm.
+// with_perm false: the caller needs no sorted position -> point map (outputs staged in
+// sorted order and gathered through the keys, no per-point cotangents to read), so
+// bin_scatter skips those 4-byte scattered writes and a.perm stays null
 static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t n, char* ws,
-                       cudaStream_t st)
+                       cudaStream_t st, bool with_perm = true)
 {
     int* keys = (int*)ws;
     int* perm = (int*)(ws + al256(4 * (size_t)n));
@@ -667,10 +670,11 @@ static int run_binning(EvalArgs& a, const BinPlan& b, const double* xyz, int64_t
     if (rc) return rc;
     bin_scan<<<1, 1024, 0, st>>>(counts, cursor, b.n_bins);
     if ((rc = check_launch("bin_scan"))) return rc;
-    bin_scatter<<<tiles, 256, smem3, st>>>(xyz, n, tile, b.n_bins, keys, cursor, perm, xs);
+    bin_scatter<<<tiles, 256, smem3, st>>>(xyz, n, tile, b.n_bins, keys, cursor,
+                                           with_perm ? perm : nullptr, xs);
     if ((rc = check_launch("bin_scatter"))) return rc;
     a.xyz = xs;
-    a.perm = perm;
+    a.perm = with_perm ? perm : nullptr;
     return AGB_OK;
 }
 
@@ -718,7 +722,8 @@ static int eval_impl(const agb_component* comps, int n_comps, const agb_leaf* le
             if (own_ws) cudaFreeAsync(ws, st);
             return set_err(AGB_ERR_ARG, "agb_eval_ws: workspace must be 256-byte aligned");
         }
-        rc = run_binning(a, b, xyz, n, (char*)ws, st);
+        const bool vjp = mode == AGB_MODE_VJP || mode == AGB_MODE_VJPF;
+        rc = run_binning(a, b, xyz, n, (char*)ws, st, !stage || vjp);
         if (stage) {
             a.stage = (double*)((char*)ws + ws_bytes(b, n));
             a.dest = (const int*)ws;             // bin_scatter leaves pos of point i in keys[i]
@@ -1121,8 +1126,10 @@ extern "C" int agb_eval_timed(const agb_component* comps, int n_comps, const agb
             return set_err(AGB_ERR_ARG, "agb_eval_timed: workspace of %zu bytes is smaller than "
                            "the %zu bytes agb_eval_timed_workspace_bytes asks for",
                            workspace_bytes, need + TP_LEAF_BYTES);
-        if ((rc = run_binning(a, b, xyz, n, ws, st))) return rc;
-        if (room >= staged) {
+        const bool stage = room >= staged;
+        const bool vjp = mode == AGB_MODE_VJP || mode == AGB_MODE_VJPF;
+        if ((rc = run_binning(a, b, xyz, n, ws, st, !stage || vjp))) return rc;
+        if (stage) {
             a.stage = (double*)(ws + ws_bytes(b, n));
             a.dest = (const int*)ws;
         }
