@@ -541,9 +541,18 @@ def main():
 
     # points pre-sorted by the binning key: the eval kernel alone on them sees the
     # same access pattern as inside a binned step (used to time that kernel)
+    # (the library's key: the point's block of 2^lb input rows, then its radial interval
+    # of the lmax-32 Multipole, n_int for the inner region, n_int + 1 beyond the grid)
     main_tb = pot._components[0].tables
-    rr = np.log(np.maximum(np.linalg.norm(xyz_np, axis=1), 1e-300))
-    key = np.clip(np.floor((rr - main_tb.logr_min) * main_tb.inv_dlogr), -1, main_tb.n_int)
+    rr = np.linalg.norm(xyz_np, axis=1)
+    tt = (np.log(np.maximum(rr, 1e-300)) - main_tb.logr_min) * main_tb.inv_dlogr
+    interval = np.where((rr < 1e-300) | (tt < 0), main_tb.n_int,
+                        np.where(tt >= main_tb.n_int, main_tb.n_int + 1,
+                                 np.floor(np.maximum(tt, 0)))).astype(np.int64)
+    lb = 19
+    while -(-N // (1 << lb)) * (main_tb.n_int + 2) > 8192:
+        lb += 1
+    key = (np.arange(N) >> lb) * (main_tb.n_int + 2) + interval
     xyz_sorted = torch.from_numpy(np.ascontiguousarray(xyz_np[np.argsort(key, kind="stable")])).to(dev)
 
     def device_step(t, prec, pts=None, binning=True):
