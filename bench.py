@@ -34,10 +34,10 @@ WORKLOAD = ("time-dependent composite: Multipole lmax=32 x 100 nodes + MiyamotoN
             "isotropic Hernquist a=10 kpc points")
 G = 4.30091727067736e-06
 # DRAM bytes (read + write) per point of one mixed-precision launch on this workload:
-# ncu dram__bytes_read.sum + dram__bytes_write.sum = 30.86 MB + 1.72 MB (mean of three
-# launches) at 1M points (profiles/eval_kernel_composite_1M_full.txt), scaled linearly
-# with the point count
-TRAFFIC_BYTES_PER_POINT = 32.58
+# ncu dram__bytes_read.sum + dram__bytes_write.sum = 100.85 MB + 86.01 MB for one 4M-point
+# launch of a binned step (512 threads per block; profiles/eval_kernel_composite_4M_full.txt),
+# scaled linearly with the point count
+TRAFFIC_BYTES_PER_POINT = 46.71
 # wall-clock budget of the reference arm's timed steps (seconds)
 REF_BUDGET_S = 150.0
 
@@ -707,7 +707,7 @@ def main():
                     "flops executed)",
             "achieved": achieved32, "peak": eff_peak32, "frac": achieved32 / eff_peak32,
             "traffic": TRAFFIC_BYTES_PER_POINT * N,
-            "traffic_source": "ncu DRAM read+write of the mixed launch at 1M points, scaled to N",
+            "traffic_source": "ncu DRAM read+write of one mixed launch at 4M points, scaled to N",
             "fp64_kernel": {"achieved": achieved64, "peak": pk64, "frac": achieved64 / pk64},
             "timing": "eval kernel alone, CUDA events on its stream, points pre-sorted by interval",
             "flops_per_step": fh + fp, "fp32_eligible_flops": fh,
