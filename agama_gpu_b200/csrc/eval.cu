@@ -378,12 +378,14 @@ static void launch_eval(EvalArgs& a, cudaStream_t st)
 {
     constexpr bool SHAPES = !AN && !DYN && MODE != AGB_MODE_VJP && MODE != AGB_MODE_VJPF;
     int b = (a.out_flags >> AGB_OUT_BLOCK_SHIFT) & 3;
-    // the default shape of large force calls: 512 threads per block, one block per SM.
-    // Measured on the 4M-point composite, binned step: mixed 4.18 -> 4.06 ms, FP64
-    // 7.02 -> 6.77 ms against 256 threads x 2 blocks per SM
+    // the default shape of large force calls of trees with a Multipole: 512 threads per
+    // block, one block per SM.  Measured on the 4M-point composite, binned step: mixed
+    // 4.18 -> 4.06 ms, FP64 7.02 -> 6.77 ms against 256 threads x 2 blocks per SM
     const int shape_bits = (15 << AGB_OUT_GRID_SHIFT) | (15 << AGB_OUT_PPT_SHIFT);
-    if (MODE == AGB_MODE_GRAD && b == 0 && !(a.out_flags & shape_bits) && a.n > (1LL << 21))
-        b = 2;
+    if (MODE == AGB_MODE_GRAD && b == 0 && !(a.out_flags & shape_bits) && a.n > (1LL << 21)) {
+        for (int L = 0; L < a.n_leaves; ++L)
+            if (a.comps[a.leaves[L].comp].kind == AGB_KIND_MULTIPOLE) { b = 2; break; }
+    }
     if constexpr (SHAPES) {
         if (b == 1) return launch_eval_bs<MODE, R, AN, DYN, 128>(a, st);
         if constexpr (eval_min_blocks(MODE, AN, 256) >= 2)
