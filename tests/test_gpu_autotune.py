@@ -49,6 +49,28 @@ def test_launch_shapes_agree(n, tmp_path, monkeypatch):
     assert fresh._tuned == pot._tuned
 
 
+def test_large_force_call_default_shape_matches_256_threads():
+    """Above 2^21 points a force call of a tree with a Multipole defaults to 512 threads per
+    block; its results equal the 256-thread shape's (both precisions, sorted and unsorted)."""
+    import torch
+    from agama_gpu_b200 import _lib, autotune
+    from agama_gpu_b200.synthetic import hernquist_points
+    pot = _pot()
+    n = (1 << 21) + 4099
+    x = torch.from_numpy(hernquist_points(n, 10.0, 6)).cuda()
+    for prec in ("fp64", "mixed"):
+        pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
+        for binning in (True, False):
+            pot.set_binning(binning)
+            pot.__dict__.pop("_tuned", None)
+            p512, f512, _, _ = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
+            autotune._set(pot, _lib.MODE_GRAD, pc, n, 1 << _lib.OUT_GRID_SHIFT)   # 256 x 1
+            p256, f256, _, _ = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
+            assert torch.equal(p512, p256) and torch.equal(f512, f256), (prec, binning)
+    pot.set_binning(True)
+    pot.__dict__.pop("_tuned", None)
+
+
 def test_tune_batch_keeps_results():
     import torch
     import agama_gpu_b200 as agb
