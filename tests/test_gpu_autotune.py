@@ -49,9 +49,10 @@ def test_launch_shapes_agree(n, tmp_path, monkeypatch):
     assert fresh._tuned == pot._tuned
 
 
-def test_large_force_call_default_shape_matches_256_threads():
-    """Above 2^21 points a force call of a tree with a Multipole defaults to 512 threads per
-    block; its results equal the 256-thread shape's (both precisions, sorted and unsorted)."""
+def test_large_call_default_shapes_match_256_threads():
+    """Above 2^21 points a call of a tree with a Multipole defaults to 512 threads per
+    block (force) or 128 (Hessian; 16 points per thread in FP64); the results equal the
+    256-thread shape's (both precisions, sorted and unsorted)."""
     import torch
     from agama_gpu_b200 import _lib, autotune
     from agama_gpu_b200.synthetic import hernquist_points
@@ -62,11 +63,14 @@ def test_large_force_call_default_shape_matches_256_threads():
         pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
         for binning in (True, False):
             pot.set_binning(binning)
-            pot.__dict__.pop("_tuned", None)
-            p512, f512, _, _ = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
-            autotune._set(pot, _lib.MODE_GRAD, pc, n, 1 << _lib.OUT_GRID_SHIFT)   # 256 x 1
-            p256, f256, _, _ = pot._launch(x, 0.0, _lib.MODE_GRAD, True, precision=prec)
-            assert torch.equal(p512, p256) and torch.equal(f512, f256), (prec, binning)
+            for mode in (_lib.MODE_GRAD, _lib.MODE_HESS):
+                pot.__dict__.pop("_tuned", None)
+                a = pot._launch(x, 0.0, mode, True, precision=prec)
+                autotune._set(pot, mode, pc, n, 1 << _lib.OUT_GRID_SHIFT)   # 256 x 1 per slot
+                b = pot._launch(x, 0.0, mode, True, precision=prec)
+                for u, v in zip(a, b):
+                    if v is not None:
+                        assert torch.equal(u, v), (prec, binning, mode)
     pot.set_binning(True)
     pot.__dict__.pop("_tuned", None)
 
