@@ -77,9 +77,9 @@ extern "C" {
    bits 12-13: threads per block: 0 = the default, 1 = 128, 2 = 512 (512 in the
                potential, force and density modes; the Hessian modes keep 256).
                The default is 256, except for calls of more than 2^21 points of a
-               tree with a Multipole and no other shape bit set: force calls take
-               512 threads, one block per SM; Hessian calls 128 threads (and 16
-               points per thread in FP64).  Host-leaf calls of agb_eval / agb_eval_ws /
+               tree with a Multipole and no other shape bit set: force and density
+               calls take 512 threads, one block per SM; Hessian calls 128 threads
+               (and 16 points per thread in FP64).  Host-leaf calls of agb_eval / agb_eval_ws /
                agb_eval_static only.
    bits 16-19: points per thread p, 1-15: each block takes a contiguous range of
                threads x 2^(p-1) points and the grid grows with n (overrides

@@ -51,8 +51,8 @@ def test_launch_shapes_agree(n, tmp_path, monkeypatch):
 
 def test_large_call_default_shapes_match_256_threads():
     """Above 2^21 points a call of a tree with a Multipole defaults to 512 threads per
-    block (force) or 128 (Hessian; 16 points per thread in FP64); the results equal the
-    256-thread shape's (both precisions, sorted and unsorted)."""
+    block (force, density) or 128 (Hessian; 16 points per thread in FP64); the results
+    equal the 256-thread shape's (both precisions, sorted and unsorted)."""
     import torch
     from agama_gpu_b200 import _lib, autotune
     from agama_gpu_b200.synthetic import hernquist_points
@@ -63,7 +63,7 @@ def test_large_call_default_shapes_match_256_threads():
         pc = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
         for binning in (True, False):
             pot.set_binning(binning)
-            for mode in (_lib.MODE_GRAD, _lib.MODE_HESS):
+            for mode in (_lib.MODE_GRAD, _lib.MODE_HESS, _lib.MODE_DENS):
                 pot.__dict__.pop("_tuned", None)
                 a = pot._launch(x, 0.0, mode, True, precision=prec)
                 autotune._set(pot, mode, pc, n, 1 << _lib.OUT_GRID_SHIFT)   # 256 x 1 per slot
