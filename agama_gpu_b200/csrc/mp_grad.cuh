@@ -658,7 +658,7 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
 // global memory directly.  Warps whose points straddle intervals add each
 // lane's six values with atomics.
 template <typename R>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(64, 4)
 mp_adjoint_kernel(const __grid_constant__ MPAdjArgs a)
 {
     extern __shared__ __align__(16) unsigned char agb_adj_smem[];
