@@ -1317,10 +1317,11 @@ static int multipole_adjoint_impl(const agb_component* comp, const agb_leaf* lea
     if (!rc) {
         // per warp: the (U, V) tile, plus the interval accumulator.  Blocks of 2 warps
         // (64 threads at 255 registers, 4 resident per SM: the same 8 warps as one block
-        // of 256, scheduled in finer pieces), two waves of them: the backward leapfrog
-        // step at 2.1M particles 2.006 -> 1.960 ms (128 threads: 1.968, 32: 1.986 ms).
+        // of 256, scheduled in finer pieces), four waves of them: the backward leapfrog
+        // step at 2.1M particles 2.006 -> 1.925 ms (two waves 1.955, one 1.945, eight
+        // 1.984 ms; 128-thread blocks 1.968, 32-thread 1.986 ms in two waves).
         // 384 threads at 168 registers spilled and made the step 22 % slower.
-        const int grid = (int)std::min<long long>((long long)num_sms() * 8, (n + 63) / 64);
+        const int grid = (int)std::min<long long>((long long)num_sms() * 16, (n + 63) / 64);
         const long long warps = (long long)grid * 2, groups = (n + 31) / 32;
         g.chunk = ((groups + warps - 1) / warps) * 32;
         const int tile = precision == AGB_PREC_MIXED ? adj_tile_bytes<float>() : adj_tile_bytes<double>();
