@@ -1390,7 +1390,7 @@ struct AdjStepPtrs {
 // One thread per particle.  The staged record (read through its sorted
 // position) and lv are loaded before the analytic leaves' arithmetic, so the
 // latency of that gather overlaps the FP64 Hessian instead of following it.
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(64, 8)
 adjoint_step_kernel(const __grid_constant__ EvalArgs a, const __grid_constant__ AdjStepPtrs p)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -1547,7 +1547,8 @@ extern "C" int agb_adjoint_step(const agb_component* comps, int n_comps, const a
     q.dest = keep.dest; q.stage = keep.stage;
     q.n = n; q.stage_rec = drift ? 6 : 3; q.drift = drift ? 1 : 0; q.lv_cot = lv_cot ? 1 : 0;
     q.dt = dt; q.c = c; q.c_in = c_in; q.k = k; q.dt_drift = dt_drift;
-    adjoint_step_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(a, q);
+    // 64-thread blocks, 8 per SM (the same 16 warps as 2 x 256): 1.3 % faster backward step
+    adjoint_step_kernel<<<grid_for(n * 4), 64, 0, (cudaStream_t)stream>>>(a, q);
     return check_launch("adjoint_step_kernel");
 }
 
