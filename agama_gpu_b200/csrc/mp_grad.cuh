@@ -616,7 +616,7 @@ __device__ __forceinline__ void mp_adj_walk(const DevComp& c, int kw, R s, doubl
             const int ts = m * AGB_SKIP_N;
             Pp = (m == 0) ? seed : R(0);
             dPp = R(0);
-            #pragma unroll 3
+            #pragma unroll 4
             for (l = l0 + 2; l <= c.lmax; l += 2) {
                 const auto ab = MPConst<R>::skip(ts + (l >> 1));
                 const R t = c2 + (R)ab.x;
